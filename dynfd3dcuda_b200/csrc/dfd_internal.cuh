@@ -1,0 +1,135 @@
+// Internal definitions shared by the CUDA kernels and the host side of the
+// B200 dynamic-rupture time step.
+//
+// HBM layout (per context, all FP32 unless noted):
+//   W[4]      four 9-field volume buffers (nx, nz, ny), y fastest, 3 ghost nodes;
+//             a step cycles A -> B -> C -> B -> A so that the stencil input of a stage is
+//             never written during that stage and no right-hand-side array exists
+//   M         13 fields xix xiy xiz etx ety etz ztx zty ztz jac lam mu rho
+//   aux       per PML face, 3 buffers (current, step start, RK accumulator) of 9 fields
+//   FW[2]     split-node state ping-pong (9, 2, nz, ny); Fm / Ft RK registers
+//   tables    fault coefficient tables as planes [table][element][nz*ny] (coalesced)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dfd {
+
+// 5-point one-sided DRP (MacCormack-type) coefficients and the traction-image
+// coefficients (reference macdrp.h:23-40), with the 2-/3-point boundary operators
+// (macdrp.h:101-130).
+#define DFD_C1 0.29164704779069994f
+#define DFD_C2 0.66674514216519998f
+#define DFD_C3 1.2501177132452999f
+#define DFD_C4 0.33341180882999999f
+#define DFD_C5 0.041686285540599999f
+#define DFD_A0P (-1.250039237746600f)
+#define DFD_A0M (1.250039237746600f)
+#define DFD_A1 1.541764761036000f
+#define DFD_A2 (-0.333411808829999f)
+#define DFD_A3 0.0416862855405999f
+#define DFD_C24_1 (7.0f / 6.0f)
+#define DFD_C24_2 (4.0f / 3.0f)
+#define DFD_C24_3 (1.0f / 6.0f)
+
+// fault coefficient table planes (index t of ntab, each 9 elements per node unless noted)
+enum Tab {
+  T_D21_1 = 0, T_D22_1, T_D23_1, T_D31_1, T_D32_1, T_D33_1,
+  T_D21_2, T_D22_2, T_D23_2, T_D31_2, T_D32_2, T_D33_2,
+  T_M2P1, T_M2P2, T_M2P3, T_M2P4, T_M2P5,
+  T_P2M1, T_P2M2, T_P2M3, T_P2M4, T_P2M5,
+  T_T1VXM, T_VYVXM, T_VZVXM, T_T1VXP, T_VYVXP, T_VZVXP,
+  NTAB9
+};
+// free-surface row tables, 9 elements per j
+enum TabF { TF_VX2VZ1 = 0, TF_VY2VZ1, TF_VX2VZ2, TF_VY2VZ2, TF_P2M1, TF_P2M2, TF_P2M3, TF_M2P1, TF_M2P2, TF_M2P3, NTABF };
+
+struct Dims {
+  int ni, nj, nk;       // interior sizes NX NY NZ
+  int nx, ny, nz;       // padded sizes
+  int i0;               // padded x index of the fault plane (nx/2)
+  int N;                // PML thickness
+  long long nxyz, nyz;  // field strides
+};
+
+// Arguments of the fused volume stage kernel.
+struct VolArgs {
+  Dims d;
+  const float* __restrict__ Win;   // stencil input of this stage
+  const float* __restrict__ W0;    // step-start state (stages 1, 2)
+  float* __restrict__ Wout;        // output of this stage
+  float* __restrict__ T;           // RK accumulator
+  const float* __restrict__ M;
+  const float* __restrict__ rBx;   // 1/beta per axis (PML), 1 outside
+  const float* __restrict__ rBy;
+  const float* __restrict__ rBz;
+  const float* __restrict__ Bx;    // beta per axis
+  const float* __restrict__ By;
+  const float* __restrict__ Bz;
+  const float* __restrict__ Dpx;   // d/beta per axis
+  const float* __restrict__ Dpy;
+  const float* __restrict__ Dpz;
+  const float* __restrict__ Apx;   // alpha per axis
+  const float* __restrict__ Apy;
+  const float* __restrict__ Apz;
+  float* aux[6];                   // current PML state per face (x1 x2 y1 y2 z1 z2) or null
+  float* aux0[6];                  // step-start copy
+  float* auxT[6];                  // RK accumulator
+  const float* __restrict__ mVx2Vz;  // (nx, ny, 9) free-surface transforms
+  const float* __restrict__ mVy2Vz;
+  const float* __restrict__ dampx;   // Cerjan 1-D profiles (padded index) or null
+  const float* __restrict__ dampy;
+  const float* __restrict__ dampz;
+  const int* __restrict__ united;    // (NZ, NY) or null when the fault is off
+  float rDH, rka, rkb;
+  int irk, freenode;
+};
+
+// Arguments of the two fault kernels (per-node trial kernel and band kernel).
+struct FaultArgs {
+  Dims d;
+  float* Win;                      // stage input volume (the trial kernel writes W[i0])
+  const float* __restrict__ W0;
+  float* Wout;
+  float* T;
+  const float* __restrict__ M;
+  const float* __restrict__ mVx2Vz;
+  const float* __restrict__ mVy2Vz;
+  const float* __restrict__ dampx;
+  const float* __restrict__ dampy;
+  const float* __restrict__ dampz;
+  const float* FWin;               // split nodes, stage input
+  float* FWout;                    // split nodes, stage output
+  float* Fm;                       // split nodes, step start
+  float* Ft;                       // split nodes, RK accumulator
+  float* T1;                       // (3, 7, nz, ny) traction layers T11 T12 T13
+  float* mT1;                      // (3, nz, ny) T1 at the fault at step start
+  float* hT1;                      // (3, nz, ny) T1 rate
+  const float* __restrict__ tab;   // NTAB9 * 9 * nyz
+  const float* __restrict__ tabf;  // NTABF * 9 * ny
+  const float* __restrict__ vecn;  // (3, nz, ny) planes
+  const float* __restrict__ vecs1;
+  const float* __restrict__ vecs2;
+  const float* __restrict__ rhof;  // (2, nz, ny)
+  // (NZ, NY) planes
+  float *slip, *mslip, *tslip, *hslip, *State, *mState, *tState;
+  float *Vs1, *Vs2, *Tn, *Ts1, *Ts2, *tTn, *tTs1, *tTs2;
+  float *sx, *sy, *sz;             // str_init
+  const float *T0x, *T0y, *T0z, *dT0x, *dT0y, *dT0z;
+  const float *str_peak, *Dc, *C0, *a, *b, *L, *Vw;
+  float *init_t0, *friction;
+  int *init_t0_flag, *flag_rup;
+  const int *united, *faultgrid, *rupy, *rupz;
+  unsigned long long* newton;      // [0] iterations, [1] capped solves
+  const float* guess_net;          // learned-guess MLP weights or null
+  // scalars
+  float rDH, DH, DT, rka, rkb, mu_d, viscosity;
+  double dDT, smooth_load_T, f0, V0, fw, Vini;
+  int it, irk, FX, FY, FZ, freenode, friction_type, inport_stress, NY, NZ, rs_guess;
+};
+
+__host__ __device__ inline long long idx3(const Dims& d, int i, int j, int k) {
+  return (long long)j + (long long)k * d.ny + (long long)i * d.nyz;
+}
+
+}  // namespace dfd

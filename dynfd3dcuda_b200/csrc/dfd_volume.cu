@@ -1,0 +1,275 @@
+// Fused volume stage: one pass per RK stage computes the velocity-stress right-hand
+// side with the 5-point one-sided DRP operators and curvilinear metric terms
+// (reference wave.cu:8-494), the free-surface rows and traction image (wave.cu:205-487),
+// the ADE PML auxiliary equations of all six faces (pmlx.cu:8-214, pmly.cu, pmlz.cu),
+// the classic RK4 register update (rk4.cu:20-33,154-257) and the Cerjan sponge
+// (cerjan.cu:166-200).  The right-hand side never reaches HBM: each stage reads the
+// stencil input (9 fields), the 12 metric/media fields and its RK registers, and writes
+// its output and accumulator -- 39/57/57/39 floats per node for stages 0..3.
+//
+// Nodes of the seven x-layers around the fault whose (j,k) is not "united" are left
+// to the band kernel (dfd_fault.cu), exactly the nodes whose right-hand side the
+// reference overwrites in fault_dvelo / fault_dstrs.
+#include "dfd_internal.cuh"
+
+namespace dfd {
+
+template <int F>
+__device__ __forceinline__ float d5(const float* __restrict__ v, long long q, long long s) {
+  if (F == 1)
+    return -DFD_C1 * __ldg(v + q - s) - DFD_C2 * __ldg(v + q) + DFD_C3 * __ldg(v + q + s) -
+           DFD_C4 * __ldg(v + q + 2 * s) + DFD_C5 * __ldg(v + q + 3 * s);
+  else
+    return -DFD_C5 * __ldg(v + q - 3 * s) + DFD_C4 * __ldg(v + q - 2 * s) - DFD_C3 * __ldg(v + q - s) +
+           DFD_C2 * __ldg(v + q) + DFD_C1 * __ldg(v + q + s);
+}
+template <int F>
+__device__ __forceinline__ float d5a(const float* v, int c) {  // on a 7-point register line, centre c
+  if (F == 1) return -DFD_C1 * v[c - 1] - DFD_C2 * v[c] + DFD_C3 * v[c + 1] - DFD_C4 * v[c + 2] + DFD_C5 * v[c + 3];
+  else return -DFD_C5 * v[c - 3] + DFD_C4 * v[c - 2] - DFD_C3 * v[c - 1] + DFD_C2 * v[c] + DFD_C1 * v[c + 1];
+}
+
+// axis contribution of the velocity-stress system for one set of derivatives d[9]
+// (Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz) and metric row e (wave.cu:133-141)
+__device__ __forceinline__ void axis_terms(const float* d, float e0, float e1, float e2, float lam, float mu,
+                                           float rrho, float* D) {
+  float l2m = lam + 2.0f * mu;
+  D[0] = (d[3] * e0 + d[6] * e1 + d[7] * e2) * rrho;
+  D[1] = (d[6] * e0 + d[4] * e1 + d[8] * e2) * rrho;
+  D[2] = (d[7] * e0 + d[8] * e1 + d[5] * e2) * rrho;
+  D[3] = d[0] * e0 * l2m + d[1] * e1 * lam + d[2] * e2 * lam;
+  D[4] = d[0] * e0 * lam + d[1] * e1 * l2m + d[2] * e2 * lam;
+  D[5] = d[0] * e0 * lam + d[1] * e1 * lam + d[2] * e2 * l2m;
+  D[6] = (d[0] * e1 + d[1] * e0) * mu;
+  D[7] = (d[0] * e2 + d[2] * e0) * mu;
+  D[8] = (d[1] * e2 + d[2] * e1) * mu;
+}
+
+// traction vector jac * e_axis . sigma at node q
+__device__ __forceinline__ void traction(const float* __restrict__ W, const float* __restrict__ M, long long n,
+                                         long long q, int mo, float& t1, float& t2, float& t3) {
+  float e0 = __ldg(M + mo * n + q), e1 = __ldg(M + (mo + 1) * n + q), e2 = __ldg(M + (mo + 2) * n + q);
+  float jac = __ldg(M + 9 * n + q);
+  float txx = __ldg(W + 3 * n + q), tyy = __ldg(W + 4 * n + q), tzz = __ldg(W + 5 * n + q);
+  float txy = __ldg(W + 6 * n + q), txz = __ldg(W + 7 * n + q), tyz = __ldg(W + 8 * n + q);
+  t1 = (e0 * txx + e1 * txy + e2 * txz) * jac;
+  t2 = (e0 * txy + e1 * tyy + e2 * tyz) * jac;
+  t3 = (e0 * txz + e1 * tyz + e2 * tzz) * jac;
+}
+
+// PML auxiliary update of one face for this node: accumulates -aux/beta into p[] and
+// advances aux in place with the RK4 registers (pmlx.cu:165-208, rk4.cu:208-255).
+__device__ __forceinline__ void pml_face(const VolArgs& a, int face, long long qa, long long st, float rb, float b,
+                                         float dd, float al, const float* Dv, const float* dzv, float ez0,
+                                         float ez1, float ez2, float lam, float mu, float* p) {
+  float* aux = a.aux[face];
+  float* aux0 = a.aux0[face];
+  float* auxT = a.auxT[face];
+  float ad = -(al + dd);
+  float add[6];
+  if (dzv) {
+    float l2m = lam + 2.0f * mu, c = dd * b;
+    add[0] = c * (l2m * ez0 * dzv[0] + lam * ez1 * dzv[1] + lam * ez2 * dzv[2]);
+    add[1] = c * (lam * ez0 * dzv[0] + l2m * ez1 * dzv[1] + lam * ez2 * dzv[2]);
+    add[2] = c * (lam * ez0 * dzv[0] + lam * ez1 * dzv[1] + l2m * ez2 * dzv[2]);
+    add[3] = c * mu * (ez1 * dzv[0] + ez0 * dzv[1]);
+    add[4] = c * mu * (ez2 * dzv[0] + ez0 * dzv[2]);
+    add[5] = c * mu * (ez2 * dzv[1] + ez1 * dzv[2]);
+  }
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    long long x = f * st + qa;
+    float w = aux[x];
+    p[f] += -w * rb;
+    float h = ad * w + dd * Dv[f];
+    if (dzv && f >= 3) h += add[f - 3];
+    if (a.irk == 0) {
+      aux0[x] = w;
+      auxT[x] = fmaf(a.rkb, h, w);
+      aux[x] = fmaf(a.rka, h, w);
+    } else if (a.irk < 3) {
+      auxT[x] = fmaf(a.rkb, h, auxT[x]);
+      aux[x] = fmaf(a.rka, h, aux0[x]);
+    } else {
+      aux[x] = fmaf(a.rkb, h, auxT[x]);
+    }
+  }
+}
+
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(256) volume_stage_kernel(VolArgs a) {
+  const Dims& d = a.d;
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = blockIdx.y * blockDim.y + threadIdx.y;
+  int i = blockIdx.z * blockDim.z + threadIdx.z;
+  if (j >= d.nj || k >= d.nk || i >= d.ni) return;
+  int i1 = i + 3, j1 = j + 3, k1 = k + 3;
+  if (a.united && i1 >= d.i0 - 3 && i1 <= d.i0 + 3 && !a.united[j + k * d.nj]) return;  // band node
+  const long long n = d.nxyz;
+  const long long q = idx3(d, i1, j1, k1);
+  const float* __restrict__ W = a.Win;
+  const float* __restrict__ M = a.M;
+
+  float lam = __ldg(M + 10 * n + q), mu = __ldg(M + 11 * n + q);
+  float rrho = 1.0f / __ldg(M + 12 * n + q);
+  float rb1 = __ldg(a.rBx + i), rb2 = __ldg(a.rBy + j), rb3 = __ldg(a.rBz + k);
+  float h[9], p[9], dv[9], D[9];
+#pragma unroll
+  for (int f = 0; f < 9; f++) p[f] = 0.0f;
+  float dxv[3], dyv[3];
+  const bool top = a.freenode && k == d.nk - 1;
+  const bool px1 = a.aux[0] && i < d.N, px2 = a.aux[1] && i >= d.ni - d.N;
+  const bool py1 = a.aux[2] && j < d.N, py2 = a.aux[3] && j >= d.nj - d.N;
+  const bool pz1 = a.aux[4] && k < d.N, pz2 = a.aux[5] && k >= d.nk - d.N;
+  float ez0 = __ldg(M + 6 * n + q), ez1 = __ldg(M + 7 * n + q), ez2 = __ldg(M + 8 * n + q);
+
+  // ---- x ----
+#pragma unroll
+  for (int f = 0; f < 9; f++) dv[f] = d5<FX>(W + f * n, q, d.nyz) * a.rDH;
+  dxv[0] = dv[0]; dxv[1] = dv[1]; dxv[2] = dv[2];
+  axis_terms(dv, __ldg(M + q), __ldg(M + n + q), __ldg(M + 2 * n + q), lam, mu, rrho, D);
+#pragma unroll
+  for (int f = 0; f < 9; f++) h[f] = D[f] * rb1;
+  if (px1 || px2) {
+    float dz[3];
+    if (top) {
+      const float* m = a.mVx2Vz + (j1 + (long long)i1 * d.ny) * 9;
+#pragma unroll
+      for (int r = 0; r < 3; r++) dz[r] = m[3 * r] * dxv[0] + m[3 * r + 1] * dxv[1] + m[3 * r + 2] * dxv[2];
+    }
+    long long st = (long long)d.N * d.nj * d.nk;
+    int ia = px1 ? i : i - (d.ni - d.N);
+    long long qa = j + (long long)k * d.nj + (long long)ia * d.nj * d.nk;
+    pml_face(a, px1 ? 0 : 1, qa, st, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D,
+             top ? dz : nullptr, ez0, ez1, ez2, lam, mu, p);
+  }
+  // ---- y ----
+#pragma unroll
+  for (int f = 0; f < 9; f++) dv[f] = d5<FY>(W + f * n, q, 1) * a.rDH;
+  dyv[0] = dv[0]; dyv[1] = dv[1]; dyv[2] = dv[2];
+  axis_terms(dv, __ldg(M + 3 * n + q), __ldg(M + 4 * n + q), __ldg(M + 5 * n + q), lam, mu, rrho, D);
+#pragma unroll
+  for (int f = 0; f < 9; f++) h[f] += D[f] * rb2;
+  if (py1 || py2) {
+    float dz[3];
+    if (top) {
+      const float* m = a.mVy2Vz + (j1 + (long long)i1 * d.ny) * 9;
+#pragma unroll
+      for (int r = 0; r < 3; r++) dz[r] = m[3 * r] * dyv[0] + m[3 * r + 1] * dyv[1] + m[3 * r + 2] * dyv[2];
+    }
+    long long st = (long long)d.N * d.nk * d.ni;
+    int ja = py1 ? j : j - (d.nj - d.N);
+    long long qa = ja + (long long)k * d.N + (long long)i * d.N * d.nk;
+    pml_face(a, py1 ? 2 : 3, qa, st, rb2, __ldg(a.By + j), __ldg(a.Dpy + j), __ldg(a.Apy + j), D,
+             top ? dz : nullptr, ez0, ez1, ez2, lam, mu, p);
+  }
+  // ---- z ----
+#pragma unroll
+  for (int f = 0; f < 9; f++) dv[f] = d5<FZ>(W + f * n, q, d.ny) * a.rDH;
+  float Dz_plain[9];
+  axis_terms(dv, ez0, ez1, ez2, lam, mu, rrho, Dz_plain);
+#pragma unroll
+  for (int f = 0; f < 9; f++) D[f] = Dz_plain[f];
+  if (a.freenode && k >= d.nk - 3) {
+    // velocity z-derivatives on the top rows (wave.cu:205-245)
+    float dz[3];
+    if (k == d.nk - 1) {
+      const float* mx = a.mVx2Vz + (j1 + (long long)i1 * d.ny) * 9;
+      const float* my = a.mVy2Vz + (j1 + (long long)i1 * d.ny) * 9;
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        dz[r] = (mx[3 * r] * dxv[0] + mx[3 * r + 1] * dxv[1] + mx[3 * r + 2] * dxv[2]) +
+                (my[3 * r] * dyv[0] + my[3 * r + 1] * dyv[1] + my[3 * r + 2] * dyv[2]);
+    } else if (k == d.nk - 2) {
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const float* v = W + r * n;
+        dz[r] = (FZ == 1 ? (__ldg(v + q + d.ny) - __ldg(v + q)) : (__ldg(v + q) - __ldg(v + q - d.ny))) * a.rDH;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const float* v = W + r * n;
+        dz[r] = (FZ == 1 ? (-DFD_C24_1 * __ldg(v + q) + DFD_C24_2 * __ldg(v + q + d.ny) - DFD_C24_3 * __ldg(v + q + 2 * d.ny))
+                         : (DFD_C24_3 * __ldg(v + q - 2 * d.ny) - DFD_C24_2 * __ldg(v + q - d.ny) + DFD_C24_1 * __ldg(v + q))) *
+                a.rDH;
+      }
+    }
+    float dd[9];
+    dd[0] = dz[0]; dd[1] = dz[1]; dd[2] = dz[2];
+    dd[3] = dv[3]; dd[4] = dv[4]; dd[5] = dv[5]; dd[6] = dv[6]; dd[7] = dv[7]; dd[8] = dv[8];
+    float Dm[9];
+    axis_terms(dd, ez0, ez1, ez2, lam, mu, rrho, Dm);
+#pragma unroll
+    for (int f = 3; f < 9; f++) D[f] = Dm[f];
+  }
+#pragma unroll
+  for (int f = 0; f < 9; f++) h[f] += D[f] * rb3;
+  if (pz1 || pz2) {
+    long long st = (long long)d.N * d.ni * d.nj;
+    int ka = pz1 ? k : k - (d.nk - d.N);
+    long long qa = j + (long long)ka * d.nj + (long long)i * d.nj * d.N;
+    pml_face(a, pz1 ? 4 : 5, qa, st, rb3, __ldg(a.Bz + k), __ldg(a.Dpz + k), __ldg(a.Apz + k), Dz_plain, nullptr,
+             ez0, ez1, ez2, lam, mu, p);
+  }
+  // ---- traction image for the momentum equation on the top three rows (wave.cu:398-487)
+  if (a.freenode && k >= d.nk - 3) {
+    int ik = d.nk - 1 - k;
+    float rrhojac = rrho / __ldg(M + 9 * n + q);
+    float v1[3][7], v2[3][7], v3[3][7];
+#pragma unroll
+    for (int l = 0; l < 7; l++) {
+      traction(W, M, n, q + (l - 3) * d.nyz, 0, v1[0][l], v1[1][l], v1[2][l]);
+      traction(W, M, n, q + (l - 3), 3, v2[0][l], v2[1][l], v2[2][l]);
+      traction(W, M, n, q + (long long)(l - 3) * d.ny, 6, v3[0][l], v3[1][l], v3[2][l]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      v3[c][ik + 3] = 0.0f;
+      for (int l = 0; l < 3 - ik; l++) v3[c][6 - l] = -v3[c][l + 2 * ik];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float tx = d5a<FX>(v1[c], 3) * a.rDH, ty = d5a<FY>(v2[c], 3) * a.rDH, tz = d5a<FZ>(v3[c], 3) * a.rDH;
+      h[c] = (tx * rb1 + ty * rb2 + tz * rb3) * rrhojac;
+    }
+  }
+  // ---- RK4 registers and Cerjan sponge
+  float damp = 1.0f;
+  if (a.dampx) damp = fminf(fminf(__ldg(a.dampx + i1), __ldg(a.dampy + j1)), __ldg(a.dampz + k1));
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    float hf = h[f] + p[f];
+    long long x = f * n + q;
+    float w;
+    if (a.irk == 0) {
+      float w0 = __ldg(W + x);
+      a.T[x] = fmaf(a.rkb, hf, w0);
+      w = fmaf(a.rka, hf, w0);
+    } else if (a.irk < 3) {
+      a.T[x] = fmaf(a.rkb, hf, a.T[x]);
+      w = fmaf(a.rka, hf, __ldg(a.W0 + x));
+    } else {
+      w = fmaf(a.rkb, hf, a.T[x]);
+    }
+    a.Wout[x] = w * damp;
+  }
+}
+
+void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s) {
+  dim3 block(32, 4, 2);
+  dim3 grid((a.d.nj + 31) / 32, (a.d.nk + 3) / 4, (a.d.ni + 1) / 2);
+  int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: volume_stage_kernel<-1, -1, -1><<<grid, block, 0, s>>>(a); break;
+    case 1: volume_stage_kernel<-1, -1, 1><<<grid, block, 0, s>>>(a); break;
+    case 2: volume_stage_kernel<-1, 1, -1><<<grid, block, 0, s>>>(a); break;
+    case 3: volume_stage_kernel<-1, 1, 1><<<grid, block, 0, s>>>(a); break;
+    case 4: volume_stage_kernel<1, -1, -1><<<grid, block, 0, s>>>(a); break;
+    case 5: volume_stage_kernel<1, -1, 1><<<grid, block, 0, s>>>(a); break;
+    case 6: volume_stage_kernel<1, 1, -1><<<grid, block, 0, s>>>(a); break;
+    default: volume_stage_kernel<1, 1, 1><<<grid, block, 0, s>>>(a); break;
+  }
+}
+
+}  // namespace dfd

@@ -1,0 +1,139 @@
+/*
+ * dfd_b200.h -- C ABI of the B200-native curved-grid finite-difference
+ * dynamic-rupture time step (drop-in for the single-rank path of
+ * wenqiang-geophys/dynfd3dcuda).
+ *
+ * Every entry point returns an int status (DFD_OK == 0).  The library owns all device
+ * memory of a context; host arrays cross the boundary in the reference's layouts:
+ *   volume field    (nx, nz, ny) with y fastest, nx = NX+6 (3 ghost nodes per side),
+ *                   field order Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz   (common.h:99-101)
+ *   fault plane     (NZ, NY) with y fastest                        (alloc.cu:123-168)
+ *   split nodes     (9, 2, nz, ny): field, side (-,+), z, y         (alloc.cu:96)
+ * There is no global state: every parameter lives in the context, so several contexts
+ * (one per thread or per scenario) can coexist on one GPU.
+ */
+#ifndef DFD_B200_H
+#define DFD_B200_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DFD_OK = 0,
+  DFD_ERR_PARAM = 1,      /* bad or unsupported parameter */
+  DFD_ERR_CUDA = 2,       /* CUDA call failed (sticky in the context) */
+  DFD_ERR_IO = 3,         /* file missing or malformed */
+  DFD_ERR_STATE = 4,      /* call out of order (e.g. step before precompute) */
+  DFD_ERR_CFL = 5,        /* DT above the stability limit 1.3 hmin / vpmax */
+  DFD_ERR_NONFINITE = 6,  /* NaN/Inf found in the fault state */
+  DFD_ERR_NEWTON = 7      /* rate-and-state Newton hit its iteration cap */
+};
+
+/* Job parameters: the reference's Params fields (common.h:49-84) plus the reference's
+ * compile-time switches (Makefile:57-161) as runtime flags with the reference's
+ * defaults.  Filled by dfd_params_default() and dfd_params_load_json(). */
+typedef struct dfd_params {
+  int NX, NY, NZ;
+  int NT;
+  double TMAX, DT, DH;
+  int INPORT_GRID_TYPE, INPORT_STRESS_TYPE, Friction_type;
+  int EXPORT_TIME_SKIP, EXPORT_WAVE_SLICE_X, EXPORT_WAVE_SLICE_Y, EXPORT_WAVE_SLICE_Z;
+  int PML_N;
+  double PML_velocity, PML_bmax, PML_fc;
+  int DAMP_N;
+  double mu_s, mu_d, mu_0, Dc, C0;
+  double f0, V0, Vini, fw, L;
+  double smooth_load_T, viscosity;
+  int Fault_grid[4];
+  int Asp_grid[4];
+  double bi_vp1, bi_vs1, bi_rho1, bi_vp2, bi_vs2, bi_rho2;
+  /* switches (reference macros): free surface, PML, Cerjan sponge, normal refinement */
+  int free_surface, use_pml, use_cerjan, normal_refine;
+  /* 0 = plain Newton initial guess (reference), 1 = learned guess with Newton fallback */
+  int rs_guess;
+  char OUT[1024];
+  char Fault_geometry[1024];
+  char Fault_init_stress[1024];
+  char Media1D[1024];
+} dfd_params;
+
+typedef struct dfd_ctx dfd_ctx;
+
+/* Named on-fault / split-node / layer arrays for dfd_get_fault / dfd_set_fault. */
+enum {
+  DFD_F_SLIP = 0, DFD_F_HSLIP, DFD_F_VS1, DFD_F_VS2, DFD_F_TN, DFD_F_TS1, DFD_F_TS2, DFD_F_STATE,
+  DFD_F_INIT_T0, DFD_F_TTN, DFD_F_TTS1, DFD_F_TTS2, DFD_F_STR_PEAK, DFD_F_FRICTION,
+  DFD_F_UNITED, DFD_F_FAULTGRID,            /* int32 masks, returned as float */
+  DFD_F_SPLIT,                               /* (9, 2, nz, ny) split-node state   */
+  DFD_F_T1,                                  /* (3, 7, nz, ny) T11 T12 T13 layers */
+  DFD_F_HT1,                                 /* (3, nz, ny) hT11 hT12 hT13        */
+  DFD_F_COUNT
+};
+
+/* ---- parameters (set_params.cu:56-297) ---- */
+int dfd_params_default(dfd_params *p);
+int dfd_params_load_json(const char *path, dfd_params *p);
+
+/* ---- lifetime (replaces alloc_wave / alloc_fault / alloc_fault_coef / alloc_pml,
+ *      alloc.cu:16-508, and set_device_params, set_params.cu:39-54) ---- */
+int dfd_create(const dfd_params *p, int device, dfd_ctx **out);
+int dfd_destroy(dfd_ctx *ctx);
+int dfd_dims(const dfd_ctx *ctx, int *nx, int *ny, int *nz);
+
+/* ---- inputs (replace construct_coord coord.cu:153-328, init_media1d media.cu:63-138,
+ *      nc_read_init_stress init.cu:904-1022) ---- */
+/* fault surface x,y,z: 3 planes of (NZ, NY) float32 (Fault_geometry file) */
+int dfd_load_fault_geometry(dfd_ctx *ctx, const float *fxyz);
+/* 1-D layered medium: n rows of depth, rho, vp, vs (Media1D file) */
+int dfd_load_media1d(dfd_ctx *ctx, int n, const float *layers);
+/* 15 planes of (NZ, NY): Tx Ty Tz dTx dTy dTz mu_s mu_d Dc C0 a b L Vw State */
+int dfd_load_fault_init(dfd_ctx *ctx, const float *planes);
+
+/* ---- setup: grid, metric, media, PML and Cerjan profiles on the host in FP64, fault
+ *      and free-surface coefficient tables on the GPU in FP64 (replaces cal_metric
+ *      metric.cu:15-171, abs_init init_pml.cu:42-155, init_cerjan_host cerjan.cu:31-164,
+ *      init_fault_coef fault_coef.cu:26-1312, init_wave_free :1320-1498, init_fault
+ *      init.cu:160-849), then the CFL check of main.cu:323-345 ---- */
+int dfd_precompute(dfd_ctx *ctx);
+
+/* ---- time stepping ---- */
+/* one RK stage irk (0..3) of step it: the fused replacement of state_rk, trial_sw /
+ * trial_rs, fault2wave, wave_deriv, abs_deriv_{x,y,z}, fault_dvelo, fault_dstrs_{f,b},
+ * wave_rk, fault_rk, apply_cerjan (main.cu:448-516).  Stages must be issued in order. */
+int dfd_stage(dfd_ctx *ctx, int it, int irk);
+/* one full step (four stages, replayed from a CUDA graph per flag pattern) */
+int dfd_step(dfd_ctx *ctx, int it);
+/* nsteps steps starting at it0, without host synchronisation in between */
+int dfd_run(dfd_ctx *ctx, int it0, int nsteps);
+int dfd_synchronize(dfd_ctx *ctx);
+
+/* ---- state access ---- */
+int dfd_get_wave(dfd_ctx *ctx, float *host);        /* 9*nx*ny*nz */
+int dfd_set_wave(dfd_ctx *ctx, const float *host);  /* 9*nx*ny*nz */
+int dfd_get_metric(dfd_ctx *ctx, float *host);      /* 13*nx*ny*nz: xix..ztz jac lam mu rho */
+int dfd_get_fault(dfd_ctx *ctx, int field, float *host);
+int dfd_get_slice(dfd_ctx *ctx, int axis, int index, float *host);  /* Vx,Vy,Vz on one slice */
+/* host-side health check: 0 ok, DFD_ERR_NONFINITE if the fault state holds NaN/Inf */
+int dfd_check_finite(dfd_ctx *ctx);
+/* cumulative Newton iterations and non-converged solves of the rate-and-state trial */
+int dfd_newton_stats(dfd_ctx *ctx, long long *iterations, long long *capped);
+
+/* ---- NetCDF-classic output with the reference layout (io_fault.cu:16-285,
+ *      io_wave_xy.cu:9-188): fault_mpi000000.nc and wave_{xy,xz,yz}_mpi000000.nc ---- */
+int dfd_output_open(dfd_ctx *ctx, const char *outdir);
+int dfd_output_write(dfd_ctx *ctx, int it_skip);
+int dfd_output_close(dfd_ctx *ctx);
+
+/* ---- learned initial guess of the rate-and-state Newton solve ---- */
+/* MLP 4 -> 32 -> 32 -> 1 weights, packed W1(32x4) b1(32) W2(32x32) b2(32) W3(32) b3(1)
+ * plus 8 normalisation constants (mean, scale of the 4 inputs) = 1225 floats */
+int dfd_set_guess_net(dfd_ctx *ctx, const float *weights, int n);
+
+const char *dfd_error_string(int status);
+const char *dfd_last_error(const dfd_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,255 @@
+"""Seeded synthetic job inputs in the reference's own formats.
+
+Each case is a job dictionary with the reference's params.json keys plus the arrays
+the reference reads from its input files:
+
+  fxyz    (3, NZ, NY) float32  -- the Fault_geometry file (x, y, z of the fault surface,
+                                  coord.cu:71-151; the grid is that surface extruded in x)
+  stress  (15, NZ, NY) float32 -- the Fault_init_stress file planes
+                                  Tx,Ty,Tz,dTx,dTy,dTz,mu_s,mu_d,Dc,C0,a,b,L,Vw,State
+                                  (init.cu:904-1005)
+  layers  (n, 4) float32       -- a Media1D table depth,rho,vp,vs (media.cu:63-138)
+  wave0   (9, nx, nz, ny) f64  -- optional initial wavefield (volume-only checks)
+
+The fault-surface and stress formulas restate the reference's job scripts
+(jobs/tpv3_free_dh100m/conf_fault_grid.m:1-49, conf_fault_stress.m:42-152,
+jobs/tpv10_new/conf_fault_stress.m) in numpy; the public benchmark data they are
+compared with in the reference (SCEC TPV FEM traces) are not used anywhere.
+"""
+import json
+import os
+
+import numpy as np
+
+
+def flat_geometry(NY, NZ, DH):
+    """Planar vertical fault x=0 (conf_fault_grid.m:15-22, 0-based indices)."""
+    j = np.arange(NY)[None, :]
+    k = np.arange(NZ)[:, None]
+    x = np.zeros((NZ, NY))
+    y = (j - NY / 2) * DH + 0 * k
+    z = (k + 1 - NZ) * DH + 0 * j
+    return np.stack([x, y, z]).astype(np.float32)
+
+
+def curved_geometry(NY, NZ, DH, dip_deg=60.0, hill_amp=500.0, hill_width=5e3, nhills=2, seed=0):
+    """Dipping planar fault meshed by a curvilinear grid with Gaussian-hill topography
+    on the free surface: the surface height varies along strike (the reference grid is
+    the fault surface extruded along x, coord.cu:299-311) and is tapered linearly to a
+    flat bottom.  The dip offsets x by depth / tan(dip) (the TPV10 geometry, coord.cu:257-260)."""
+    rng = np.random.default_rng(seed)
+    j = np.arange(NY)[None, :].astype(np.float64)
+    k = np.arange(NZ)[:, None].astype(np.float64)
+    y = (j - NY / 2) * DH + 0 * k
+    top = np.zeros_like(j)
+    for _ in range(nhills):
+        yc = rng.uniform(-0.3, 0.3) * NY * DH
+        amp = hill_amp * rng.uniform(0.5, 1.0)
+        top = top + amp * np.exp(-((j - NY / 2) * DH - yc) ** 2 / hill_width ** 2)
+    depth_flat = (NZ - 1 - k) * DH  # depth below z=0 on a flat surface
+    zbot = -(NZ - 1) * DH
+    frac = k / (NZ - 1)
+    z = zbot + frac * (0 - zbot) + frac * top  # bottom flat, top follows the hills
+    depth = np.maximum(-z, 0.0)
+    x = depth / np.tan(np.deg2rad(dip_deg)) - depth_flat.mean() / np.tan(np.deg2rad(dip_deg))
+    return np.stack([x, y + 0 * k, z + 0 * j]).astype(np.float32)
+
+
+def surface_normal(fxyz, DH):
+    """Unit normal of the fault surface x(y,z) from central differences (the base
+    vector the reference's job scripts project the stress tensor on)."""
+    x, y, z = [a.astype(np.float64) for a in fxyz]
+    ty = np.stack([np.gradient(x, axis=1), np.gradient(y, axis=1), np.gradient(z, axis=1)])
+    tz = np.stack([np.gradient(x, axis=0), np.gradient(y, axis=0), np.gradient(z, axis=0)])
+    n = np.cross(ty, tz, axis=0)
+    n /= np.linalg.norm(n, axis=0, keepdims=True)
+    n *= np.sign(n[0:1])  # +x side
+    return n
+
+
+def sw_stress(fxyz, Fault_grid, tn=-120e6, ts=-70e6, patch=None, patch_ts=-81.6e6, mu_s=0.677, mu_d=0.525,
+              Dc=0.4, C0=0.0, outside_mu_s=1000.0, outside_C0=1000e6, normal=None):
+    """Slip-weakening initial traction and friction planes (conf_fault_stress.m:42-126)."""
+    _, NZ, NY = fxyz.shape
+    y, z = fxyz[1].astype(np.float64), fxyz[2].astype(np.float64)
+    n = np.zeros((3, NZ, NY)); n[0] = 1.0
+    if normal is not None:
+        n = normal
+    sxy = np.full((NZ, NY), ts)
+    if patch is not None:
+        yc, zc, hw = patch
+        inside = (np.abs(y - yc) < hw) & (np.abs(z - zc) < hw)
+        sxy[inside] = patch_ts
+    # traction = sigma . n with sigma = [[tn, sxy, 0], [sxy, 0, 0], [0, 0, 0]]
+    Tx = tn * n[0] + sxy * n[1]
+    Ty = sxy * n[0]
+    Tz = np.zeros_like(Tx)
+    out = np.zeros((15, NZ, NY))
+    out[0], out[1], out[2] = Tx, Ty, Tz
+    j1, j2, k1, k2 = Fault_grid
+    ms = np.full((NZ, NY), outside_mu_s)
+    c0 = np.full((NZ, NY), outside_C0)
+    ms[k1 - 1:k2, j1 - 1:j2] = mu_s
+    c0[k1 - 1:k2, j1 - 1:j2] = C0
+    out[6], out[7], out[8], out[9] = ms, mu_d, Dc, c0
+    return out.astype(np.float32)
+
+
+def depth_stress(fxyz, Fault_grid, grad=7378.0, ratio=0.55, normal=None, mu_s=0.76, mu_d=0.448, Dc=0.5, C0=0.2e6,
+                 patch=None):
+    """Depth-dependent stress (TPV10 style, jobs/tpv10_new/conf_fault_stress.m): normal
+    stress grad*depth, shear = ratio*normal along the dip direction, nucleation patch at
+    (mu_s+0.0057)*normal."""
+    _, NZ, NY = fxyz.shape
+    z = fxyz[2].astype(np.float64)
+    depth = np.maximum(-z, 0.5 * 100.0)
+    n = normal if normal is not None else np.stack([np.ones_like(z), 0 * z, 0 * z])
+    # dip direction: the in-plane tangent orthogonal to strike (y)
+    ey = np.stack([0 * z, np.ones_like(z), 0 * z])
+    d = np.cross(n, ey, axis=0)
+    d /= np.linalg.norm(d, axis=0, keepdims=True)
+    d *= -np.sign(d[2:3] + 1e-30)  # pointing down-dip
+    sn = -grad * depth
+    tau = ratio * np.abs(sn)
+    if patch is not None:
+        yc, zc, hw = patch
+        y = fxyz[1].astype(np.float64)
+        inside = (np.abs(y - yc) < hw) & (np.abs(z - zc) < hw)
+        tau = np.where(inside, (mu_s + 0.0057) * np.abs(sn) + 0.2e6, tau)
+    T = sn * n + tau * d
+    out = np.zeros((15, NZ, NY))
+    out[0:3] = T
+    j1, j2, k1, k2 = Fault_grid
+    ms = np.full((NZ, NY), 1000.0)
+    c0 = np.full((NZ, NY), 1000e6)
+    ms[k1 - 1:k2, j1 - 1:j2] = mu_s
+    c0[k1 - 1:k2, j1 - 1:j2] = C0
+    out[6], out[7], out[8], out[9] = ms, mu_d, Dc, c0
+    return out.astype(np.float32)
+
+
+def rs_fields(stress, fxyz, a_range=(0.01, 0.02), b=0.014, L=0.4, Vw=0.1, V0=1e-6, Vini=1e-16, seed=0,
+              normal=None, patch=None, patch_dtau=25e6):
+    """Rate-and-state planes (conf_fault_stress.m:127-152): a log-uniform per node,
+    steady-state initial state psi = a ln(2 V0/Vini sinh(|tau|/(|sigma_n| a)))."""
+    rng = np.random.default_rng(seed)
+    _, NZ, NY = fxyz.shape
+    lo, hi = np.log(a_range[0]), np.log(a_range[1])
+    a = np.exp(rng.uniform(lo, hi, size=(NZ, NY)))
+    out = stress.astype(np.float64).copy()
+    n = normal if normal is not None else np.stack([np.ones((NZ, NY)), np.zeros((NZ, NY)), np.zeros((NZ, NY))])
+    T = out[0:3]
+    tn = (T * n).sum(0)
+    ts = np.linalg.norm(T - tn * n, axis=0)
+    psi = a * np.log(2.0 * V0 / Vini * np.sinh(ts / np.abs(tn) / a))
+    out[10], out[11], out[12], out[13], out[14] = a, b, L, Vw, psi
+    if patch is not None:
+        yc, zc, hw = patch
+        y, z = fxyz[1].astype(np.float64), fxyz[2].astype(np.float64)
+        r = np.sqrt((y - yc) ** 2 + (z - zc) ** 2)
+        with np.errstate(over="ignore", divide="ignore"):
+            F = np.where(r < hw, np.exp(np.minimum(r ** 2 / (r ** 2 - hw ** 2 + 1e-30), 0.0)), 0.0)
+        sdir = (T - tn * n) / np.maximum(ts, 1.0)
+        out[3:6] = patch_dtau * F * sdir
+    return out.astype(np.float32)
+
+
+def smooth_wave(NX, NY, NZ, seed=0, amp=1e5):
+    """Seeded smooth initial wavefield with zero ghost layers (9, nx, nz, ny)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = NX + 6, NY + 6, NZ + 6
+    W = np.zeros((9, nx, nz, ny))
+    i = np.arange(nx)[:, None, None]
+    k = np.arange(nz)[None, :, None]
+    j = np.arange(ny)[None, None, :]
+    for f in range(9):
+        ci, cj, ck = rng.uniform(0.3, 0.7, 3) * np.array([nx, ny, nz])
+        w = rng.uniform(2.0, 4.0)
+        scale = amp if f >= 3 else amp * 1e-6
+        W[f] = scale * np.exp(-((i - ci) ** 2 + (j - cj) ** 2 + (k - ck) ** 2) / (2 * w * w))
+    W[:, :3] = 0; W[:, -3:] = 0
+    W[:, :, :3] = 0; W[:, :, -3:] = 0
+    W[:, :, :, :3] = 0; W[:, :, :, -3:] = 0
+    return W
+
+
+def get_case(name):
+    """Return (params, fxyz, stress, layers, wave0, meta) for a named case."""
+    if name == "vol_small":
+        p = dict(NX=20, NY=22, NZ=18, DH=100.0, DT=0.004, TMAX=0.05, PML_N=5, PML_velocity=6000.0,
+                 INPORT_GRID_TYPE=0)
+        return p, None, None, None, smooth_wave(20, 22, 18, seed=1), dict(steps=12, every=4, volume=True)
+    if name == "vol_curved":
+        p = dict(NX=20, NY=24, NZ=18, DH=100.0, DT=0.004, TMAX=0.05, PML_N=5, PML_velocity=6000.0,
+                 INPORT_GRID_TYPE=1, bi_vp2=5000.0, bi_vs2=2900.0, bi_rho2=2500.0)
+        fx = curved_geometry(24, 18, 100.0, hill_amp=300.0, hill_width=600.0, seed=3)
+        return p, fx, None, None, smooth_wave(20, 24, 18, seed=2), dict(steps=12, every=4, volume=True)
+    if name in ("sw_flat", "sw_flat_nr"):
+        NX, NY, NZ, DH = 24, 76, 40, 100.0
+        fg = [21, 56, 21, 40]
+        p = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.008, TMAX=0.4, PML_N=6, PML_velocity=6000.0,
+                 INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=0, Fault_grid=fg,
+                 mu_s=0.677, mu_d=0.525, Dc=0.4, C0=0.0, NormalRefine=1 if name == "sw_flat" else 0)
+        fx = flat_geometry(NY, NZ, DH)
+        st = sw_stress(fx, fg, patch=(0.0, -500.0, 450.0), patch_ts=-95e6, Dc=0.05, mu_d=0.525)
+        return p, fx, st, None, None, dict(steps=60, every=20, volume=False)
+    if name == "sw_curved":
+        NX, NY, NZ, DH = 24, 76, 40, 100.0
+        fg = [21, 56, 21, 40]
+        p = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.006, TMAX=0.3, PML_N=6, PML_velocity=6000.0,
+                 INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=0, Fault_grid=fg,
+                 mu_s=0.76, mu_d=0.448, Dc=0.05, C0=0.2e6)
+        fx = curved_geometry(NY, NZ, DH, hill_amp=200.0, hill_width=800.0, seed=5)
+        n = surface_normal(fx, DH)
+        st = depth_stress(fx, fg, normal=n, Dc=0.05, patch=(0.0, -500.0, 450.0))
+        return p, fx, st, None, None, dict(steps=50, every=25, volume=False)
+    if name == "rs_flat":
+        NX, NY, NZ, DH = 24, 76, 40, 100.0
+        fg = [21, 56, 21, 40]
+        p = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.008, TMAX=0.32, PML_N=6, PML_velocity=6000.0,
+                 INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=2, Fault_grid=fg,
+                 RS_V0=1e-6, RS_f0=0.6, RS_fw=0.2, RS_Vini=1e-16, RS_L=0.4, smooth_load_T=0.1)
+        fx = flat_geometry(NY, NZ, DH)
+        st = sw_stress(fx, fg, tn=-120e6, ts=-40e6)
+        st = rs_fields(st, fx, seed=7, L=0.02, patch=(0.0, -500.0, 600.0), patch_dtau=45e6)
+        return p, fx, st, None, None, dict(steps=40, every=20, volume=False)
+    raise KeyError(name)
+
+
+CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat"]
+
+
+def write_inputs(name, outdir):
+    """Write params.json, Fault_geometry / Fault_init_stress NetCDF-classic files and the
+    optional initial wavefield for the reference harness."""
+    from scipy.io import netcdf_file
+
+    p, fx, st, layers, w0, meta = get_case(name)
+    os.makedirs(outdir, exist_ok=True)
+    job = dict(p)
+    job["OUT"] = outdir
+    job["PX"] = job["PY"] = job["PZ"] = 1
+    if fx is not None:
+        fn = os.path.join(outdir, "fault_coord.nc")
+        with netcdf_file(fn, "w") as f:
+            f.createDimension("nz", fx.shape[1])
+            f.createDimension("ny", fx.shape[2])
+            for c, nm in enumerate("xyz"):
+                v = f.createVariable(nm, "f4", ("nz", "ny"))
+                v[:] = fx[c]
+        job["Fault_geometry"] = fn
+    if st is not None:
+        fn = os.path.join(outdir, "init_stress.nc")
+        names = ["Tx", "Ty", "Tz", "dTx", "dTy", "dTz", "mu_s", "mu_d", "Dc", "C0", "a", "b", "L", "Vw", "State"]
+        with netcdf_file(fn, "w") as f:
+            f.createDimension("nz", st.shape[1])
+            f.createDimension("ny", st.shape[2])
+            for c, nm in enumerate(names):
+                v = f.createVariable(nm, "f4", ("nz", "ny"))
+                v[:] = st[c]
+        job["Fault_init_stress"] = fn
+    with open(os.path.join(outdir, "params.json"), "w") as f:
+        json.dump(job, f, indent=1)
+    if w0 is not None:
+        w0.astype(np.float64).tofile(os.path.join(outdir, "wave0.f64"))
+    return job, meta
