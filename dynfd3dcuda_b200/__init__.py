@@ -1,0 +1,230 @@
+"""B200-native curved-grid finite-difference dynamic-rupture time step.
+
+Python mirror of the C ABI in include/dfd_b200.h (libdfd_b200.so, built in-tree by
+dynfd3dcuda_b200/build.py).  The job dictionary uses the reference's params.json keys
+(set_params.cu:137-282); input arrays use the reference's file layouts:
+
+    fxyz    (3, NZ, NY) float32   Fault_geometry x, y, z
+    stress  (15, NZ, NY) float32  Fault_init_stress Tx Ty Tz dTx dTy dTz mu_s mu_d Dc C0 a b L Vw State
+    layers  (n, 4) float32        Media1D rows depth rho vp vs
+
+There is no CPU fallback: constructing a Simulation without the CUDA library or without
+a GPU raises.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libdfd_b200.so")
+_lib = None
+
+FIELDS = ["slip", "hslip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State", "init_t0", "tTn", "tTs1", "tTs2",
+          "str_peak", "friction", "united", "faultgrid", "split", "T1", "hT1"]
+STATUS = {0: "ok", 1: "bad or unsupported parameter", 2: "CUDA error", 3: "file missing or malformed",
+          4: "call out of order", 5: "DT above the stability limit", 6: "non-finite fault state",
+          7: "Newton solve hit its iteration cap"}
+
+
+class DfdError(RuntimeError):
+    def __init__(self, status, msg=""):
+        super().__init__(f"{STATUS.get(status, status)}{': ' + msg if msg else ''}")
+        self.status = status
+
+
+class DfdParams(ctypes.Structure):
+    _fields_ = [
+        ("NX", ctypes.c_int), ("NY", ctypes.c_int), ("NZ", ctypes.c_int), ("NT", ctypes.c_int),
+        ("TMAX", ctypes.c_double), ("DT", ctypes.c_double), ("DH", ctypes.c_double),
+        ("INPORT_GRID_TYPE", ctypes.c_int), ("INPORT_STRESS_TYPE", ctypes.c_int), ("Friction_type", ctypes.c_int),
+        ("EXPORT_TIME_SKIP", ctypes.c_int), ("EXPORT_WAVE_SLICE_X", ctypes.c_int),
+        ("EXPORT_WAVE_SLICE_Y", ctypes.c_int), ("EXPORT_WAVE_SLICE_Z", ctypes.c_int),
+        ("PML_N", ctypes.c_int), ("PML_velocity", ctypes.c_double), ("PML_bmax", ctypes.c_double),
+        ("PML_fc", ctypes.c_double), ("DAMP_N", ctypes.c_int),
+        ("mu_s", ctypes.c_double), ("mu_d", ctypes.c_double), ("mu_0", ctypes.c_double), ("Dc", ctypes.c_double),
+        ("C0", ctypes.c_double), ("f0", ctypes.c_double), ("V0", ctypes.c_double), ("Vini", ctypes.c_double),
+        ("fw", ctypes.c_double), ("L", ctypes.c_double), ("smooth_load_T", ctypes.c_double),
+        ("viscosity", ctypes.c_double), ("Fault_grid", ctypes.c_int * 4), ("Asp_grid", ctypes.c_int * 4),
+        ("bi_vp1", ctypes.c_double), ("bi_vs1", ctypes.c_double), ("bi_rho1", ctypes.c_double),
+        ("bi_vp2", ctypes.c_double), ("bi_vs2", ctypes.c_double), ("bi_rho2", ctypes.c_double),
+        ("rupture", ctypes.c_int), ("free_surface", ctypes.c_int), ("use_pml", ctypes.c_int),
+        ("use_cerjan", ctypes.c_int), ("normal_refine", ctypes.c_int), ("rs_guess", ctypes.c_int),
+        ("OUT", ctypes.c_char * 1024), ("Fault_geometry", ctypes.c_char * 1024),
+        ("Fault_init_stress", ctypes.c_char * 1024), ("Media1D", ctypes.c_char * 1024),
+    ]
+
+
+# job-file key -> struct field, for keys whose names differ (set_params.cu:137-282 plus the
+# reference's compile-time switches as job keys)
+_KEYMAP = {"RS_V0": "V0", "RS_Vini": "Vini", "RS_f0": "f0", "RS_fw": "fw", "RS_L": "L", "rho1": "bi_rho1",
+           "Rupture": "rupture", "FreeSurface": "free_surface", "usePML": "use_pml", "useCerjan": "use_cerjan",
+           "NormalRefine": "normal_refine", "RS_guess": "rs_guess"}
+
+
+def lib():
+    """Load libdfd_b200.so (built in-tree); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError(f"{LIBPATH} is missing: build it with `python -m dynfd3dcuda_b200.build`")
+        L = ctypes.CDLL(LIBPATH)
+        P, I, V = ctypes.POINTER, ctypes.c_int, ctypes.c_void_p
+        sigs = {
+            "dfd_params_default": [P(DfdParams)], "dfd_params_load_json": [ctypes.c_char_p, P(DfdParams)],
+            "dfd_create": [P(DfdParams), I, P(V)], "dfd_destroy": [V], "dfd_dims": [V, P(I), P(I), P(I)],
+            "dfd_load_fault_geometry": [V, V], "dfd_load_media1d": [V, I, V], "dfd_load_fault_init": [V, V],
+            "dfd_precompute": [V], "dfd_stage": [V, I, I], "dfd_step": [V, I], "dfd_run": [V, I, I],
+            "dfd_synchronize": [V], "dfd_get_wave": [V, V], "dfd_set_wave": [V, V], "dfd_get_metric": [V, V],
+            "dfd_get_fault": [V, I, V], "dfd_get_slice": [V, I, I, V], "dfd_check_finite": [V],
+            "dfd_newton_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong)],
+            "dfd_output_open": [V, ctypes.c_char_p], "dfd_output_write": [V, I], "dfd_output_close": [V],
+            "dfd_set_guess_net": [V, V, I],
+        }
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.dfd_error_string.restype = ctypes.c_char_p
+        L.dfd_error_string.argtypes = [I]
+        L.dfd_last_error.restype = ctypes.c_char_p
+        L.dfd_last_error.argtypes = [V]
+        _lib = L
+    return _lib
+
+
+def params_struct(job):
+    """Reference job dictionary (params.json keys) -> dfd_params, with the reference defaults."""
+    L = lib()
+    s = DfdParams()
+    L.dfd_params_default(ctypes.byref(s))
+    for key, val in job.items():
+        name = _KEYMAP.get(key, key)
+        if name in ("Fault_grid", "Asp_grid"):
+            arr = getattr(s, name)
+            for i in range(4):
+                arr[i] = int(val[i])
+        elif name in ("OUT", "Fault_geometry", "Fault_init_stress", "Media1D"):
+            setattr(s, name, str(val).encode()[:1023])
+        elif any(name == f[0] for f in DfdParams._fields_):
+            cur = getattr(s, name)
+            setattr(s, name, int(val) if isinstance(cur, int) else float(val))
+    s.NT = int(float(np.float32(s.TMAX)) / float(np.float32(s.DT)))
+    return s
+
+
+class Simulation:
+    """One rupture simulation resident on one GPU (a dfd_ctx)."""
+
+    def __init__(self, job, fxyz=None, stress=None, layers=None, device=0, precompute=True):
+        if isinstance(job, str):
+            with open(job) as f:
+                job = json.load(f)
+        self.job = dict(job)
+        self.p = params_struct(self.job)
+        L = lib()
+        h = ctypes.c_void_p()
+        self._check(L.dfd_create(ctypes.byref(self.p), device, ctypes.byref(h)))
+        self.h = h
+        nx, ny, nz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        L.dfd_dims(self.h, ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz))
+        self.nx, self.ny, self.nz = nx.value, ny.value, nz.value
+        self.NX, self.NY, self.NZ = self.p.NX, self.p.NY, self.p.NZ
+        if fxyz is not None:
+            a = np.ascontiguousarray(fxyz, np.float32)
+            self._check(L.dfd_load_fault_geometry(self.h, a.ctypes.data))
+        if stress is not None:
+            a = np.ascontiguousarray(stress, np.float32)
+            self._check(L.dfd_load_fault_init(self.h, a.ctypes.data))
+        if layers is not None:
+            a = np.ascontiguousarray(layers, np.float32)
+            self._check(L.dfd_load_media1d(self.h, a.shape[0], a.ctypes.data))
+        if precompute:
+            self.precompute()
+
+    def _check(self, r):
+        if r:
+            msg = ""
+            if getattr(self, "h", None):
+                msg = (lib().dfd_last_error(self.h) or b"").decode()
+            raise DfdError(r, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def precompute(self):
+        self._check(lib().dfd_precompute(self.h))
+
+    def stage(self, it, irk):
+        self._check(lib().dfd_stage(self.h, it, irk))
+
+    def step(self, it):
+        self._check(lib().dfd_step(self.h, it))
+
+    def run(self, it0, nsteps):
+        self._check(lib().dfd_run(self.h, it0, nsteps))
+
+    def synchronize(self):
+        self._check(lib().dfd_synchronize(self.h))
+
+    def wave(self):
+        out = np.empty((9, self.nx, self.nz, self.ny), np.float32)
+        self._check(lib().dfd_get_wave(self.h, out.ctypes.data))
+        return out
+
+    def set_wave(self, w):
+        a = np.ascontiguousarray(w, np.float32)
+        assert a.size == 9 * self.nx * self.ny * self.nz
+        self._check(lib().dfd_set_wave(self.h, a.ctypes.data))
+
+    def metric(self):
+        out = np.empty((13, self.nx, self.nz, self.ny), np.float32)
+        self._check(lib().dfd_get_metric(self.h, out.ctypes.data))
+        return out
+
+    def fault(self, name):
+        f = FIELDS.index(name)
+        if name == "split":
+            out = np.empty((9, 2, self.nz, self.ny), np.float32)
+        elif name == "T1":
+            out = np.empty((3, 7, self.nz, self.ny), np.float32)
+        elif name == "hT1":
+            out = np.empty((3, self.nz, self.ny), np.float32)
+        else:
+            out = np.empty((self.NZ, self.NY), np.float32)
+        self._check(lib().dfd_get_fault(self.h, f, out.ctypes.data))
+        return out
+
+    def slice(self, axis, index):
+        na = self.NZ if axis == 0 else self.NX
+        nb = self.NZ if axis == 1 else self.NY
+        out = np.empty((3, na, nb), np.float32)
+        self._check(lib().dfd_get_slice(self.h, axis, index, out.ctypes.data))
+        return out
+
+    def check_finite(self):
+        self._check(lib().dfd_check_finite(self.h))
+
+    def newton_stats(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(lib().dfd_newton_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def set_guess_net(self, w):
+        a = np.ascontiguousarray(w, np.float32).ravel()
+        self._check(lib().dfd_set_guess_net(self.h, a.ctypes.data, a.size))
+
+    def output_open(self, outdir):
+        self._check(lib().dfd_output_open(self.h, outdir.encode()))
+
+    def output_write(self, it_skip):
+        self._check(lib().dfd_output_write(self.h, it_skip))
+
+    def output_close(self):
+        self._check(lib().dfd_output_close(self.h))

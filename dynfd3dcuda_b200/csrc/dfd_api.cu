@@ -1,0 +1,775 @@
+// C ABI of the B200 dynamic-rupture time step: context (device memory owner), setup,
+// stage sequencing with a side stream for the fault band, CUDA-graph replay of whole
+// steps, state access and NetCDF output.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dfd_host.h"
+#include "dfd_internal.cuh"
+
+namespace dfd {
+void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s);
+void launch_fault_node(const FaultArgs& a, cudaStream_t s);
+void launch_fault_band(const FaultArgs& a, cudaStream_t s);
+void launch_fault_coef(const Dims& d, const float* M, float* tab, float* tabf, float* vecn, float* vecs1,
+                       float* vecs2, float* rhof, cudaStream_t s);
+void launch_wave_free(const Dims& d, const float* M, const float* Bx, const float* By, const float* Bz, float* mx,
+                      float* my, cudaStream_t s);
+void launch_metric(const GridArgs& g, float* M, cudaStream_t s);
+void launch_cfl(const GridArgs& g, const float* M, float* hmin, float* vpmax, cudaStream_t s);
+
+__global__ void set_it_kernel(int* it, int v) { *it = v; }
+__global__ void inc_it_kernel(int* it) { *it += 1; }
+__global__ void nonfinite_kernel(const float* a, long long n, int* flag) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (!isfinite(a[i])) *flag = 1;
+}
+// (nx, nz, ny) field -> (a, b) slice gathers of Vx, Vy, Vz (get_wave_slice_*, io_wave_*.cu)
+__global__ void slice_kernel(Dims d, const float* W, int axis, int index, float* out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int na = axis == 0 ? d.nk : d.ni, nb = axis == 1 ? d.nk : d.nj;
+  if (t >= na * nb) return;
+  int a = t / nb, b = t % nb, i, j, k;
+  if (axis == 0) { i = index; k = a; j = b; }
+  else if (axis == 1) { j = index; i = a; k = b; }
+  else { k = index; i = a; j = b; }
+  long long q = idx3(d, i + 3, j + 3, k + 3);
+  for (int c = 0; c < 3; c++) out[(long long)c * na * nb + t] = W[c * d.nxyz + q];
+}
+}  // namespace dfd
+
+using namespace dfd;
+
+// fault 2-D planes held in one allocation
+enum Plane {
+  P_SLIP, P_MSLIP, P_TSLIP, P_HSLIP, P_STATE, P_MSTATE, P_TSTATE, P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_TTN, P_TTS1,
+  P_TTS2, P_SX, P_SY, P_SZ, P_T0X, P_T0Y, P_T0Z, P_DT0X, P_DT0Y, P_DT0Z, P_PEAK, P_DC, P_C0, P_A, P_B, P_L, P_VW,
+  P_T0, P_FRIC, NPLANE
+};
+enum IPlane { I_T0FLAG, I_FLAGRUP, I_UNITED, I_FAULTGRID, I_RUPY, I_RUPZ, NIPLANE };
+
+struct dfd_ctx {
+  dfd_params p;
+  Dims d;
+  int device = 0;
+  cudaStream_t s0 = nullptr, s1 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  std::vector<void*> allocs;
+  float* W[4] = {};
+  float* M = nullptr;
+  float *rB[3] = {}, *B[3] = {}, *Dp[3] = {}, *Ap[3] = {};
+  float* aux[6][3] = {};
+  float *mVx2Vz = nullptr, *mVy2Vz = nullptr;
+  float* damp[3] = {};
+  float *FW[2] = {}, *Fm = nullptr, *Ft = nullptr, *T1 = nullptr, *mT1 = nullptr, *hT1 = nullptr;
+  float *tab = nullptr, *tabf = nullptr, *vecn = nullptr, *vecs1 = nullptr, *vecs2 = nullptr, *rhof = nullptr;
+  float* pl = nullptr;
+  int* ipl = nullptr;
+  unsigned long long* newton = nullptr;
+  int* it_dev = nullptr;
+  int* flag_dev = nullptr;
+  float* guess_net = nullptr;
+  // host-side inputs
+  std::vector<float> fxyz, planes, layers;
+  std::vector<double> xl, fx, fy, fz;
+  bool ready = false;
+  int next_stage = 0;
+  std::string err;
+  int sticky = DFD_OK;
+  cudaGraphExec_t graph[8] = {};
+  // output
+  NcWriter ncf, ncw[3];
+  int vf[16] = {}, vw[3][3] = {};
+  bool out_open = false;
+};
+
+static int fail(dfd_ctx* c, int code, const std::string& m) {
+  if (c) { c->err = m; if (code == DFD_ERR_CUDA) c->sticky = code; }
+  return code;
+}
+static int cuda_check(dfd_ctx* c, cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return DFD_OK;
+  return fail(c, DFD_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                                     \
+  do {                                                               \
+    int _r = cuda_check(ctx, (call), #call);                         \
+    if (_r) return _r;                                               \
+  } while (0)
+
+template <typename T>
+static int dalloc(dfd_ctx* ctx, T** p, size_t n) {
+  void* v = nullptr;
+  cudaError_t e = cudaMalloc(&v, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "cudaMalloc");
+  ctx->allocs.push_back(v);
+  cudaMemset(v, 0, n * sizeof(T) + 16);
+  *p = (T*)v;
+  return DFD_OK;
+}
+
+extern "C" {
+
+const char* dfd_error_string(int s) {
+  switch (s) {
+    case DFD_OK: return "ok";
+    case DFD_ERR_PARAM: return "bad or unsupported parameter";
+    case DFD_ERR_CUDA: return "CUDA error";
+    case DFD_ERR_IO: return "file missing or malformed";
+    case DFD_ERR_STATE: return "call out of order";
+    case DFD_ERR_CFL: return "DT above the stability limit";
+    case DFD_ERR_NONFINITE: return "non-finite fault state";
+    case DFD_ERR_NEWTON: return "Newton solve hit its iteration cap";
+  }
+  return "unknown status";
+}
+const char* dfd_last_error(const dfd_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int dfd_params_size(void) { return (int)sizeof(dfd_params); }
+
+int dfd_params_default(dfd_params* p) {
+  if (!p) return DFD_ERR_PARAM;
+  params_default(p);
+  return DFD_OK;
+}
+
+int dfd_params_load_json(const char* path, dfd_params* p) {
+  if (!path || !p) return DFD_ERR_PARAM;
+  FILE* f = fopen(path, "rb");
+  if (!f) return DFD_ERR_IO;
+  std::string text;
+  char buf[4096];
+  size_t n;
+  while ((n = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, n);
+  fclose(f);
+  params_default(p);
+  return params_from_json(text.c_str(), p, nullptr);
+}
+
+int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
+  if (!p || !out) return DFD_ERR_PARAM;
+  *out = nullptr;
+  std::string e;
+  dfd_params q = *p;
+  finalize_params(&q);
+  int r = check_params(&q, &e);
+  if (r) { fprintf(stderr, "dfd_create: %s\n", e.c_str()); return r; }
+  dfd_ctx* ctx = new dfd_ctx();
+  ctx->p = q;
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return DFD_ERR_CUDA; }
+  Dims& d = ctx->d;
+  d.ni = q.NX; d.nj = q.NY; d.nk = q.NZ;
+  d.nx = q.NX + 6; d.ny = q.NY + 6; d.nz = q.NZ + 6;
+  d.i0 = d.nx / 2;
+  d.N = q.PML_N;
+  d.nxyz = (long long)d.nx * d.ny * d.nz;
+  d.nyz = (long long)d.ny * d.nz;
+  auto done = [&](int rc) { if (rc) { dfd_destroy(ctx); return rc; } return 0; };
+  if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s0, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
+  if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s1, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
+  cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+  int rc = 0;
+  for (int b = 0; b < 4 && !rc; b++) rc = dalloc(ctx, &ctx->W[b], 9 * d.nxyz);
+  if (!rc) rc = dalloc(ctx, &ctx->M, 13 * d.nxyz);
+  int len[3] = {d.ni, d.nj, d.nk};
+  for (int a = 0; a < 3 && !rc; a++) {
+    rc = dalloc(ctx, &ctx->rB[a], len[a]);
+    if (!rc) rc = dalloc(ctx, &ctx->B[a], len[a]);
+    if (!rc) rc = dalloc(ctx, &ctx->Dp[a], len[a]);
+    if (!rc) rc = dalloc(ctx, &ctx->Ap[a], len[a]);
+  }
+  if (!rc && q.use_pml) {
+    long long sz[6] = {(long long)d.N * d.nj * d.nk, (long long)d.N * d.nj * d.nk, (long long)d.N * d.nk * d.ni,
+                       (long long)d.N * d.nk * d.ni, (long long)d.N * d.ni * d.nj, (long long)d.N * d.ni * d.nj};
+    for (int f = 0; f < 6 && !rc; f++) {
+      if (f == 5 && q.free_surface) continue;
+      for (int r3 = 0; r3 < 3 && !rc; r3++) rc = dalloc(ctx, &ctx->aux[f][r3], 9 * sz[f]);
+    }
+  }
+  if (!rc) rc = dalloc(ctx, &ctx->mVx2Vz, 9LL * d.nx * d.ny);
+  if (!rc) rc = dalloc(ctx, &ctx->mVy2Vz, 9LL * d.nx * d.ny);
+  if (!rc && q.use_cerjan) {
+    rc = dalloc(ctx, &ctx->damp[0], d.nx);
+    if (!rc) rc = dalloc(ctx, &ctx->damp[1], d.ny);
+    if (!rc) rc = dalloc(ctx, &ctx->damp[2], d.nz);
+  }
+  if (!rc && q.rupture) {
+    for (int b = 0; b < 2 && !rc; b++) rc = dalloc(ctx, &ctx->FW[b], 18 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->Fm, 18 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->Ft, 18 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->T1, 21 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->mT1, 3 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->hT1, 3 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->tab, (long long)NTAB9 * 9 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->tabf, (long long)NTABF * 9 * d.ny);
+    if (!rc) rc = dalloc(ctx, &ctx->vecn, 3 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->vecs1, 3 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->vecs2, 3 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->rhof, 2 * d.nyz);
+    if (!rc) rc = dalloc(ctx, &ctx->pl, (long long)NPLANE * d.nj * d.nk);
+    if (!rc) rc = dalloc(ctx, &ctx->ipl, (long long)NIPLANE * d.nj * d.nk);
+  }
+  if (!rc) rc = dalloc(ctx, &ctx->newton, 2);
+  if (!rc) rc = dalloc(ctx, &ctx->it_dev, 1);
+  if (!rc) rc = dalloc(ctx, &ctx->flag_dev, 1);
+  if (!rc) rc = dalloc(ctx, &ctx->guess_net, 1232);
+  if (rc) { dfd_destroy(ctx); return rc; }
+  *out = ctx;
+  return DFD_OK;
+}
+
+int dfd_destroy(dfd_ctx* ctx) {
+  if (!ctx) return DFD_OK;
+  cudaSetDevice(ctx->device);
+  dfd_output_close(ctx);
+  for (auto& g : ctx->graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (ctx->s0) cudaStreamSynchronize(ctx->s0);
+  if (ctx->s1) cudaStreamSynchronize(ctx->s1);
+  for (void* v : ctx->allocs) cudaFree(v);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->s0) cudaStreamDestroy(ctx->s0);
+  if (ctx->s1) cudaStreamDestroy(ctx->s1);
+  delete ctx;
+  return DFD_OK;
+}
+
+int dfd_dims(const dfd_ctx* ctx, int* nx, int* ny, int* nz) {
+  if (!ctx) return DFD_ERR_PARAM;
+  if (nx) *nx = ctx->d.nx;
+  if (ny) *ny = ctx->d.ny;
+  if (nz) *nz = ctx->d.nz;
+  return DFD_OK;
+}
+
+int dfd_load_fault_geometry(dfd_ctx* ctx, const float* fxyz) {
+  if (!ctx || !fxyz) return DFD_ERR_PARAM;
+  size_t n = 3ull * ctx->p.NY * ctx->p.NZ;
+  ctx->fxyz.assign(fxyz, fxyz + n);
+  ctx->ready = false;
+  return DFD_OK;
+}
+int dfd_load_media1d(dfd_ctx* ctx, int n, const float* layers) {
+  if (!ctx || n < 0 || (n > 0 && !layers)) return DFD_ERR_PARAM;
+  ctx->layers.assign(layers, layers + 4 * (size_t)n);
+  ctx->ready = false;
+  return DFD_OK;
+}
+int dfd_load_fault_init(dfd_ctx* ctx, const float* planes) {
+  if (!ctx || !planes) return DFD_ERR_PARAM;
+  size_t n = 15ull * ctx->p.NY * ctx->p.NZ;
+  ctx->planes.assign(planes, planes + n);
+  ctx->ready = false;
+  return DFD_OK;
+}
+
+int dfd_precompute(dfd_ctx* ctx) {
+  if (!ctx) return DFD_ERR_PARAM;
+  if (ctx->sticky) return ctx->sticky;
+  cudaSetDevice(ctx->device);
+  const dfd_params& p = ctx->p;
+  const Dims& d = ctx->d;
+  cudaStream_t s = ctx->s0;
+  if (p.INPORT_GRID_TYPE == 1 && ctx->fxyz.empty())
+    return fail(ctx, DFD_ERR_STATE, "INPORT_GRID_TYPE=1 needs dfd_load_fault_geometry");
+  if (p.rupture && p.INPORT_STRESS_TYPE != 1)
+    return fail(ctx, DFD_ERR_PARAM, "rupture runs need INPORT_STRESS_TYPE=1 and dfd_load_fault_init");
+  if (p.rupture && ctx->planes.empty()) return fail(ctx, DFD_ERR_STATE, "missing dfd_load_fault_init");
+  // ---- grid, metric, media (FP64 on the GPU)
+  x_line(&p, ctx->xl);
+  surface(&p, ctx->fxyz.empty() ? nullptr : ctx->fxyz.data(), ctx->fx, ctx->fy, ctx->fz);
+  double *dxl, *dfx, *dfy, *dfz;
+  float* dlay = nullptr;
+  CK(cudaMalloc(&dxl, sizeof(double) * ctx->xl.size()));
+  CK(cudaMalloc(&dfx, sizeof(double) * ctx->fx.size()));
+  CK(cudaMalloc(&dfy, sizeof(double) * ctx->fy.size()));
+  CK(cudaMalloc(&dfz, sizeof(double) * ctx->fz.size()));
+  CK(cudaMemcpy(dxl, ctx->xl.data(), sizeof(double) * ctx->xl.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfx, ctx->fx.data(), sizeof(double) * ctx->fx.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfy, ctx->fy.data(), sizeof(double) * ctx->fy.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfz, ctx->fz.data(), sizeof(double) * ctx->fz.size(), cudaMemcpyHostToDevice));
+  if (!ctx->layers.empty()) {
+    CK(cudaMalloc(&dlay, sizeof(float) * ctx->layers.size()));
+    CK(cudaMemcpy(dlay, ctx->layers.data(), sizeof(float) * ctx->layers.size(), cudaMemcpyHostToDevice));
+  }
+  GridArgs g;
+  g.d = d; g.xl = dxl; g.fx = dfx; g.fy = dfy; g.fz = dfz; g.layers = dlay;
+  g.nlayer = (int)(ctx->layers.size() / 4);
+  g.NXhalf = p.NX / 2;
+  g.rDH = 1.0 / p.DH;
+  g.lam1 = p.bi_rho1 * (p.bi_vp1 * p.bi_vp1 - 2 * p.bi_vs1 * p.bi_vs1);
+  g.mu1 = p.bi_rho1 * p.bi_vs1 * p.bi_vs1;
+  g.rho1 = p.bi_rho1;
+  g.lam2 = p.bi_rho2 * (p.bi_vp2 * p.bi_vp2 - 2 * p.bi_vs2 * p.bi_vs2);
+  g.mu2 = p.bi_rho2 * p.bi_vs2 * p.bi_vs2;
+  g.rho2 = p.bi_rho2;
+  launch_metric(g, ctx->M, s);
+  CK(cudaGetLastError());
+  // CFL check (main.cu:323-345)
+  size_t ncol = (size_t)d.nj * d.nk;
+  float *dh, *dv;
+  CK(cudaMalloc(&dh, sizeof(float) * ncol));
+  CK(cudaMalloc(&dv, sizeof(float) * ncol));
+  launch_cfl(g, ctx->M, dh, dv, s);
+  CK(cudaGetLastError());
+  std::vector<float> hh(ncol), hv(ncol);
+  CK(cudaMemcpyAsync(hh.data(), dh, sizeof(float) * ncol, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hv.data(), dv, sizeof(float) * ncol, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  cudaFree(dh); cudaFree(dv); cudaFree(dxl); cudaFree(dfx); cudaFree(dfy); cudaFree(dfz);
+  if (dlay) cudaFree(dlay);
+  float hmin = 1e38f, vpmax = 0.0f;
+  for (size_t i = 0; i < ncol; i++) { hmin = fminf(hmin, hh[i]); vpmax = fmaxf(vpmax, hv[i]); }
+  float dtmax = 1.3f * hmin / vpmax;
+  if (!(p.DT < dtmax)) {
+    char m[160];
+    snprintf(m, sizeof m, "DT = %g >= dtmax = %g (hmin %g m, vpmax %g m/s)", p.DT, dtmax, hmin, vpmax);
+    return fail(ctx, DFD_ERR_CFL, m);
+  }
+  // ---- PML 1-D profiles
+  bool fs = p.free_surface != 0;
+  int len[3] = {d.ni, d.nj, d.nk};
+  for (int a = 0; a < 3; a++) {
+    std::vector<float> A, B, D, rb;
+    bool lo = p.use_pml != 0, hi = p.use_pml && !(a == 2 && fs);
+    pml_profile(&p, len[a], lo, hi, A, B, D);
+    rb.resize(B.size());
+    for (size_t i = 0; i < B.size(); i++) rb[i] = 1.0f / B[i];
+    CK(cudaMemcpy(ctx->Ap[a], A.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->B[a], B.data(), sizeof(float) * B.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->Dp[a], D.data(), sizeof(float) * D.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->rB[a], rb.data(), sizeof(float) * rb.size(), cudaMemcpyHostToDevice));
+  }
+  if (p.use_cerjan) {
+    int np[3] = {d.nx, d.ny, d.nz};
+    for (int a = 0; a < 3; a++) {
+      std::vector<float> prof;
+      cerjan_profile(&p, np[a], true, !(a == 2 && fs), prof);
+      CK(cudaMemcpy(ctx->damp[a], prof.data(), sizeof(float) * prof.size(), cudaMemcpyHostToDevice));
+    }
+  }
+  if (fs) launch_wave_free(d, ctx->M, ctx->B[0], ctx->B[1], ctx->B[2], ctx->mVx2Vz, ctx->mVy2Vz, s);
+  // ---- fault tables and initial state
+  size_t nf = (size_t)d.nj * d.nk;
+  if (p.rupture) {
+    launch_fault_coef(d, ctx->M, ctx->tab, ctx->tabf, ctx->vecn, ctx->vecs1, ctx->vecs2, ctx->rhof, s);
+    CK(cudaGetLastError());
+    std::vector<float> vn(3 * d.nyz), v1(3 * d.nyz), v2(3 * d.nyz);
+    CK(cudaMemcpyAsync(vn.data(), ctx->vecn, sizeof(float) * vn.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(v1.data(), ctx->vecs1, sizeof(float) * v1.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(v2.data(), ctx->vecs2, sizeof(float) * v2.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    FaultHost h;
+    fault_init(&p, ctx->planes.data(), vn.data(), v1.data(), v2.data(), h);
+    CK(cudaMemsetAsync(ctx->pl, 0, sizeof(float) * NPLANE * nf, s));
+    CK(cudaMemsetAsync(ctx->ipl, 0, sizeof(int) * NIPLANE * nf, s));
+    struct { int plane; std::vector<float>* v; } up[] = {
+        {P_SX, &h.sx}, {P_SY, &h.sy}, {P_SZ, &h.sz}, {P_T0X, &h.T0x}, {P_T0Y, &h.T0y}, {P_T0Z, &h.T0z},
+        {P_DT0X, &h.dT0x}, {P_DT0Y, &h.dT0y}, {P_DT0Z, &h.dT0z}, {P_PEAK, &h.str_peak}, {P_DC, &h.Dc},
+        {P_C0, &h.C0}, {P_A, &h.a}, {P_B, &h.b}, {P_L, &h.L}, {P_VW, &h.Vw}, {P_STATE, &h.State},
+        {P_TN, &h.Tn}, {P_TS1, &h.Ts1}, {P_TS2, &h.Ts2}, {P_T0, &h.init_t0}};
+    for (auto& u : up)
+      CK(cudaMemcpyAsync(ctx->pl + u.plane * nf, u.v->data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
+    struct { int plane; std::vector<int>* v; } iup[] = {
+        {I_UNITED, &h.united}, {I_FAULTGRID, &h.faultgrid}, {I_RUPY, &h.rupy}, {I_RUPZ, &h.rupz}};
+    for (auto& u : iup)
+      CK(cudaMemcpyAsync(ctx->ipl + u.plane * nf, u.v->data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s));
+    for (int b = 0; b < 2; b++) CK(cudaMemsetAsync(ctx->FW[b], 0, sizeof(float) * 18 * d.nyz, s));
+    CK(cudaMemsetAsync(ctx->Fm, 0, sizeof(float) * 18 * d.nyz, s));
+    CK(cudaMemsetAsync(ctx->Ft, 0, sizeof(float) * 18 * d.nyz, s));
+    CK(cudaMemsetAsync(ctx->T1, 0, sizeof(float) * 21 * d.nyz, s));
+    CK(cudaMemsetAsync(ctx->mT1, 0, sizeof(float) * 3 * d.nyz, s));
+    CK(cudaMemsetAsync(ctx->hT1, 0, sizeof(float) * 3 * d.nyz, s));
+  }
+  for (int b = 0; b < 4; b++) CK(cudaMemsetAsync(ctx->W[b], 0, sizeof(float) * 9 * d.nxyz, s));
+  {
+    long long sz[6] = {(long long)d.N * d.nj * d.nk, (long long)d.N * d.nj * d.nk, (long long)d.N * d.nk * d.ni,
+                       (long long)d.N * d.nk * d.ni, (long long)d.N * d.ni * d.nj, (long long)d.N * d.ni * d.nj};
+    for (int f = 0; f < 6; f++)
+      for (int r3 = 0; r3 < 3; r3++)
+        if (ctx->aux[f][r3]) CK(cudaMemsetAsync(ctx->aux[f][r3], 0, sizeof(float) * 9 * sz[f], s));
+  }
+  CK(cudaMemsetAsync(ctx->newton, 0, 2 * sizeof(unsigned long long), s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  for (auto& gr : ctx->graph)
+    if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
+  ctx->ready = true;
+  ctx->next_stage = 0;
+  return DFD_OK;
+}
+
+}  // extern "C"
+
+static const int kFlags[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1},
+                                 {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
+
+// enqueue one stage on the context streams (no synchronisation)
+static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk) {
+  const dfd_params& p = ctx->p;
+  const Dims& d = ctx->d;
+  int sg = (irk % 2) ? -1 : 1;
+  int FX = kFlags[pattern][0] * sg, FY = kFlags[pattern][1] * sg, FZ = kFlags[pattern][2] * sg;
+  static const int bin[4] = {0, 1, 2, 1}, bout[4] = {1, 2, 1, 0};
+  float a_ = irk == 0 ? 0.5f : irk == 1 ? 0.5f : irk == 2 ? 1.0f : 1e10f;
+  float b_ = (irk == 0 || irk == 3) ? (float)(1.0 / 6.0) : (float)(1.0 / 3.0);
+  float DT = (float)p.DT;
+  float rka = a_ * DT, rkb = b_ * DT;
+  size_t nf = (size_t)d.nj * d.nk;
+  FaultArgs fa;
+  if (p.rupture) {
+    memset(&fa, 0, sizeof fa);
+    fa.d = d;
+    fa.Win = ctx->W[bin[irk]]; fa.W0 = ctx->W[0]; fa.Wout = ctx->W[bout[irk]]; fa.T = ctx->W[3];
+    fa.M = ctx->M; fa.mVx2Vz = ctx->mVx2Vz; fa.mVy2Vz = ctx->mVy2Vz;
+    fa.dampx = ctx->damp[0]; fa.dampy = ctx->damp[1]; fa.dampz = ctx->damp[2];
+    fa.FWin = ctx->FW[irk % 2]; fa.FWout = ctx->FW[(irk + 1) % 2]; fa.Fm = ctx->Fm; fa.Ft = ctx->Ft;
+    fa.T1 = ctx->T1; fa.mT1 = ctx->mT1; fa.hT1 = ctx->hT1;
+    fa.tab = ctx->tab; fa.tabf = ctx->tabf; fa.vecn = ctx->vecn; fa.vecs1 = ctx->vecs1; fa.vecs2 = ctx->vecs2;
+    fa.rhof = ctx->rhof;
+    float* P_ = ctx->pl;
+    auto pl = [&](int k) { return P_ + k * nf; };
+    fa.slip = pl(P_SLIP); fa.mslip = pl(P_MSLIP); fa.tslip = pl(P_TSLIP); fa.hslip = pl(P_HSLIP);
+    fa.State = pl(P_STATE); fa.mState = pl(P_MSTATE); fa.tState = pl(P_TSTATE);
+    fa.Vs1 = pl(P_VS1); fa.Vs2 = pl(P_VS2); fa.Tn = pl(P_TN); fa.Ts1 = pl(P_TS1); fa.Ts2 = pl(P_TS2);
+    fa.tTn = pl(P_TTN); fa.tTs1 = pl(P_TTS1); fa.tTs2 = pl(P_TTS2);
+    fa.sx = pl(P_SX); fa.sy = pl(P_SY); fa.sz = pl(P_SZ);
+    fa.T0x = pl(P_T0X); fa.T0y = pl(P_T0Y); fa.T0z = pl(P_T0Z);
+    fa.dT0x = pl(P_DT0X); fa.dT0y = pl(P_DT0Y); fa.dT0z = pl(P_DT0Z);
+    fa.str_peak = pl(P_PEAK); fa.Dc = pl(P_DC); fa.C0 = pl(P_C0);
+    fa.a = pl(P_A); fa.b = pl(P_B); fa.L = pl(P_L); fa.Vw = pl(P_VW);
+    fa.init_t0 = pl(P_T0); fa.friction = pl(P_FRIC);
+    fa.init_t0_flag = ctx->ipl + I_T0FLAG * nf; fa.flag_rup = ctx->ipl + I_FLAGRUP * nf;
+    fa.united = ctx->ipl + I_UNITED * nf; fa.faultgrid = ctx->ipl + I_FAULTGRID * nf;
+    fa.rupy = ctx->ipl + I_RUPY * nf; fa.rupz = ctx->ipl + I_RUPZ * nf;
+    fa.newton = ctx->newton; fa.it_dev = ctx->it_dev; fa.guess_net = ctx->guess_net;
+    fa.rDH = (float)(1.0 / p.DH); fa.DH = (float)p.DH; fa.DT = DT; fa.rka = rka; fa.rkb = rkb;
+    fa.mu_d = (float)p.mu_d; fa.viscosity = (float)p.viscosity;
+    fa.dDT = (double)DT; fa.smooth_load_T = (double)(float)p.smooth_load_T;
+    fa.f0 = (double)(float)p.f0; fa.V0 = (double)(float)p.V0; fa.fw = (double)(float)p.fw;
+    fa.Vini = (double)(float)p.Vini;
+    fa.irk = irk; fa.FX = FX; fa.FY = FY; fa.FZ = FZ;
+    fa.freenode = p.free_surface; fa.friction_type = p.Friction_type; fa.inport_stress = p.INPORT_STRESS_TYPE;
+    fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess;
+    launch_fault_node(fa, ctx->s0);
+    cudaEventRecord(ctx->ev_fork, ctx->s0);
+    cudaStreamWaitEvent(ctx->s1, ctx->ev_fork, 0);
+    launch_fault_band(fa, ctx->s1);
+    cudaEventRecord(ctx->ev_join, ctx->s1);
+  }
+  VolArgs va;
+  memset(&va, 0, sizeof va);
+  va.d = d;
+  va.Win = ctx->W[bin[irk]]; va.W0 = ctx->W[0]; va.Wout = ctx->W[bout[irk]]; va.T = ctx->W[3];
+  va.M = ctx->M;
+  va.rBx = ctx->rB[0]; va.rBy = ctx->rB[1]; va.rBz = ctx->rB[2];
+  va.Bx = ctx->B[0]; va.By = ctx->B[1]; va.Bz = ctx->B[2];
+  va.Dpx = ctx->Dp[0]; va.Dpy = ctx->Dp[1]; va.Dpz = ctx->Dp[2];
+  va.Apx = ctx->Ap[0]; va.Apy = ctx->Ap[1]; va.Apz = ctx->Ap[2];
+  for (int f = 0; f < 6; f++) { va.aux[f] = ctx->aux[f][0]; va.aux0[f] = ctx->aux[f][1]; va.auxT[f] = ctx->aux[f][2]; }
+  va.mVx2Vz = ctx->mVx2Vz; va.mVy2Vz = ctx->mVy2Vz;
+  va.dampx = ctx->damp[0]; va.dampy = ctx->damp[1]; va.dampz = ctx->damp[2];
+  va.united = p.rupture ? ctx->ipl + I_UNITED * nf : nullptr;
+  va.rDH = (float)(1.0 / p.DH); va.rka = rka; va.rkb = rkb;
+  va.irk = irk; va.freenode = p.free_surface;
+  launch_volume_stage(va, FX, FY, FZ, ctx->s0);
+  if (p.rupture) cudaStreamWaitEvent(ctx->s0, ctx->ev_join, 0);
+  return cuda_check(ctx, cudaGetLastError(), "stage launch");
+}
+
+extern "C" {
+
+int dfd_stage(dfd_ctx* ctx, int it, int irk) {
+  if (!ctx) return DFD_ERR_PARAM;
+  if (ctx->sticky) return ctx->sticky;
+  if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
+  if (irk != ctx->next_stage) return fail(ctx, DFD_ERR_STATE, "stages must be issued in order 0..3");
+  cudaSetDevice(ctx->device);
+  if (irk == 0) dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it);
+  int r = enqueue_stage(ctx, ((it % 8) + 8) % 8, irk);
+  if (r) return r;
+  ctx->next_stage = (irk + 1) % 4;
+  return DFD_OK;
+}
+
+// capture the four stages of one step (flag pattern) and the step-counter advance
+static int build_graph(dfd_ctx* ctx, int pattern) {
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(ctx->s0, cudaStreamCaptureModeThreadLocal));
+  int r = 0;
+  for (int irk = 0; irk < 4 && !r; irk++) r = enqueue_stage(ctx, pattern, irk);
+  dfd::inc_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev);
+  cudaError_t e = cudaStreamEndCapture(ctx->s0, &g);
+  if (r) return r;
+  CK(e);
+  CK(cudaGraphInstantiate(&ctx->graph[pattern], g, 0));
+  cudaGraphDestroy(g);
+  return DFD_OK;
+}
+
+int dfd_run(dfd_ctx* ctx, int it0, int nsteps) {
+  if (!ctx) return DFD_ERR_PARAM;
+  if (ctx->sticky) return ctx->sticky;
+  if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
+  if (ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "a step is half done (dfd_stage)");
+  cudaSetDevice(ctx->device);
+  dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it0);
+  for (int s = 0; s < nsteps; s++) {
+    int pat = (((it0 + s) % 8) + 8) % 8;
+    if (!ctx->graph[pat]) {
+      int r = build_graph(ctx, pat);
+      if (r) return r;
+    }
+    CK(cudaGraphLaunch(ctx->graph[pat], ctx->s0));
+  }
+  return DFD_OK;
+}
+
+int dfd_step(dfd_ctx* ctx, int it) { return dfd_run(ctx, it, 1); }
+
+int dfd_synchronize(dfd_ctx* ctx) {
+  if (!ctx) return DFD_ERR_PARAM;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s1));
+  return ctx->sticky;
+}
+
+int dfd_get_wave(dfd_ctx* ctx, float* host) {
+  if (!ctx || !host) return DFD_ERR_PARAM;
+  if (ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "wavefield is mid-step");
+  CK(cudaStreamSynchronize(ctx->s0));
+  CK(cudaMemcpy(host, ctx->W[0], sizeof(float) * 9 * ctx->d.nxyz, cudaMemcpyDeviceToHost));
+  return DFD_OK;
+}
+int dfd_set_wave(dfd_ctx* ctx, const float* host) {
+  if (!ctx || !host) return DFD_ERR_PARAM;
+  if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
+  CK(cudaStreamSynchronize(ctx->s0));
+  CK(cudaMemcpy(ctx->W[0], host, sizeof(float) * 9 * ctx->d.nxyz, cudaMemcpyHostToDevice));
+  return DFD_OK;
+}
+int dfd_get_metric(dfd_ctx* ctx, float* host) {
+  if (!ctx || !host) return DFD_ERR_PARAM;
+  CK(cudaStreamSynchronize(ctx->s0));
+  CK(cudaMemcpy(host, ctx->M, sizeof(float) * 13 * ctx->d.nxyz, cudaMemcpyDeviceToHost));
+  return DFD_OK;
+}
+
+int dfd_get_fault(dfd_ctx* ctx, int field, float* host) {
+  if (!ctx || !host || field < 0 || field >= DFD_F_COUNT) return DFD_ERR_PARAM;
+  if (!ctx->p.rupture) return fail(ctx, DFD_ERR_STATE, "rupture is off");
+  CK(cudaStreamSynchronize(ctx->s0));
+  size_t nf = (size_t)ctx->d.nj * ctx->d.nk;
+  static const int map[] = {P_SLIP, P_HSLIP, P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_STATE,
+                            P_T0, P_TTN, P_TTS1, P_TTS2, P_PEAK, P_FRIC};
+  if (field <= DFD_F_FRICTION) {
+    CK(cudaMemcpy(host, ctx->pl + map[field] * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
+  } else if (field == DFD_F_UNITED || field == DFD_F_FAULTGRID) {
+    std::vector<int> t(nf);
+    CK(cudaMemcpy(t.data(), ctx->ipl + (field == DFD_F_UNITED ? I_UNITED : I_FAULTGRID) * nf, sizeof(int) * nf,
+                  cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < nf; i++) host[i] = (float)t[i];
+  } else if (field == DFD_F_SPLIT) {
+    CK(cudaMemcpy(host, ctx->FW[0], sizeof(float) * 18 * ctx->d.nyz, cudaMemcpyDeviceToHost));
+  } else if (field == DFD_F_T1) {
+    CK(cudaMemcpy(host, ctx->T1, sizeof(float) * 21 * ctx->d.nyz, cudaMemcpyDeviceToHost));
+  } else {
+    CK(cudaMemcpy(host, ctx->hT1, sizeof(float) * 3 * ctx->d.nyz, cudaMemcpyDeviceToHost));
+  }
+  return DFD_OK;
+}
+
+int dfd_get_slice(dfd_ctx* ctx, int axis, int index, float* host) {
+  if (!ctx || !host || axis < 0 || axis > 2) return DFD_ERR_PARAM;
+  const Dims& d = ctx->d;
+  int lim = axis == 0 ? d.ni : axis == 1 ? d.nj : d.nk;
+  if (index < 0 || index >= lim) return DFD_ERR_PARAM;
+  int na = axis == 0 ? d.nk : d.ni, nb = axis == 1 ? d.nk : d.nj;
+  float* dv;
+  CK(cudaMalloc(&dv, sizeof(float) * 3 * na * nb));
+  dfd::slice_kernel<<<(na * nb + 255) / 256, 256, 0, ctx->s0>>>(d, ctx->W[0], axis, index, dv);
+  cudaError_t e = cudaMemcpyAsync(host, dv, sizeof(float) * 3 * na * nb, cudaMemcpyDeviceToHost, ctx->s0);
+  cudaStreamSynchronize(ctx->s0);
+  cudaFree(dv);
+  return cuda_check(ctx, e, "slice");
+}
+
+int dfd_check_finite(dfd_ctx* ctx) {
+  if (!ctx) return DFD_ERR_PARAM;
+  if (!ctx->p.rupture) return DFD_OK;
+  size_t nf = (size_t)ctx->d.nj * ctx->d.nk;
+  CK(cudaMemsetAsync(ctx->flag_dev, 0, sizeof(int), ctx->s0));
+  dfd::nonfinite_kernel<<<64, 256, 0, ctx->s0>>>(ctx->pl, (long long)(P_TTS2 + 1) * nf, ctx->flag_dev);
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, ctx->flag_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
+  if (flag) return fail(ctx, DFD_ERR_NONFINITE, "NaN or Inf in the fault state");
+  return DFD_OK;
+}
+
+int dfd_newton_stats(dfd_ctx* ctx, long long* iterations, long long* capped) {
+  if (!ctx) return DFD_ERR_PARAM;
+  unsigned long long v[2] = {0, 0};
+  CK(cudaStreamSynchronize(ctx->s0));
+  CK(cudaMemcpy(v, ctx->newton, sizeof v, cudaMemcpyDeviceToHost));
+  if (iterations) *iterations = (long long)v[0];
+  if (capped) *capped = (long long)v[1];
+  return DFD_OK;
+}
+
+int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {
+  if (!ctx || !w || n != 1225) return DFD_ERR_PARAM;
+  CK(cudaMemcpy(ctx->guess_net, w, sizeof(float) * n, cudaMemcpyHostToDevice));
+  return DFD_OK;
+}
+
+// ------------------------------------------------------------------ output --
+int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
+  if (!ctx || !outdir) return DFD_ERR_PARAM;
+  if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
+  const dfd_params& p = ctx->p;
+  const Dims& d = ctx->d;
+  std::string dir(outdir);
+  // fault file (io_fault.cu:16-71)
+  if (p.rupture) {
+    NcWriter& w = ctx->ncf;
+    if (!w.open(dir + "/fault_mpi000000.nc")) return fail(ctx, DFD_ERR_IO, "cannot create fault output");
+    int nt = w.dim("nt", 0), nzd = w.dim("nz", d.nk), nyd = w.dim("ny", d.nj);
+    std::vector<int> d2 = {nzd, nyd}, d3 = {nt, nzd, nyd};
+    const char* fixed[] = {"x", "y", "z", "init_t0", "C0", "str_peak"};
+    for (int i = 0; i < 6; i++) ctx->vf[i] = w.var(fixed[i], 5, d2);
+    ctx->vf[6] = w.var("united", 4, d2);
+    ctx->vf[7] = w.var("a", 5, d2);
+    ctx->vf[8] = w.var("b", 5, d2);
+    ctx->vf[9] = w.var("Vw", 5, d2);
+    const char* rec[] = {"Vs1", "Vs2", "tn", "ts1", "ts2", "Us0", "State"};
+    for (int i = 0; i < 7; i++) ctx->vf[10 + i] = w.var(rec[i], 5, d3);
+    w.var("rup_index_y", 4, d3);
+    w.var("rup_index_z", 4, d3);
+    w.var("rup_sensor", 5, d3);
+    w.var("TP_T", 5, d3);
+    w.var("TP_P", 5, d3);
+    w.enddef();
+    size_t nf = (size_t)d.nj * d.nk;
+    std::vector<float> x(nf), y(nf), z(nf), t(nf);
+    for (int k = 0; k < d.nk; k++)
+      for (int j = 0; j < d.nj; j++) {
+        size_t q = j + (size_t)k * d.nj, f = (j + 3) + (size_t)(k + 3) * d.ny;
+        x[q] = (float)(ctx->xl[d.i0] + ctx->fx[f]);
+        y[q] = (float)ctx->fy[f];
+        z[q] = (float)ctx->fz[f];
+      }
+    w.put_fixed(ctx->vf[0], x.data());
+    w.put_fixed(ctx->vf[1], y.data());
+    w.put_fixed(ctx->vf[2], z.data());
+    CK(cudaMemcpy(t.data(), ctx->pl + P_C0 * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
+    w.put_fixed(ctx->vf[4], t.data());
+    CK(cudaMemcpy(t.data(), ctx->pl + P_PEAK * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
+    w.put_fixed(ctx->vf[5], t.data());
+    std::vector<int> u(nf);
+    CK(cudaMemcpy(u.data(), ctx->ipl + I_UNITED * nf, sizeof(int) * nf, cudaMemcpyDeviceToHost));
+    w.put_fixed(ctx->vf[6], u.data());
+    int ab[3] = {P_A, P_B, P_VW};
+    for (int i = 0; i < 3; i++) {
+      CK(cudaMemcpy(t.data(), ctx->pl + ab[i] * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
+      w.put_fixed(ctx->vf[7 + i], t.data());
+    }
+    w.sync();
+  }
+  // wave slices (io_wave_xy.cu / io_wave_xz.cu / io_wave_yz.cu)
+  const char* names[3] = {"wave_yz", "wave_xz", "wave_xy"};
+  int idx[3] = {p.EXPORT_WAVE_SLICE_X, p.EXPORT_WAVE_SLICE_Y, p.EXPORT_WAVE_SLICE_Z};
+  int lim[3] = {d.ni, d.nj, d.nk};
+  for (int a = 0; a < 3; a++) {
+    if (idx[a] < 0 || idx[a] >= lim[a]) continue;
+    NcWriter& w = ctx->ncw[a];
+    if (!w.open(dir + "/" + names[a] + "_mpi000000.nc")) return fail(ctx, DFD_ERR_IO, "cannot create slice output");
+    int nt = w.dim("nt", 0);
+    int da, db;
+    if (a == 0) { da = w.dim("nz", d.nk); db = w.dim("ny", d.nj); }
+    else if (a == 1) { da = w.dim("nx", d.ni); db = w.dim("nz", d.nk); }
+    else { da = w.dim("nx", d.ni); db = w.dim("ny", d.nj); }
+    std::vector<int> d2 = {da, db}, d3 = {nt, da, db};
+    int cx = w.var("x", 5, d2), cy = w.var("y", 5, d2), cz = w.var("z", 5, d2);
+    ctx->vw[a][0] = w.var("Vx", 5, d3);
+    ctx->vw[a][1] = w.var("Vy", 5, d3);
+    ctx->vw[a][2] = w.var("Vz", 5, d3);
+    w.enddef();
+    int na = a == 0 ? d.nk : d.ni, nb = a == 1 ? d.nk : d.nj;
+    std::vector<float> X((size_t)na * nb), Y(X.size()), Z(X.size());
+    for (int ia = 0; ia < na; ia++)
+      for (int ib = 0; ib < nb; ib++) {
+        int i, j, k;
+        if (a == 0) { i = idx[a]; k = ia; j = ib; }
+        else if (a == 1) { j = idx[a]; i = ia; k = ib; }
+        else { k = idx[a]; i = ia; j = ib; }
+        size_t f = (j + 3) + (size_t)(k + 3) * d.ny, q = (size_t)ia * nb + ib;
+        X[q] = (float)(ctx->xl[i + 3] + ctx->fx[f]);
+        Y[q] = (float)ctx->fy[f];
+        Z[q] = (float)ctx->fz[f];
+      }
+    w.put_fixed(cx, X.data());
+    w.put_fixed(cy, Y.data());
+    w.put_fixed(cz, Z.data());
+    w.sync();
+  }
+  ctx->out_open = true;
+  return DFD_OK;
+}
+
+// one output record (the reference writes it before the step, main.cu:425-437)
+int dfd_output_write(dfd_ctx* ctx, int it_skip) {
+  if (!ctx || !ctx->out_open) return DFD_ERR_STATE;
+  const Dims& d = ctx->d;
+  size_t nf = (size_t)d.nj * d.nk;
+  if (ctx->p.rupture) {
+    CK(cudaStreamSynchronize(ctx->s0));
+    static const int rec[7] = {P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_SLIP, P_STATE};
+    std::vector<float> t(nf);
+    for (int i = 0; i < 7; i++) {
+      CK(cudaMemcpy(t.data(), ctx->pl + rec[i] * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
+      ctx->ncf.put_record(ctx->vf[10 + i], it_skip, t.data());
+    }
+    CK(cudaMemcpy(t.data(), ctx->pl + P_T0 * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
+    ctx->ncf.put_fixed(ctx->vf[3], t.data());
+    std::vector<int> u(nf);
+    CK(cudaMemcpy(u.data(), ctx->ipl + I_RUPY * nf, sizeof(int) * nf, cudaMemcpyDeviceToHost));
+    ctx->ncf.put_record(17, it_skip, u.data());
+    CK(cudaMemcpy(u.data(), ctx->ipl + I_RUPZ * nf, sizeof(int) * nf, cudaMemcpyDeviceToHost));
+    ctx->ncf.put_record(18, it_skip, u.data());
+    std::fill(t.begin(), t.end(), 0.0f);
+    for (int v = 19; v < 22; v++) ctx->ncf.put_record(v, it_skip, t.data());
+    ctx->ncf.sync();
+  }
+  int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y, ctx->p.EXPORT_WAVE_SLICE_Z};
+  int lim[3] = {d.ni, d.nj, d.nk};
+  for (int a = 0; a < 3; a++) {
+    if (idx[a] < 0 || idx[a] >= lim[a]) continue;
+    int na = a == 0 ? d.nk : d.ni, nb = a == 1 ? d.nk : d.nj;
+    std::vector<float> buf((size_t)3 * na * nb);
+    int r = dfd_get_slice(ctx, a, idx[a], buf.data());
+    if (r) return r;
+    for (int c = 0; c < 3; c++) ctx->ncw[a].put_record(ctx->vw[a][c], it_skip, buf.data() + (size_t)c * na * nb);
+    ctx->ncw[a].sync();
+  }
+  return DFD_OK;
+}
+
+int dfd_output_close(dfd_ctx* ctx) {
+  if (!ctx) return DFD_ERR_PARAM;
+  ctx->ncf.close();
+  for (auto& w : ctx->ncw) w.close();
+  ctx->out_open = false;
+  return DFD_OK;
+}
+
+}  // extern "C"

@@ -280,7 +280,8 @@ __global__ void __launch_bounds__(128) fault_node_kernel(FaultArgs a) {
   float jacvec = a.M[9 * n + qm] * n0;
 #pragma unroll
   for (int c = 0; c < 3; c++) nv[c] /= n0;
-  double t = a.irk == 0 ? a.it * a.dDT : (a.irk == 3 ? (a.it + 1) * a.dDT : (a.it + 0.5) * a.dDT);
+  const int it = *a.it_dev;
+  double t = a.irk == 0 ? it * a.dDT : (a.irk == 3 ? (it + 1) * a.dDT : (it + 0.5) * a.dDT);
   float G = (float)gt_func(t, a.smooth_load_T);
   float dV[3];
 #pragma unroll
@@ -413,7 +414,7 @@ __global__ void __launch_bounds__(128) fault_node_kernel(FaultArgs a) {
   a.tTs2[q2] = Tau[0] * s2[0] + Tau[1] * s2[1] + Tau[2] * s2[2];
   a.tTn[q2] = Tau_n;
   if (!a.init_t0_flag[q2] && Vcheck > 1e-3f) {
-    a.init_t0[q2] = (float)(a.it * a.dDT);
+    a.init_t0[q2] = (float)(it * a.dDT);
     a.init_t0_flag[q2] = 1;
     a.flag_rup[q2] = 1;
   }

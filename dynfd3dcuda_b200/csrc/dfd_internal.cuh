@@ -121,11 +121,26 @@ struct FaultArgs {
   int *init_t0_flag, *flag_rup;
   const int *united, *faultgrid, *rupy, *rupz;
   unsigned long long* newton;      // [0] iterations, [1] capped solves
+  const int* it_dev;               // current step index (device copy, advanced inside graphs)
   const float* guess_net;          // learned-guess MLP weights or null
   // scalars
   float rDH, DH, DT, rka, rkb, mu_d, viscosity;
   double dDT, smooth_load_T, f0, V0, fw, Vini;
   int it, irk, FX, FY, FZ, freenode, friction_type, inport_stress, NY, NZ, rs_guess;
+};
+
+// Separable grid description for the FP64 metric kernel (dfd_setup.cu).
+struct GridArgs {
+  Dims d;
+  const double* xl;  // (nx) extended x line
+  const double* fx;  // (nz, ny) extended fault surface
+  const double* fy;
+  const double* fz;
+  const float* layers;  // (nlayer, 4) depth rho vp vs
+  int nlayer;
+  int NXhalf;           // NX/2: bimaterial split on the padded index (metric.cu:140-142)
+  double rDH;
+  double lam1, mu1, rho1, lam2, mu2, rho2;
 };
 
 __host__ __device__ inline long long idx3(const Dims& d, int i, int j, int k) {

@@ -48,8 +48,9 @@ typedef struct dfd_params {
   int Fault_grid[4];
   int Asp_grid[4];
   double bi_vp1, bi_vs1, bi_rho1, bi_vp2, bi_vs2, bi_rho2;
-  /* switches (reference macros): free surface, PML, Cerjan sponge, normal refinement */
-  int free_surface, use_pml, use_cerjan, normal_refine;
+  /* switches (reference macros): rupture (fault kernels on), free surface, PML, Cerjan
+   * sponge, normal refinement of the x grid around the fault */
+  int rupture, free_surface, use_pml, use_cerjan, normal_refine;
   /* 0 = plain Newton initial guess (reference), 1 = learned guess with Newton fallback */
   int rs_guess;
   char OUT[1024];
@@ -72,6 +73,8 @@ enum {
 };
 
 /* ---- parameters (set_params.cu:56-297) ---- */
+/* sizeof(dfd_params), for bindings that mirror the struct */
+int dfd_params_size(void);
 int dfd_params_default(dfd_params *p);
 int dfd_params_load_json(const char *path, dfd_params *p);
 
@@ -90,8 +93,9 @@ int dfd_load_media1d(dfd_ctx *ctx, int n, const float *layers);
 /* 15 planes of (NZ, NY): Tx Ty Tz dTx dTy dTz mu_s mu_d Dc C0 a b L Vw State */
 int dfd_load_fault_init(dfd_ctx *ctx, const float *planes);
 
-/* ---- setup: grid, metric, media, PML and Cerjan profiles on the host in FP64, fault
- *      and free-surface coefficient tables on the GPU in FP64 (replaces cal_metric
+/* ---- setup: grid, metric and media on the GPU in FP64 (no 3-D coordinate array), PML
+ *      and Cerjan profiles on the host, fault and free-surface coefficient tables on the
+ *      GPU in FP64 (replaces construct_coord coord.cu:153-328, cal_metric
  *      metric.cu:15-171, abs_init init_pml.cu:42-155, init_cerjan_host cerjan.cu:31-164,
  *      init_fault_coef fault_coef.cu:26-1312, init_wave_free :1320-1498, init_fault
  *      init.cu:160-849), then the CFL check of main.cu:323-345 ---- */

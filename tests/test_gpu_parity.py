@@ -1,0 +1,114 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 oracle and the reference.
+
+Every case of tests/golden/cases.py runs on the GPU in FP32 and on the CPU oracle in
+FP64 (the oracle itself is pinned to the reference's own CUDA build by
+test_oracle_golden.py); the GPU result is also compared with the reference's FP32 build
+fixtures directly.
+
+Tolerances (relative to the field's max magnitude): the product computes the stencils in
+FP32 while the reference's FP32 build evaluates them in FP64 arithmetic (double literals,
+macdrp.h:23-40), so FP32 rounding accumulates over the run; the rupture cases amplify it
+at the rupture front.  Rupture times must agree to within one time step.
+"""
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+J0, J1 = 24, 52
+TOL = {"vol_small": 2e-5, "vol_curved": 2e-5, "sw_flat": 2e-4, "sw_flat_nr": 2e-4, "sw_curved": 5e-4,
+       "rs_flat": 2e-3}
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    s = np.abs(b).max()
+    return np.abs(a - b).max() / (s if s > 0 else 1.0)
+
+
+def make_sim(name):
+    import dynfd3dcuda_b200 as dfd
+
+    p, fx, st, layers, w0, meta = cases.get_case(name)
+    job = dict(p)
+    if meta["volume"]:
+        job["Rupture"] = 0
+    sim = dfd.Simulation(job, fx, st, layers)
+    if w0 is not None:
+        sim.set_wave(w0.astype(np.float32))
+    return sim, p, fx, st, layers, w0, meta
+
+
+@pytest.mark.parametrize("name", cases.CASES)
+@pytest.mark.parametrize("mode", ["graph", "stage"])
+def test_cuda_matches_oracle(oracle_lib, name, mode):
+    sim, p, fx, st, layers, w0, meta = make_sim(name)
+    o = oracle_lib.Oracle(p, fx, st, layers, double=True)
+    if w0 is not None:
+        o.set("W", w0)
+    NX, NY, NZ = p["NX"], p["NY"], p["NZ"]
+    nx = NX + 6
+    i0 = nx // 2
+    # FP64 GPU precompute vs FP64 oracle: metric and media to FP32 rounding
+    M = sim.metric()
+    Mo = o.get("M").reshape(M.shape)
+    for f in range(13):
+        assert rel(M[f], Mo[f]) < 2e-6, f
+    tol = TOL[name]
+    g = np.load(f"{cases.__file__[:-8]}/{name}_sp.npz")
+    steps = [int(s) for s in g["steps"]]
+    it = 0
+    for s in steps:
+        while it < s:
+            if mode == "graph":
+                sim.run(it, 1)
+            else:
+                for irk in range(4):
+                    sim.stage(it, irk)
+            (o.step_volume if meta["volume"] else o.step)(it)
+            it += 1
+        W = sim.wave()
+        Wo = o.wave()
+        for f in range(9):
+            assert rel(W[f], Wo[f]) < tol, (s, f)
+        if not meta["volume"]:
+            for nm in ("slip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State"):
+                a = sim.fault(nm)
+                b = o.get(nm).reshape(NZ, NY)
+                assert rel(a, b) < tol, (s, nm, rel(a, b))
+                assert rel(a, g[f"{nm}_s{s}"]) < tol, (s, nm, "vs reference FP32 build")
+            t0 = sim.fault("init_t0")
+            assert np.abs(t0 - o.get("init_t0").reshape(NZ, NY)).max() <= 1.01 * p["DT"]
+    sim.check_finite()
+    W = sim.wave()
+    if meta["volume"]:
+        assert rel(W, g["W_final"]) < tol
+    else:
+        assert rel(W[:, i0 - 3:i0 + 4, :, J0:J1], g["W_block"]) < tol
+        assert rel(sim.fault("split")[..., J0:J1], g["FW_block"]) < tol
+    sim.close()
+
+
+def test_stage_and_graph_paths_agree():
+    """The per-stage entry point and the CUDA-graph step replay are the same computation."""
+    a, *_ = make_sim("sw_flat")
+    b, *_ = make_sim("sw_flat")
+    for it in range(12):
+        a.run(it, 1)
+        for irk in range(4):
+            b.stage(it, irk)
+    assert np.array_equal(a.wave(), b.wave())
+    assert np.array_equal(a.fault("slip"), b.fault("slip"))
+
+
+def test_run_many_steps_equals_single_steps():
+    a, *_ = make_sim("rs_flat")
+    b, *_ = make_sim("rs_flat")
+    a.run(0, 16)
+    for it in range(16):
+        b.run(it, 1)
+    assert np.array_equal(a.wave(), b.wave())
+    assert np.array_equal(a.fault("State"), b.fault("State"))
