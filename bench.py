@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark: grid-point-steps per second of the curved-grid rupture time step on B200.
+
+Workload (default): the curved-grid slip-weakening job -- 400 (strike) x 300 (normal) x
+200 (depth) nodes at DH = 100 m, a 60-degree dipping planar fault meshed by a curvilinear
+grid, free-surface topography of seeded Gaussian hills (amplitude 500 m, width 5 km),
+normal stress 7378 Pa/m of depth and shear 0.55 x normal, TPV10 friction, 12-node PML,
+DT = 6 ms.  Inputs are seeded synthetic data in the reference's file layouts
+(tests/golden/cases.py); each of the four 24.5 M-node volume buffers (0.88 GB) is far
+larger than the 126 MB L2, so no explicit flush is needed between steps.
+
+  value      Gpt-steps/s of the stepping loop on the device (CUDA events, max over ranks)
+  e2e        the same metric through the C ABI end to end: context creation, upload of the
+             job's host arrays from pinned memory, setup, K steps, and every step a copy of
+             the eight on-fault output planes back to pinned host memory (the reference
+             writes them every step, main.cu:425-437)
+  roofline   the fused volume kernel: 768 algorithmic bytes per node per step (39/57/57/39
+             floats over the four RK stages) over its event-timed duration, against the
+             measured HBM copy bandwidth
+  cpu_baseline / --impl reference: the OpenMP FP32 CPU restatement of the same scheme
+             (oracle/), the reference having no CPU path, on a bounded sample of steps
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+       [--config curved|flat|profile|large]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "tests", "golden"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+ALG_BYTES_PER_NODE_STEP = 768  # 192 floats: stages 39 + 57 + 57 + 39
+LAUNCHES_PER_STEP = 13         # 4 x (fault node + fault band + volume) + step-counter kernel
+
+
+def workload(name):
+    """(job, fxyz, stress, layers, label) of a benchmark configuration."""
+    import cases
+
+    if name == "curved":
+        NX, NY, NZ, DH = 300, 400, 200, 100.0
+        fg = [51, 350, 51, 200]
+        # DT = 6 ms: the 60-degree sheared, normal-refined grid has hmin = 32 m, so the
+        # reference's stability limit 1.3 hmin / vpmax (main.cu:323) is 6.94 ms
+        job = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.006, TMAX=9.003, PML_N=12, PML_velocity=6000.0,
+                   PML_bmax=2.5, PML_fc=1.592356687898089, INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1,
+                   Friction_type=0, Fault_grid=fg, mu_s=0.76, mu_d=0.448, Dc=0.5, C0=0.2e6,
+                   EXPORT_WAVE_SLICE_X=NX // 2, EXPORT_WAVE_SLICE_Y=NY // 2, EXPORT_WAVE_SLICE_Z=NZ - 1)
+        fx = cases.curved_geometry(NY, NZ, DH, dip_deg=60.0, hill_amp=500.0, hill_width=5e3, nhills=2, seed=2024)
+        n = cases.surface_normal(fx, DH)
+        st = cases.depth_stress(fx, fg, grad=7378.0, ratio=0.55, normal=n, patch=(0.0, -8.0e3, 1.5e3))
+        label = "curved-grid SW rupture 400x300x200 (strike x normal x depth), dh=100 m, dip 60, hills, PML 12"
+        return job, fx, st, None, label
+    if name == "flat":
+        NX, NY, NZ, DH = 100, 200, 100, 100.0
+        fg = [26, 175, 26, 100]
+        job = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.008, TMAX=8.004, PML_N=12, PML_velocity=6000.0,
+                   INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=0, Fault_grid=fg, mu_s=0.677,
+                   mu_d=0.525, Dc=0.4, C0=0.0, NormalRefine=0)
+        fx = cases.flat_geometry(NY, NZ, DH)
+        st = cases.sw_stress(fx, fg, patch=(0.0, -7.5e3, 1.5e3), patch_ts=-81.6e6)
+        label = "Cartesian SW rupture 200x100x100 (strike x normal x depth), dh=100 m, PML 12"
+        return job, fx, st, None, label
+    if name == "profile":
+        # mid-size case for ncu captures: 6.5 M nodes, each volume buffer 0.24 GB (> L2)
+        NX, NY, NZ, DH = 160, 256, 160, 100.0
+        fg = [41, 216, 41, 160]
+        job = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.008, TMAX=8.004, PML_N=12, PML_velocity=6000.0,
+                   INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=0, Fault_grid=fg, mu_s=0.677,
+                   mu_d=0.525, Dc=0.4, C0=0.0, NormalRefine=0)
+        fx = cases.flat_geometry(NY, NZ, DH)
+        st = cases.sw_stress(fx, fg, patch=(0.0, -6.0e3, 1.5e3), patch_ts=-81.6e6)
+        label = "profiling case: Cartesian SW rupture 256x160x160, dh=100 m, PML 12"
+        return job, fx, st, None, label
+    if name == "large":
+        NX, NY, NZ, DH = 600, 1000, 300, 50.0
+        fg = [101, 900, 61, 300]
+        depth = np.linspace(0, 15e3, 16)
+        vs = np.linspace(2000.0, 3600.0, 16)
+        layers = np.stack([depth, 2670.0 + 0 * depth, np.sqrt(3.0) * vs, vs], 1).astype(np.float32)
+        job = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.004, TMAX=8.002, PML_N=20, PML_velocity=6236.0,
+                   INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=0, Fault_grid=fg, mu_s=0.677,
+                   mu_d=0.525, Dc=0.4, C0=0.0, useCerjan=1, DAMP_N=20)
+        fx = cases.curved_geometry(NY, NZ, DH, dip_deg=90.0, hill_amp=0.0, seed=7)
+        rng = np.random.default_rng(7)
+        jj = np.arange(NY)[None, :]
+        fx[0] = (200.0 * np.sin(2 * np.pi * jj / NY * rng.uniform(1, 3)) + 0 * fx[0]).astype(np.float32)
+        n = cases.surface_normal(fx, DH)
+        st = cases.depth_stress(fx, fg, grad=7378.0, ratio=0.55, normal=n, mu_s=0.677, mu_d=0.525, Dc=0.4, C0=0.0,
+                                patch=(0.0, -7.5e3, 1.5e3))
+        label = "large curved-fault SW rupture 1000x600x300 (180 M nodes), dh=50 m, 1-D layered, PML 20 + Cerjan"
+        return job, fx, st, layers, label
+    raise SystemExit(f"unknown config {name}")
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if vis:
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if index < len(ids):
+                index = ids[index]
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        load = [s for s in sm if s > 0.5 * smax] or sm
+        reasons = set()
+        for r in rows:
+            for name, val in (("hw_slowdown", r[5]), ("hw_thermal_slowdown", r[6]), ("sw_thermal_slowdown", r[7]),
+                              ("sw_power_cap", r[8])):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax, "samples": len(rows),
+                "reasons": sorted(reasons)}
+
+
+def cpu_baseline(job, fx, st, layers, budget_s=25.0, max_steps=None):
+    """FP32 OpenMP CPU restatement on the same job for a bounded number of steps."""
+    import oracle
+
+    threads = oracle.threads()
+    t0 = time.time()
+    o = oracle.Oracle(job, fx, st, layers, double=False)
+    setup = time.time() - t0
+    npts = job["NX"] * job["NY"] * job["NZ"]
+    done, t_step = 0, 0.0
+    while True:
+        t1 = time.time()
+        o.step(done)
+        t_step += time.time() - t1
+        done += 1
+        if t_step > budget_s or (max_steps and done >= max_steps) or (t_step / done) * (done + 1) > 3 * budget_s:
+            break
+    del o
+    return {"value": npts * done / t_step / 1e9, "unit": "Gpt-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{done} time steps of the full workload grid after a {setup:.1f} s setup "
+                      f"(FP32 oracle/dfd_oracle.cpp, OpenMP {threads} threads)"}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_node():
+    """DRAM bytes per node per step of the volume kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "volume_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_node_step"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    job, fx, st, layers, label = workload(args.config)
+    npts = job["NX"] * job["NY"] * job["NZ"]
+    import oracle
+
+    o = oracle.Oracle(job, fx, st, layers, double=False)
+    for it in range(args.warmup):
+        o.step(it)
+    t0 = time.time()
+    done = 0
+    while done < args.steps:
+        o.step(args.warmup + done)
+        done += 1
+        el = time.time() - t0
+        if el > 90.0:
+            break
+    el = time.time() - t0
+    v = npts * done / el / 1e9
+    cores = oracle.threads()
+    line = {"impl": "reference", "metric": "Gpt-steps/s", "value": v, "unit": "Gpt-steps/s", "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": label, "nodes": npts},
+            "cpu_baseline": {"value": v, "unit": "Gpt-steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{done} of {args.steps} requested steps (capped at 90 s) on {cores} threads; "
+                                       "the reference has no CPU implementation, this is the OpenMP FP32 "
+                                       "restatement of its scheme"},
+            "e2e": {"value": v, "unit": "Gpt-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="curved", choices=["curved", "flat", "profile", "large"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import dynfd3dcuda_b200 as dfd
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    job, fx, st, layers, label = workload(args.config)
+    npts = job["NX"] * job["NY"] * job["NZ"]
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- device-resident throughput (replica per rank, no data-path collective)
+    sim = dfd.Simulation(job, fx, st, layers, device=local)
+    sim.run(0, args.warmup)
+    sim.synchronize()
+    barrier()
+    clk = Clocks(local)
+    clk.start()
+    total_ms, vol_ms, other_ms = sim.run_timed(args.warmup, args.steps)
+    clocks = clk.stop()
+    sim.check_finite()
+    barrier()
+    t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = npts * args.steps * world / (max_ms / 1e3) / 1e9
+    sim.close()
+
+    # ---------------- end to end through the C ABI from pinned host memory
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory()  # noqa: E731
+    hfx, hst = pin(fx), pin(st)
+    hlay = pin(layers) if layers is not None else None
+    nf = job["NY"] * job["NZ"]
+    hout = torch.empty((2, 8, nf), dtype=torch.float32).pin_memory()
+    barrier()
+    t0 = time.perf_counter()
+    e = dfd.Simulation(job, hfx.numpy(), hst.numpy(), hlay.numpy() if hlay is not None else None, device=local)
+    for s in range(args.steps):
+        e.run(s, 1)
+        e.fetch_outputs(hout[s % 2].data_ptr())
+        if s % 2 == 1:
+            e.synchronize()
+    e.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e.close()
+    t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_s = float(t.item())
+    h2d = (hfx.numel() + hst.numel() + (hlay.numel() if hlay is not None else 0)) * 4 / args.steps
+    d2h = 8 * nf * 4
+
+    peak, peak_kind = peaks()
+    achieved = ALG_BYTES_PER_NODE_STEP * npts * args.steps / (vol_ms / 1e3) / 1e9
+    tpn = traffic_per_node()
+    line = {
+        "metric": "Gpt-steps/s", "value": value, "unit": "Gpt-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": label, "nodes": npts, "fault_nodes": nf, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (each 9-field buffer 0.88 GB); no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": tpn * npts / 4 if tpn else None,
+                     "kernel": "volume_stage_kernel", "bytes_per_node_step": ALG_BYTES_PER_NODE_STEP,
+                     "volume_kernel_ms_per_step": vol_ms / args.steps, "peak_source": peak_kind},
+        "e2e": {"value": npts * args.steps * world / e2e_s / 1e9, "unit": "Gpt-steps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "includes": "create + host-array upload + FP64 setup + steps + per-step output fetch"},
+        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(job, fx, st, layers)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

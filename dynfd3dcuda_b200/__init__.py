@@ -80,7 +80,8 @@ def lib():
             "dfd_get_fault": [V, I, V], "dfd_get_slice": [V, I, I, V], "dfd_check_finite": [V],
             "dfd_newton_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong)],
             "dfd_output_open": [V, ctypes.c_char_p], "dfd_output_write": [V, I], "dfd_output_close": [V],
-            "dfd_set_guess_net": [V, V, I],
+            "dfd_set_guess_net": [V, V, I], "dfd_fetch_outputs": [V, V],
+            "dfd_run_timed": [V, I, I, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)
@@ -215,6 +216,16 @@ class Simulation:
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(lib().dfd_newton_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def fetch_outputs(self, host_ptr):
+        """Enqueue the copy of the (8, NZ, NY) per-step outputs into host memory at host_ptr."""
+        self._check(lib().dfd_fetch_outputs(self.h, host_ptr))
+
+    def run_timed(self, it0, nsteps):
+        """Run nsteps stage by stage; returns (total_ms, volume_kernel_ms, other_ms) from CUDA events."""
+        t, v, f = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        self._check(lib().dfd_run_timed(self.h, it0, nsteps, ctypes.byref(t), ctypes.byref(v), ctypes.byref(f)))
+        return t.value, v.value, f.value
 
     def set_guess_net(self, w):
         a = np.ascontiguousarray(w, np.float32).ravel()

@@ -46,10 +46,12 @@ __global__ void slice_kernel(Dims d, const float* W, int axis, int index, float*
 using namespace dfd;
 
 // fault 2-D planes held in one allocation
+// (the eight per-step output planes come first so one copy fetches them)
 enum Plane {
-  P_SLIP, P_MSLIP, P_TSLIP, P_HSLIP, P_STATE, P_MSTATE, P_TSTATE, P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_TTN, P_TTS1,
+  P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_SLIP, P_STATE, P_T0,
+  P_MSLIP, P_TSLIP, P_HSLIP, P_MSTATE, P_TSTATE, P_TTN, P_TTS1,
   P_TTS2, P_SX, P_SY, P_SZ, P_T0X, P_T0Y, P_T0Z, P_DT0X, P_DT0Y, P_DT0Z, P_PEAK, P_DC, P_C0, P_A, P_B, P_L, P_VW,
-  P_T0, P_FRIC, NPLANE
+  P_FRIC, NPLANE
 };
 enum IPlane { I_T0FLAG, I_FLAGRUP, I_UNITED, I_FAULTGRID, I_RUPY, I_RUPZ, NIPLANE };
 
@@ -413,7 +415,7 @@ static const int kFlags[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1
                                  {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
 
 // enqueue one stage on the context streams (no synchronisation)
-static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk) {
+static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr) {
   const dfd_params& p = ctx->p;
   const Dims& d = ctx->d;
   int sg = (irk % 2) ? -1 : 1;
@@ -480,7 +482,9 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk) {
   va.united = p.rupture ? ctx->ipl + I_UNITED * nf : nullptr;
   va.rDH = (float)(1.0 / p.DH); va.rka = rka; va.rkb = rkb;
   va.irk = irk; va.freenode = p.free_surface;
+  if (vb) cudaEventRecord(*vb, ctx->s0);
   launch_volume_stage(va, FX, FY, FZ, ctx->s0);
+  if (ve) cudaEventRecord(*ve, ctx->s0);
   if (p.rupture) cudaStreamWaitEvent(ctx->s0, ctx->ev_join, 0);
   return cuda_check(ctx, cudaGetLastError(), "stage launch");
 }
@@ -623,6 +627,49 @@ int dfd_newton_stats(dfd_ctx* ctx, long long* iterations, long long* capped) {
   CK(cudaMemcpy(v, ctx->newton, sizeof v, cudaMemcpyDeviceToHost));
   if (iterations) *iterations = (long long)v[0];
   if (capped) *capped = (long long)v[1];
+  return DFD_OK;
+}
+
+int dfd_fetch_outputs(dfd_ctx* ctx, float* host) {
+  if (!ctx || !host) return DFD_ERR_PARAM;
+  if (!ctx->p.rupture) return fail(ctx, DFD_ERR_STATE, "rupture is off");
+  size_t nf = (size_t)ctx->d.nj * ctx->d.nk;
+  CK(cudaMemcpyAsync(host, ctx->pl, sizeof(float) * 8 * nf, cudaMemcpyDeviceToHost, ctx->s0));
+  return DFD_OK;
+}
+
+int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* volume_ms, float* fault_ms) {
+  if (!ctx) return DFD_ERR_PARAM;
+  if (ctx->sticky) return ctx->sticky;
+  if (!ctx->ready || ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "not ready for a step");
+  cudaSetDevice(ctx->device);
+  int nev = 8 * nsteps + 2;
+  std::vector<cudaEvent_t> ev(nev);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(ev[0], ctx->s0));
+  int k = 1;
+  for (int s = 0; s < nsteps; s++) {
+    int it = it0 + s;
+    dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it);
+    for (int irk = 0; irk < 4; irk++) {
+      int r = enqueue_stage(ctx, ((it % 8) + 8) % 8, irk, &ev[k], &ev[k + 1]);
+      if (r) return r;
+      k += 2;
+    }
+  }
+  CK(cudaEventRecord(ev[nev - 1], ctx->s0));
+  CK(cudaEventSynchronize(ev[nev - 1]));
+  float tot = 0, vol = 0;
+  CK(cudaEventElapsedTime(&tot, ev[0], ev[nev - 1]));
+  for (int i = 1; i + 1 < nev - 1; i += 2) {
+    float m = 0;
+    CK(cudaEventElapsedTime(&m, ev[i], ev[i + 1]));
+    vol += m;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (total_ms) *total_ms = tot;
+  if (volume_ms) *volume_ms = vol;
+  if (fault_ms) *fault_ms = tot - vol;
   return DFD_OK;
 }
 

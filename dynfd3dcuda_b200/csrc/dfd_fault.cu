@@ -462,7 +462,15 @@ __global__ void __launch_bounds__(128) fault_band_kernel(FaultArgs a) {
   int k = blockIdx.y * blockDim.y + threadIdx.y;
   if (j >= d.nj || k >= d.nk) return;
   int q2 = j + k * d.nj;
-  if (a.united[q2]) return;
+  if (a.united[q2]) {
+    // welded nodes: the RK-weighted outputs run over every node in the reference
+    // (rk4.cu:521-569) and are zero there (no trial traction, no split velocity)
+    if (a.irk == 0) {
+      a.Tn[q2] = 0.0f; a.Ts1[q2] = 0.0f; a.Ts2[q2] = 0.0f;
+      a.Vs1[q2] = 0.0f; a.Vs2[q2] = 0.0f; a.hslip[q2] = 0.0f;
+    }
+    return;
+  }
   const long long n = d.nxyz, nyz = d.nyz;
   const int j1 = j + 3, k1 = k + 3, km = d.nk - k, i0 = d.i0;
   const long long pf = j1 + (long long)k1 * d.ny;

@@ -118,6 +118,13 @@ int dfd_set_wave(dfd_ctx *ctx, const float *host);  /* 9*nx*ny*nz */
 int dfd_get_metric(dfd_ctx *ctx, float *host);      /* 13*nx*ny*nz: xix..ztz jac lam mu rho */
 int dfd_get_fault(dfd_ctx *ctx, int field, float *host);
 int dfd_get_slice(dfd_ctx *ctx, int axis, int index, float *host);  /* Vx,Vy,Vz on one slice */
+/* enqueue (asynchronously, after the work already issued) a copy of the eight per-step
+ * on-fault output planes Vs1 Vs2 Tn Ts1 Ts2 slip State init_t0, (8, NZ, NY), into host
+ * memory (pinned for a true async copy); completes at the next dfd_synchronize */
+int dfd_fetch_outputs(dfd_ctx *ctx, float *host);
+/* nsteps steps issued stage by stage with CUDA events around every volume-kernel launch:
+ * total device time, time inside the volume kernels, and the rest (milliseconds) */
+int dfd_run_timed(dfd_ctx *ctx, int it0, int nsteps, float *total_ms, float *volume_ms, float *fault_ms);
 /* host-side health check: 0 ok, DFD_ERR_NONFINITE if the fault state holds NaN/Inf */
 int dfd_check_finite(dfd_ctx *ctx);
 /* cumulative Newton iterations and non-converged solves of the rate-and-state trial */

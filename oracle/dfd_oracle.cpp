@@ -255,6 +255,7 @@ template <typename R> struct Sim {
     }
     double* X = Cd.data(); double* Y = X + nxyz; double* Z = Y + nxyz;
     double x0 = -(p.NX / 2) * p.DH, y0 = -(p.NY / 2) * p.DH, z0 = (1 - p.NZ) * p.DH;
+#pragma omp parallel for schedule(static)
     for (int i = 3; i < nx - 3; i++)
       for (int k = 3; k < nz - 3; k++)
         for (int j = 3; j < ny - 3; j++) {
@@ -300,6 +301,7 @@ template <typename R> struct Sim {
   void cal_metric(int nlayer, const float* layers) {
     const double* X = Cd.data(); const double* Y = X + nxyz; const double* Z = Y + nxyz;
     double r = 1.0 / p.DH;
+#pragma omp parallel for schedule(static)
     for (int i = 3; i < nx - 3; i++)
       for (int k = 3; k < nz - 3; k++)
         for (int j = 3; j < ny - 3; j++) {
