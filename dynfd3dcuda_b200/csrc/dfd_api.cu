@@ -12,7 +12,7 @@
 #include "dfd_internal.cuh"
 
 namespace dfd {
-void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s);
+void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell);
 void launch_fault_node(const FaultArgs& a, cudaStream_t s);
 void launch_fault_band(const FaultArgs& a, cudaStream_t s);
 void launch_fault_coef(const Dims& d, const float* M, float* tab, float* tabf, float* vecn, float* vecs1,
@@ -59,8 +59,8 @@ struct dfd_ctx {
   dfd_params p;
   Dims d;
   int device = 0;
-  cudaStream_t s0 = nullptr, s1 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
   std::vector<void*> allocs;
   float* W[4] = {};
   float* M = nullptr;
@@ -175,8 +175,10 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   auto done = [&](int rc) { if (rc) { dfd_destroy(ctx); return rc; } return 0; };
   if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s0, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
   if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s1, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
+  if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s2, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
   cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ctx->ev_join2, cudaEventDisableTiming);
   int rc = 0;
   for (int b = 0; b < 4 && !rc; b++) rc = dalloc(ctx, &ctx->W[b], 9 * d.nxyz);
   if (!rc) rc = dalloc(ctx, &ctx->M, 13 * d.nxyz);
@@ -235,11 +237,14 @@ int dfd_destroy(dfd_ctx* ctx) {
     if (g) cudaGraphExecDestroy(g);
   if (ctx->s0) cudaStreamSynchronize(ctx->s0);
   if (ctx->s1) cudaStreamSynchronize(ctx->s1);
+  if (ctx->s2) cudaStreamSynchronize(ctx->s2);
   for (void* v : ctx->allocs) cudaFree(v);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->ev_join2) cudaEventDestroy(ctx->ev_join2);
   if (ctx->s0) cudaStreamDestroy(ctx->s0);
   if (ctx->s1) cudaStreamDestroy(ctx->s1);
+  if (ctx->s2) cudaStreamDestroy(ctx->s2);
   delete ctx;
   return DFD_OK;
 }
@@ -462,11 +467,16 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
     fa.freenode = p.free_surface; fa.friction_type = p.Friction_type; fa.inport_stress = p.INPORT_STRESS_TYPE;
     fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess;
     launch_fault_node(fa, ctx->s0);
-    cudaEventRecord(ctx->ev_fork, ctx->s0);
+  }
+  // fork: fault band on s1, volume shell on s2, volume interior on s0
+  cudaEventRecord(ctx->ev_fork, ctx->s0);
+  if (vb) cudaEventRecord(*vb, ctx->s0);
+  if (p.rupture) {
     cudaStreamWaitEvent(ctx->s1, ctx->ev_fork, 0);
     launch_fault_band(fa, ctx->s1);
     cudaEventRecord(ctx->ev_join, ctx->s1);
   }
+  cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
   VolArgs va;
   memset(&va, 0, sizeof va);
   va.d = d;
@@ -482,10 +492,11 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   va.united = p.rupture ? ctx->ipl + I_UNITED * nf : nullptr;
   va.rDH = (float)(1.0 / p.DH); va.rka = rka; va.rkb = rkb;
   va.irk = irk; va.freenode = p.free_surface;
-  if (vb) cudaEventRecord(*vb, ctx->s0);
-  launch_volume_stage(va, FX, FY, FZ, ctx->s0);
-  if (ve) cudaEventRecord(*ve, ctx->s0);
+  launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2);
+  cudaEventRecord(ctx->ev_join2, ctx->s2);
   if (p.rupture) cudaStreamWaitEvent(ctx->s0, ctx->ev_join, 0);
+  cudaStreamWaitEvent(ctx->s0, ctx->ev_join2, 0);
+  if (ve) cudaEventRecord(*ve, ctx->s0);
   return cuda_check(ctx, cudaGetLastError(), "stage launch");
 }
 
@@ -544,6 +555,7 @@ int dfd_synchronize(dfd_ctx* ctx) {
   cudaSetDevice(ctx->device);
   CK(cudaStreamSynchronize(ctx->s0));
   CK(cudaStreamSynchronize(ctx->s1));
+  CK(cudaStreamSynchronize(ctx->s2));
   return ctx->sticky;
 }
 

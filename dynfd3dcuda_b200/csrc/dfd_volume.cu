@@ -96,13 +96,11 @@ __device__ __forceinline__ void pml_face(const VolArgs& a, int face, long long q
   }
 }
 
+// General node update: every boundary treatment (PML faces, free-surface rows and
+// traction image, sponge).  Used for the shell of the domain outside the interior box.
 template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(256) volume_stage_kernel(VolArgs a) {
+__device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, int j, int k) {
   const Dims& d = a.d;
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int k = blockIdx.y * blockDim.y + threadIdx.y;
-  int i = blockIdx.z * blockDim.z + threadIdx.z;
-  if (j >= d.nj || k >= d.nk || i >= d.ni) return;
   int i1 = i + 3, j1 = j + 3, k1 = k + 3;
   if (a.united && i1 >= d.i0 - 3 && i1 <= d.i0 + 3 && !a.united[j + k * d.nj]) return;  // band node
   const long long n = d.nxyz;
@@ -256,19 +254,150 @@ __global__ void __launch_bounds__(256) volume_stage_kernel(VolArgs a) {
   }
 }
 
-void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s) {
-  dim3 block(32, 4, 2);
-  dim3 grid((a.d.nj + 31) / 32, (a.d.nk + 3) / 4, (a.d.ni + 1) / 2);
+
+// Shell kernel: the general update on up to six boxes (PML slabs, free-surface rows) that
+// surround the interior box; one 1-D grid of (32, 4, 2) blocks is split over the boxes.
+struct Boxes {
+  int n;
+  int lo[6][3], hi[6][3];  // (i, j, k) interior-index bounds, half open
+  int start[7];            // first block of each box
+};
+
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(256, 2) volume_shell_kernel(VolArgs a, Boxes bx) {
+  int b = 0;
+  while (b + 1 < bx.n && (int)blockIdx.x >= bx.start[b + 1]) b++;
+  int loc = blockIdx.x - bx.start[b];
+  int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
+  int gj = (nj + 31) / 32, gk = (nk + 3) / 4;
+  int bj = loc % gj, bk = (loc / gj) % gk, bi = loc / (gj * gk);
+  int j = bj * 32 + threadIdx.x, k = bk * 4 + threadIdx.y, i = bi * 2 + threadIdx.z;
+  if (i >= ni || j >= nj || k >= nk) return;
+  volume_point_general<FX, FY, FZ>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
+}
+
+// Interior kernel: no PML (beta = 1, no auxiliary state), no free-surface rows.  Each
+// derivative is scattered into the nine right-hand sides as soon as it is formed, which
+// keeps the register count low enough for three resident blocks per SM; each thread
+// walks a chunk of x so that the x-stencil halo is reused from L1.
+template <int FX, int FY, int FZ>
+__device__ __forceinline__ void interior_point(const VolArgs& a, long long q, float damp) {
+  const long long n = a.d.nxyz;
+  const float* __restrict__ W = a.Win;
+  const float* __restrict__ M = a.M;
+  const float r = a.rDH;
+  float lam = __ldg(M + 10 * n + q), mu = __ldg(M + 11 * n + q);
+  float rrho = 1.0f / __ldg(M + 12 * n + q);
+  float l2m = lam + 2.0f * mu;
+  float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f, h8 = 0.f;
+#define DFD_AXIS(F, S, MO)                                                                         \
+  {                                                                                                \
+    float e0 = __ldg(M + (MO) * n + q), e1 = __ldg(M + ((MO) + 1) * n + q), e2 = __ldg(M + ((MO) + 2) * n + q); \
+    float dv;                                                                                      \
+    dv = d5<F>(W, q, S) * r;                                                                       \
+    h3 += dv * e0 * l2m; h4 += dv * e0 * lam; h5 += dv * e0 * lam; h6 += dv * e1 * mu; h7 += dv * e2 * mu; \
+    dv = d5<F>(W + n, q, S) * r;                                                                   \
+    h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h6 += dv * e0 * mu; h8 += dv * e2 * mu; \
+    dv = d5<F>(W + 2 * n, q, S) * r;                                                               \
+    h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h7 += dv * e0 * mu; h8 += dv * e1 * mu; \
+    float er0 = e0 * rrho, er1 = e1 * rrho, er2 = e2 * rrho;                                       \
+    dv = d5<F>(W + 3 * n, q, S) * r; h0 += dv * er0;                                               \
+    dv = d5<F>(W + 4 * n, q, S) * r; h1 += dv * er1;                                               \
+    dv = d5<F>(W + 5 * n, q, S) * r; h2 += dv * er2;                                               \
+    dv = d5<F>(W + 6 * n, q, S) * r; h0 += dv * er1; h1 += dv * er0;                               \
+    dv = d5<F>(W + 7 * n, q, S) * r; h0 += dv * er2; h2 += dv * er0;                               \
+    dv = d5<F>(W + 8 * n, q, S) * r; h1 += dv * er2; h2 += dv * er1;                               \
+  }
+  DFD_AXIS(FX, a.d.nyz, 0)
+  DFD_AXIS(FY, 1, 3)
+  DFD_AXIS(FZ, a.d.ny, 6)
+#undef DFD_AXIS
+  float hv[9] = {h0, h1, h2, h3, h4, h5, h6, h7, h8};
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    long long x = f * n + q;
+    float w;
+    if (a.irk == 0) {
+      float w0 = __ldg(W + x);
+      a.T[x] = fmaf(a.rkb, hv[f], w0);
+      w = fmaf(a.rka, hv[f], w0);
+    } else if (a.irk < 3) {
+      a.T[x] = fmaf(a.rkb, hv[f], a.T[x]);
+      w = fmaf(a.rka, hv[f], __ldg(a.W0 + x));
+    } else {
+      w = fmaf(a.rkb, hv[f], a.T[x]);
+    }
+    a.Wout[x] = w * damp;
+  }
+}
+
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(256, 3) volume_interior_kernel(VolArgs a, int3 lo, int3 hi, int chunk) {
+  const Dims& d = a.d;
+  int j = lo.y + blockIdx.x * blockDim.x + threadIdx.x;
+  int k = lo.z + blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= hi.y || k >= hi.z) return;
+  int ib = lo.x + blockIdx.z * chunk, ie = min(ib + chunk, hi.x);
+  bool band = a.united && !a.united[j + k * d.nj];
+  float dyz = 1.0f;
+  if (a.dampx) dyz = fminf(__ldg(a.dampy + j + 3), __ldg(a.dampz + k + 3));
+  long long q = idx3(d, ib + 3, j + 3, k + 3);
+  for (int i = ib; i < ie; i++, q += d.nyz) {
+    if (band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3) continue;
+    float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
+    interior_point<FX, FY, FZ>(a, q, damp);
+  }
+}
+
+template <int FX, int FY, int FZ>
+static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell) {
+  const Dims& d = a.d;
+  // interior box: outside every PML slab and below the free-surface rows
+  int nx0 = a.aux[0] ? d.N : 0, nx1 = a.aux[1] ? d.N : 0;
+  int ny0 = a.aux[2] ? d.N : 0, ny1 = a.aux[3] ? d.N : 0;
+  int nz0 = a.aux[4] ? d.N : 0, nz1 = a.aux[5] ? d.N : (a.freenode ? 3 : 0);
+  int3 lo = make_int3(nx0, ny0, nz0), hi = make_int3(d.ni - nx1, d.nj - ny1, d.nk - nz1);
+  const int chunk = 8;
+  if (hi.x > lo.x && hi.y > lo.y && hi.z > lo.z) {
+    dim3 block(32, 8, 1);
+    dim3 grid((hi.y - lo.y + 31) / 32, (hi.z - lo.z + 7) / 8, (hi.x - lo.x + chunk - 1) / chunk);
+    volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, lo, hi, chunk);
+  }
+  Boxes bx;
+  bx.n = 0;
+  auto add = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
+    if (i1 <= i0 || j1 <= j0 || k1 <= k0) return;
+    bx.lo[bx.n][0] = i0; bx.lo[bx.n][1] = j0; bx.lo[bx.n][2] = k0;
+    bx.hi[bx.n][0] = i1; bx.hi[bx.n][1] = j1; bx.hi[bx.n][2] = k1;
+    bx.n++;
+  };
+  add(0, lo.x, 0, d.nj, 0, d.nk);
+  add(hi.x, d.ni, 0, d.nj, 0, d.nk);
+  add(lo.x, hi.x, 0, lo.y, 0, d.nk);
+  add(lo.x, hi.x, hi.y, d.nj, 0, d.nk);
+  add(lo.x, hi.x, lo.y, hi.y, 0, lo.z);
+  add(lo.x, hi.x, lo.y, hi.y, hi.z, d.nk);
+  int tot = 0;
+  for (int b = 0; b < bx.n; b++) {
+    bx.start[b] = tot;
+    int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
+    tot += ((nj + 31) / 32) * ((nk + 3) / 4) * ((ni + 1) / 2);
+  }
+  bx.start[bx.n] = tot;
+  if (tot > 0) volume_shell_kernel<FX, FY, FZ><<<tot, dim3(32, 4, 2), 0, s_shell>>>(a, bx);
+}
+
+void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell) {
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: volume_stage_kernel<-1, -1, -1><<<grid, block, 0, s>>>(a); break;
-    case 1: volume_stage_kernel<-1, -1, 1><<<grid, block, 0, s>>>(a); break;
-    case 2: volume_stage_kernel<-1, 1, -1><<<grid, block, 0, s>>>(a); break;
-    case 3: volume_stage_kernel<-1, 1, 1><<<grid, block, 0, s>>>(a); break;
-    case 4: volume_stage_kernel<1, -1, -1><<<grid, block, 0, s>>>(a); break;
-    case 5: volume_stage_kernel<1, -1, 1><<<grid, block, 0, s>>>(a); break;
-    case 6: volume_stage_kernel<1, 1, -1><<<grid, block, 0, s>>>(a); break;
-    default: volume_stage_kernel<1, 1, 1><<<grid, block, 0, s>>>(a); break;
+    case 0: launch_flags<-1, -1, -1>(a, s, s_shell); break;
+    case 1: launch_flags<-1, -1, 1>(a, s, s_shell); break;
+    case 2: launch_flags<-1, 1, -1>(a, s, s_shell); break;
+    case 3: launch_flags<-1, 1, 1>(a, s, s_shell); break;
+    case 4: launch_flags<1, -1, -1>(a, s, s_shell); break;
+    case 5: launch_flags<1, -1, 1>(a, s, s_shell); break;
+    case 6: launch_flags<1, 1, -1>(a, s, s_shell); break;
+    default: launch_flags<1, 1, 1>(a, s, s_shell); break;
   }
 }
 
