@@ -200,6 +200,22 @@ def traffic_per_node():
         return None
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest rank's figure: all-reduce MAX over the process group (identity alone)."""
+    import torch
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(npts, steps, world, seconds):
+    """Whole-job Gpt-steps/s: every rank advances its own replica of npts nodes by steps
+    steps, and the job takes as long as its slowest rank."""
+    return npts * steps * world / seconds / 1e9
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -279,11 +295,8 @@ def main():
     clocks = clk.stop()
     sim.check_finite()
     barrier()
-    t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = npts * args.steps * world / (max_ms / 1e3) / 1e9
+    max_ms = max_over_ranks(total_ms, dist, f"cuda:{local}")
+    value = job_rate(npts, args.steps, world, max_ms / 1e3)
     sim.close()
 
     # ---------------- end to end through the C ABI from pinned host memory
@@ -303,10 +316,7 @@ def main():
     e.synchronize()
     e2e_s = time.perf_counter() - t0
     e.close()
-    t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local}")
     h2d = (hfx.numel() + hst.numel() + (hlay.numel() if hlay is not None else 0)) * 4 / args.steps
     d2h = 8 * nf * 4
 
@@ -323,7 +333,7 @@ def main():
                      "traffic": tpn * npts / 4 if tpn else None,
                      "kernel": "volume phase (interior + shell kernels, band kernel concurrent)", "bytes_per_node_step": ALG_BYTES_PER_NODE_STEP,
                      "volume_phase_ms_per_step": vol_ms / args.steps, "peak_source": peak_kind},
-        "e2e": {"value": npts * args.steps * world / e2e_s / 1e9, "unit": "Gpt-steps/s",
+        "e2e": {"value": job_rate(npts, args.steps, world, e2e_s), "unit": "Gpt-steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "includes": "create + host-array upload + FP64 setup + steps + per-step output fetch"},
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,

@@ -111,7 +111,8 @@ def params_struct(job):
         elif any(name == f[0] for f in DfdParams._fields_):
             cur = getattr(s, name)
             setattr(s, name, int(val) if isinstance(cur, int) else float(val))
-    s.NT = int(float(np.float32(s.TMAX)) / float(np.float32(s.DT)))
+    # NT = (int)((float)TMAX / (float)DT), single-precision division as the library does
+    s.NT = int(np.float32(s.TMAX) / np.float32(s.DT)) if s.DT > 0 else 0
     return s
 
 
