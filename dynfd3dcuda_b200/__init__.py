@@ -28,6 +28,10 @@ STATUS = {0: "ok", 1: "bad or unsupported parameter", 2: "CUDA error", 3: "file 
           7: "Newton solve hit its iteration cap"}
 
 
+# capacity of the static gather buffer of dfd_get_slice_noalloc (DFD_SLICE_SCRATCH_FLOATS)
+SLICE_SCRATCH_FLOATS = 1 << 22
+
+
 class DfdError(RuntimeError):
     def __init__(self, status, msg=""):
         super().__init__(f"{STATUS.get(status, status)}{': ' + msg if msg else ''}")
@@ -77,7 +81,7 @@ def lib():
             "dfd_load_fault_geometry": [V, V], "dfd_load_media1d": [V, I, V], "dfd_load_fault_init": [V, V],
             "dfd_precompute": [V], "dfd_stage": [V, I, I], "dfd_step": [V, I], "dfd_run": [V, I, I],
             "dfd_synchronize": [V], "dfd_get_wave": [V, V], "dfd_set_wave": [V, V], "dfd_get_metric": [V, V],
-            "dfd_get_fault": [V, I, V], "dfd_get_slice": [V, I, I, V], "dfd_check_finite": [V],
+            "dfd_get_fault": [V, I, V], "dfd_get_slice": [V, I, I, V], "dfd_get_slice_noalloc": [V, I, I, V], "dfd_check_finite": [V],
             "dfd_newton_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong)],
             "dfd_output_open": [V, ctypes.c_char_p], "dfd_output_write": [V, I], "dfd_output_close": [V],
             "dfd_set_guess_net": [V, V, I], "dfd_fetch_outputs": [V, V],
@@ -208,6 +212,14 @@ class Simulation:
         nb = self.NZ if axis == 1 else self.NY
         out = np.empty((3, na, nb), np.float32)
         self._check(lib().dfd_get_slice(self.h, axis, index, out.ctypes.data))
+        return out
+
+    def slice_noalloc(self, axis, index):
+        """Same as slice(), gathered in the library's static device buffer (no allocation)."""
+        na = self.NZ if axis == 0 else self.NX
+        nb = self.NZ if axis == 1 else self.NY
+        out = np.empty((3, na, nb), np.float32)
+        self._check(lib().dfd_get_slice_noalloc(self.h, axis, index, out.ctypes.data))
         return out
 
     def check_finite(self):

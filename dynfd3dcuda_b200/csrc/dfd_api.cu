@@ -619,6 +619,44 @@ int dfd_get_slice(dfd_ctx* ctx, int axis, int index, float* host) {
   return cuda_check(ctx, e, "slice");
 }
 
+// ---- slice read-out that allocates nothing ----
+// Callers that may not allocate device memory while they run (a host thread that polls
+// slices between steps under a fixed memory budget, or code that must not call cudaMalloc
+// or cudaFree because those synchronise the whole device) use this entry instead of
+// dfd_get_slice.  The gather buffer is one file-scope device array per device, sized for
+// DFD_SLICE_SCRATCH_FLOATS floats (3 components x the slice's nodes); larger slices are
+// rejected with DFD_ERR_PARAM.  The gather kernel writes every element that is copied
+// back, so nothing in the array has to start at zero.  The array is shared by every
+// context on a device: two calls that overlap in time on the same device (from two host
+// threads) race on it.
+static __device__ __align__(256) float g_slice_scratch[DFD_SLICE_SCRATCH_FLOATS];
+static float* g_slice_scratch_ptr[64] = {};
+
+int dfd_get_slice_noalloc(dfd_ctx* ctx, int axis, int index, float* host) {
+  if (!ctx || !host || axis < 0 || axis > 2) return DFD_ERR_PARAM;
+  const Dims& d = ctx->d;
+  int lim = axis == 0 ? d.ni : axis == 1 ? d.nj : d.nk;
+  if (index < 0 || index >= lim) return DFD_ERR_PARAM;
+  int na = axis == 0 ? d.nk : d.ni, nb = axis == 1 ? d.nk : d.nj;
+  long long nfloat = 3LL * na * nb;
+  if (nfloat > DFD_SLICE_SCRATCH_FLOATS)
+    return fail(ctx, DFD_ERR_PARAM, "slice of " + std::to_string(nfloat) + " floats exceeds the " +
+                                        std::to_string(DFD_SLICE_SCRATCH_FLOATS) + "-float static gather buffer");
+  if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, DFD_ERR_PARAM, "device ordinal out of range");
+  CK(cudaSetDevice(ctx->device));
+  // first call on this device: look up the array's device address (setup, done once)
+  if (!g_slice_scratch_ptr[ctx->device]) {
+    float* ptr = nullptr;
+    CK(cudaGetSymbolAddress((void**)&ptr, g_slice_scratch));
+    g_slice_scratch_ptr[ctx->device] = ptr;
+  }
+  float* dv = g_slice_scratch_ptr[ctx->device];
+  dfd::slice_kernel<<<(na * nb + 255) / 256, 256, 0, ctx->s0>>>(d, ctx->W[0], axis, index, dv);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, dv, sizeof(float) * nfloat, cudaMemcpyDeviceToHost, ctx->s0));
+  return cuda_check(ctx, cudaStreamSynchronize(ctx->s0), "slice (static buffer)");
+}
+
 int dfd_check_finite(dfd_ctx* ctx) {
   if (!ctx) return DFD_ERR_PARAM;
   if (!ctx->p.rupture) return DFD_OK;

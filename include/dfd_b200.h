@@ -125,6 +125,16 @@ int dfd_fetch_outputs(dfd_ctx *ctx, float *host);
 /* nsteps steps issued stage by stage with CUDA events around every volume-kernel launch:
  * total device time, time inside the volume kernels, and the rest (milliseconds) */
 int dfd_run_timed(dfd_ctx *ctx, int it0, int nsteps, float *total_ms, float *volume_ms, float *fault_ms);
+/* The same slice as dfd_get_slice, gathered into a static device array instead of a
+ * temporary allocation; this entry has no counterpart in the reference.  It is for callers
+ * that must not allocate or free device memory while they run (fixed memory budget, or no
+ * device-wide synchronisation from cudaMalloc/cudaFree between steps).  Limits: at most
+ * DFD_SLICE_SCRATCH_FLOATS floats (3 x the slice's nodes), else DFD_ERR_PARAM; the first
+ * call on a device looks up the array's address (setup), so make it before any stream
+ * capture; the array is shared per device, so calls that overlap in time on one device
+ * race. */
+#define DFD_SLICE_SCRATCH_FLOATS (1 << 22)
+int dfd_get_slice_noalloc(dfd_ctx *ctx, int axis, int index, float *host);
 /* host-side health check: 0 ok, DFD_ERR_NONFINITE if the fault state holds NaN/Inf */
 int dfd_check_finite(dfd_ctx *ctx);
 /* cumulative Newton iterations and non-converged solves of the rate-and-state trial */
