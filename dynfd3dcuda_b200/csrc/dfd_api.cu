@@ -12,7 +12,8 @@
 #include "dfd_internal.cuh"
 
 namespace dfd {
-void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell);
+void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
+                         const TileCtx* tc, int bin);
 void launch_fault_node(const FaultArgs& a, cudaStream_t s);
 void launch_fault_band(const FaultArgs& a, cudaStream_t s);
 void launch_fault_coef(const Dims& d, const float* M, float* tab, float* tabf, float* vecn, float* vecs1,
@@ -76,6 +77,9 @@ struct dfd_ctx {
   int* it_dev = nullptr;
   int* flag_dev = nullptr;
   float* guess_net = nullptr;
+  TileCtx tile;                    // tiled interior kernel (TMA maps)
+  int* tile_err = nullptr;
+  bool use_tile = true;
   // host-side inputs
   std::vector<float> fxyz, planes, layers;
   std::vector<double> xl, fx, fy, fz;
@@ -170,7 +174,13 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   d.nx = q.NX + 6; d.ny = q.NY + 6; d.nz = q.NZ + 6;
   d.i0 = d.nx / 2;
   d.N = q.PML_N;
-  d.nxyz = (long long)d.nx * d.ny * d.nz;
+  // row offset: the first interior-box row node (3 ghost nodes + the low y PML slab) on a
+  // 16-byte boundary; pitch a multiple of 8 elements
+  int ylo = 3 + (q.use_pml ? q.PML_N : 0);
+  d.oy = (4 - ylo % 4) % 4;
+  d.py = (d.ny + d.oy + 7) / 8 * 8;
+  d.sx = (long long)d.py * d.nz;
+  d.nxyz = d.sx * d.nx;
   d.nyz = (long long)d.ny * d.nz;
   auto done = [&](int rc) { if (rc) { dfd_destroy(ctx); return rc; } return 0; };
   if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s0, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
@@ -224,7 +234,11 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->it_dev, 1);
   if (!rc) rc = dalloc(ctx, &ctx->flag_dev, 1);
   if (!rc) rc = dalloc(ctx, &ctx->guess_net, 1232);
+  if (!rc) rc = dalloc(ctx, &ctx->tile_err, 1);
   if (rc) { dfd_destroy(ctx); return rc; }
+  // interior box through the TMA-tiled kernel unless DFD_TILE=0 selects the plain kernel
+  const char* tv = getenv("DFD_TILE");
+  ctx->use_tile = !(tv && tv[0] == '0') && tile_setup(&ctx->tile, d, ctx->W, ctx->M, ctx->tile_err, device);
   *out = ctx;
   return DFD_OK;
 }
@@ -492,7 +506,7 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   va.united = p.rupture ? ctx->ipl + I_UNITED * nf : nullptr;
   va.rDH = (float)(1.0 / p.DH); va.rka = rka; va.rkb = rkb;
   va.irk = irk; va.freenode = p.free_surface;
-  launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2);
+  launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk]);
   cudaEventRecord(ctx->ev_join2, ctx->s2);
   if (p.rupture) cudaStreamWaitEvent(ctx->s0, ctx->ev_join, 0);
   cudaStreamWaitEvent(ctx->s0, ctx->ev_join2, 0);
@@ -550,34 +564,51 @@ int dfd_run(dfd_ctx* ctx, int it0, int nsteps) {
 
 int dfd_step(dfd_ctx* ctx, int it) { return dfd_run(ctx, it, 1); }
 
+// error flag of the tiled interior kernel (a TMA copy that did not complete in time)
+static int tile_status(dfd_ctx* ctx) {
+  if (ctx->sticky || !ctx->use_tile) return ctx->sticky;
+  int e = 0;
+  CK(cudaMemcpy(&e, ctx->tile_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) { ctx->sticky = DFD_ERR_CUDA; ctx->err = "tiled interior kernel: a TMA copy did not complete"; }
+  return ctx->sticky;
+}
+
 int dfd_synchronize(dfd_ctx* ctx) {
   if (!ctx) return DFD_ERR_PARAM;
   cudaSetDevice(ctx->device);
   CK(cudaStreamSynchronize(ctx->s0));
   CK(cudaStreamSynchronize(ctx->s1));
   CK(cudaStreamSynchronize(ctx->s2));
-  return ctx->sticky;
+  return tile_status(ctx);
+}
+
+// dense host fields (nf, nx, nz, ny) <-> pitched device fields (nf, nx, nz, py) at offset oy:
+// all nf*nx*nz rows share one pitch, so one 2-D copy moves them
+static int volume_copy(dfd_ctx* ctx, float* host, float* dev, int nf, bool to_host) {
+  const Dims& d = ctx->d;
+  size_t w = sizeof(float) * d.ny, hp = w, dp = sizeof(float) * d.py;
+  size_t rows = (size_t)nf * d.nx * d.nz;
+  if (to_host) CK(cudaMemcpy2D(host, hp, dev + d.oy, dp, w, rows, cudaMemcpyDeviceToHost));
+  else CK(cudaMemcpy2D(dev + d.oy, dp, host, hp, w, rows, cudaMemcpyHostToDevice));
+  return DFD_OK;
 }
 
 int dfd_get_wave(dfd_ctx* ctx, float* host) {
   if (!ctx || !host) return DFD_ERR_PARAM;
   if (ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "wavefield is mid-step");
   CK(cudaStreamSynchronize(ctx->s0));
-  CK(cudaMemcpy(host, ctx->W[0], sizeof(float) * 9 * ctx->d.nxyz, cudaMemcpyDeviceToHost));
-  return DFD_OK;
+  return volume_copy(ctx, host, ctx->W[0], 9, true);
 }
 int dfd_set_wave(dfd_ctx* ctx, const float* host) {
   if (!ctx || !host) return DFD_ERR_PARAM;
   if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
   CK(cudaStreamSynchronize(ctx->s0));
-  CK(cudaMemcpy(ctx->W[0], host, sizeof(float) * 9 * ctx->d.nxyz, cudaMemcpyHostToDevice));
-  return DFD_OK;
+  return volume_copy(ctx, const_cast<float*>(host), ctx->W[0], 9, false);
 }
 int dfd_get_metric(dfd_ctx* ctx, float* host) {
   if (!ctx || !host) return DFD_ERR_PARAM;
   CK(cudaStreamSynchronize(ctx->s0));
-  CK(cudaMemcpy(host, ctx->M, sizeof(float) * 13 * ctx->d.nxyz, cudaMemcpyDeviceToHost));
-  return DFD_OK;
+  return volume_copy(ctx, host, ctx->M, 13, true);
 }
 
 int dfd_get_fault(dfd_ctx* ctx, int field, float* host) {
@@ -720,7 +751,7 @@ int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* vol
   if (total_ms) *total_ms = tot;
   if (volume_ms) *volume_ms = vol;
   if (fault_ms) *fault_ms = tot - vol;
-  return DFD_OK;
+  return tile_status(ctx);
 }
 
 int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {

@@ -495,11 +495,11 @@ __global__ void __launch_bounds__(128) fault_band_kernel(FaultArgs a) {
 #pragma unroll
       for (int s = 0; s < 7; s++) {
         float t[3];
-        trac3(W, M, n, q + (long long)(s - 3) * nyz, 0, t);
+        trac3(W, M, n, q + (long long)(s - 3) * d.sx, 0, t);
         v1[0][s] = t[0]; v1[1][s] = t[1]; v1[2][s] = t[2];
         trac3(W, M, n, q + (s - 3), 3, t);
         v2[0][s] = t[0]; v2[1][s] = t[1]; v2[2][s] = t[2];
-        trac3(W, M, n, q + (long long)(s - 3) * d.ny, 6, t);
+        trac3(W, M, n, q + (long long)(s - 3) * d.py, 6, t);
         v3[0][s] = t[0]; v3[1][s] = t[1]; v3[2][s] = t[2];
       }
 #pragma unroll
@@ -527,19 +527,19 @@ __global__ void __launch_bounds__(128) fault_band_kernel(FaultArgs a) {
       float fm = FW[c * 2 * nyz + pf], fp = FW[c * 2 * nyz + nyz + pf];
       float x;
       if (FX == 1) {
-        if (l == 3) x = G5(wv, q, nyz, 1);
-        else if (l == 2) x = G3(wv, q, nyz, 1);
-        else if (l == 1) x = wv[q + nyz] - wv[q];
+        if (l == 3) x = G5(wv, q, d.sx, 1);
+        else if (l == 2) x = G3(wv, q, d.sx, 1);
+        else if (l == 1) x = wv[q + d.sx] - wv[q];
         else if (l == -1) x = fm - wv[q];
-        else if (l == -2) x = -DFD_C24_1 * wv[q] + DFD_C24_2 * wv[q + nyz] - DFD_C24_3 * fm;
-        else x = -DFD_C1 * wv[q - nyz] - DFD_C2 * wv[q] + DFD_C3 * wv[q + nyz] - DFD_C4 * wv[q + 2 * nyz] + DFD_C5 * fm;
+        else if (l == -2) x = -DFD_C24_1 * wv[q] + DFD_C24_2 * wv[q + d.sx] - DFD_C24_3 * fm;
+        else x = -DFD_C1 * wv[q - d.sx] - DFD_C2 * wv[q] + DFD_C3 * wv[q + d.sx] - DFD_C4 * wv[q + 2 * d.sx] + DFD_C5 * fm;
       } else {
-        if (l == -3) x = G5(wv, q, nyz, -1);
-        else if (l == -2) x = G3(wv, q, nyz, -1);
-        else if (l == -1) x = wv[q] - wv[q - nyz];
+        if (l == -3) x = G5(wv, q, d.sx, -1);
+        else if (l == -2) x = G3(wv, q, d.sx, -1);
+        else if (l == -1) x = wv[q] - wv[q - d.sx];
         else if (l == 1) x = wv[q] - fp;
-        else if (l == 2) x = DFD_C24_3 * fp - DFD_C24_2 * wv[q - nyz] + DFD_C24_1 * wv[q];
-        else x = -DFD_C5 * fp + DFD_C4 * wv[q - 2 * nyz] - DFD_C3 * wv[q - nyz] + DFD_C2 * wv[q] + DFD_C1 * wv[q + nyz];
+        else if (l == 2) x = DFD_C24_3 * fp - DFD_C24_2 * wv[q - d.sx] + DFD_C24_1 * wv[q];
+        else x = -DFD_C5 * fp + DFD_C4 * wv[q - 2 * d.sx] - DFD_C3 * wv[q - d.sx] + DFD_C2 * wv[q] + DFD_C1 * wv[q + d.sx];
       }
       X[c] = x * r;
       Y[c] = G5(wv, q, 1, FY) * r;
@@ -556,9 +556,9 @@ __global__ void __launch_bounds__(128) fault_band_kernel(FaultArgs a) {
       for (int c = 0; c < 3; c++) {
         const float* wv = W + c * n;
         float zz;
-        if (a.freenode && km == 2) zz = G2(wv, q, d.ny, FZ);
-        else if (a.freenode && km == 3) zz = G3(wv, q, d.ny, FZ);
-        else zz = G5(wv, q, d.ny, FZ);
+        if (a.freenode && km == 2) zz = G2(wv, q, d.py, FZ);
+        else if (a.freenode && km == 3) zz = G3(wv, q, d.py, FZ);
+        else zz = G5(wv, q, d.py, FZ);
         Z[c] = zz * r;
       }
     }

@@ -2,15 +2,16 @@
 // B200 dynamic-rupture time step.
 //
 // HBM layout (per context, all FP32 unless noted):
-//   W[4]      four 9-field volume buffers (nx, nz, ny), y fastest, 3 ghost nodes;
+//   W[4]      four 9-field volume buffers (nx, nz, py), y fastest, 3 ghost nodes;
 //             a step cycles A -> B -> C -> B -> A so that the stencil input of a stage is
 //             never written during that stage and no right-hand-side array exists
-//   M         13 fields xix xiy xiz etx ety etz ztx zty ztz jac lam mu rho
+//   M         13 fields xix xiy xiz etx ety etz ztx zty ztz jac lam mu rho, same layout
 //   aux       per PML face, 3 buffers (current, step start, RK accumulator) of 9 fields
 //   FW[2]     split-node state ping-pong (9, 2, nz, ny); Fm / Ft RK registers
 //   tables    fault coefficient tables as planes [table][element][nz*ny] (coalesced)
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace dfd {
@@ -44,12 +45,20 @@ enum Tab {
 // free-surface row tables, 9 elements per j
 enum TabF { TF_VX2VZ1 = 0, TF_VY2VZ1, TF_VX2VZ2, TF_VY2VZ2, TF_P2M1, TF_P2M2, TF_P2M3, TF_M2P1, TF_M2P2, TF_M2P3, NTABF };
 
+// Volume fields are stored with a padded row pitch: node (i, j, k) (padded indices, 3 ghost
+// nodes per side) of a field sits at element (j + oy) + k*py + i*sx.  The row offset oy puts
+// the first node of the interior box (outside the PML) on a 16-byte boundary and the pitch
+// py >= ny + oy is a multiple of 8, as tiled TMA loads need.  Fault-plane arrays keep the
+// dense (nz, ny) layout.
 struct Dims {
   int ni, nj, nk;       // interior sizes NX NY NZ
   int nx, ny, nz;       // padded sizes
   int i0;               // padded x index of the fault plane (nx/2)
   int N;                // PML thickness
-  long long nxyz, nyz;  // field strides
+  int py, oy;           // volume row pitch and row offset (elements)
+  long long sx;         // volume x stride, py * nz
+  long long nxyz;       // volume field size, sx * nx
+  long long nyz;        // fault-plane size, ny * nz
 };
 
 // Arguments of the fused volume stage kernel.
@@ -143,8 +152,30 @@ struct GridArgs {
   double lam1, mu1, rho1, lam2, mu2, rho2;
 };
 
+// TMA tensor maps handed to the tiled interior kernel (dfd_tile.cu)
+struct TileMaps {
+  CUtensorMap win;  // stencil input, halo box
+  CUtensorMap w0;   // step-start state, pointwise box
+  CUtensorMap t;    // RK accumulator, pointwise box
+  CUtensorMap m9;   // metric, fields 0..8
+  CUtensorMap m3;   // lam mu rho, fields 10..12
+};
+// Per-context state of the tiled interior kernel: maps of the four volume buffers and of
+// the metric (fixed addresses, encoded once), the error flag, the SM count.
+struct TileCtx {
+  CUtensorMap halo[4];
+  CUtensorMap centre[4];
+  CUtensorMap m9, m3;
+  int* err = nullptr;
+  int nsm = 0;
+  bool ok = false;
+};
+bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* M, int* err, int device);
+bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi,
+                 cudaStream_t s);
+
 __host__ __device__ inline long long idx3(const Dims& d, int i, int j, int k) {
-  return (long long)j + (long long)k * d.ny + (long long)i * d.nyz;
+  return (long long)(j + d.oy) + (long long)k * d.py + (long long)i * d.sx;
 }
 
 }  // namespace dfd

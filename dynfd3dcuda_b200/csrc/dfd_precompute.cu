@@ -69,7 +69,7 @@ __global__ void fault_coef_kernel(Dims d, const float* __restrict__ M, float* ta
   }
   double lamf[2], muf[2];
   for (int m = 0; m < 2; m++) {
-    long long qm = q + (m == 0 ? -nyz : nyz);
+    long long qm = q + (m == 0 ? -d.sx : d.sx);
     rhof[m * nyz + f] = M[12 * n + qm];
     lamf[m] = M[10 * n + qm];
     muf[m] = M[11 * n + qm];

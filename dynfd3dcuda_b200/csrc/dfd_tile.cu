@@ -1,0 +1,373 @@
+// Interior volume stage staged through shared memory by TMA.
+//
+// The interior box (outside every PML slab, below the free-surface rows) is cut into
+// tiles of 32 (y) x 8 (z) nodes; a CTA owns one tile column and marches along x over a
+// chunk of planes.  Per plane it needs
+//   - the stencil input (9 fields) of the planes x-1..x+3 (forward x operator) or
+//     x-3..x+1 (backward), with a y/z halo on the current plane: one 4-D TMA box
+//     (40 y, 12 z, 1 x, 9 fields) per plane, held in a ring of NS plane slots;
+//   - the pointwise streams of the node: 12 metric/media fields, and the RK registers
+//     W0 (stages 1, 2) and T (stages 1..3): TMA boxes (32, 8, 1, n) in a ring of NP slots.
+// One elected thread issues the copies ahead of the consumers (mbarrier completion), so
+// HBM traffic is in flight while the 8 warps evaluate the stencils from shared memory
+// with immediate offsets.  Outputs (Wout, T) are written straight from registers.
+//
+// The kernel is persistent: one CTA per SM walks its units (tile column x chunk) and the
+// copy stream runs across unit boundaries, so the next unit's planes arrive while the
+// current one finishes.
+//
+// The right-hand side is the one of the interior kernel in dfd_volume.cu (reference
+// wave.cu:8-204 with rk4.cu:20-33): same operators, metric terms and RK update.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
+#include "dfd_internal.cuh"
+
+namespace dfd {
+
+namespace {
+constexpr int TJ = 32, TK = 8, NTHR = TJ * TK;
+constexpr int HW = TJ + 8;           // halo box width (y): 4 nodes each side (16-byte aligned)
+constexpr int HH = TK + 4;           // halo box height (z): 1 + 3 rows, side set by the z operator
+constexpr int HBOX = HW * HH;        // floats per field of a halo box
+constexpr int HSLOT = 9 * HBOX;      // floats per stencil plane slot
+constexpr int PB = TJ * TK;          // floats per field of a pointwise box
+constexpr int PSLOT = 30 * PB;       // metric 9 + lam mu rho + W0 9 + T 9
+constexpr int NS = 7, NP = 3;        // ring depths (stencil planes, pointwise planes)
+constexpr size_t SMEM_BYTES = (size_t)(NS * HSLOT + NP * PSLOT) * 4 + (NS + NP) * 8;
+constexpr long long WAIT_LIMIT = 1LL << 22;  // polls of one mbarrier before giving up
+static_assert(SMEM_BYTES <= 232448, "tile ring exceeds the shared memory of one CTA");
+static_assert((HSLOT * 4) % 128 == 0 && (PSLOT * 4) % 128 == 0 && (PB * 4) % 128 == 0, "slot alignment");
+}  // namespace
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the completion of phase `parity`; false if it did not complete
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+  for (long long n = 0; n < WAIT_LIMIT; n++)
+    if (mbar_try(b, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load4(float* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                          uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(b))
+      : "memory");
+}
+
+// one-sided 5-point operators on values (v0..v4 = the five stencil points in order)
+template <int F>
+__device__ __forceinline__ float d5v(float v0, float v1, float v2, float v3, float v4) {
+  if (F == 1) return -DFD_C1 * v0 - DFD_C2 * v1 + DFD_C3 * v2 - DFD_C4 * v3 + DFD_C5 * v4;
+  else return -DFD_C5 * v0 + DFD_C4 * v1 - DFD_C3 * v2 + DFD_C2 * v3 + DFD_C1 * v4;
+}
+// on a shared-memory line through p with stride S (forward: p-S..p+3S, backward: p-3S..p+S)
+template <int F, int S>
+__device__ __forceinline__ float d5s(const float* p) {
+  if (F == 1) return d5v<1>(p[-S], p[0], p[S], p[2 * S], p[3 * S]);
+  else return d5v<-1>(p[-3 * S], p[-2 * S], p[-S], p[0], p[S]);
+}
+
+struct TileSched {
+  int lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;  // interior box, interior indices, half open
+  int ntj, ntk, ci, nunits;               // tiles in y and z, planes per chunk, units
+};
+
+// x derivative of field f (offset o inside the plane slots)
+#define DFD_DX(F_, o) d5v<F_>(xs0[o], xs1[o], xs2[o], xs3[o], xs4[o])
+
+// 256 threads with at most 128 registers, so that a block of the shell kernel fits beside
+// the CTA on its SM
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(NTHR, 2)
+    volume_tile_kernel(const __grid_constant__ TileMaps mp, const VolArgs a, const TileSched sc, int* err) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  float* win = reinterpret_cast<float*>(smraw);
+  float* pw = win + NS * HSLOT;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(pw + NP * PSLOT);
+  const Dims& d = a.d;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  constexpr int XLO = FX == 1 ? -1 : -3;  // first stencil plane relative to x
+  constexpr int RZ = FZ == 1 ? 1 : 3;     // row of the tile's first z node inside the halo box
+  const int irk = a.irk;
+  const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1;
+  const unsigned ptx = (12 + (needW0 ? 9 : 0) + (needT ? 9 : 0)) * PB * 4;
+  const int ntile = sc.ntj * sc.ntk;
+  const int G = gridDim.x;
+
+  if (tid == 0) {
+    for (int s = 0; s < NS + NP; s++) mbar_init(bar + s, 1);
+    fence_async_shared();
+  }
+  __syncthreads();
+
+  // copy-issue state (used by thread 0 only)
+  int wu = blockIdx.x, wo = 0, pu = blockIdx.x, po = 0;
+  long long wn = 0, pn = 0, relW = 0, relP = 0;
+  auto produce = [&]() {
+    while (wu < sc.nunits && wn < relW + NS) {
+      int tc = wu / ntile, r = wu % ntile;
+      int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
+      int j0 = sc.lo_y + (r % sc.ntj) * TJ, k0 = sc.lo_z + (r / sc.ntj) * TK;
+      int slot = (int)(wn % NS);
+      mbar_expect_tx(bar + slot, HSLOT * 4);
+      tma_load4(win + slot * HSLOT, &mp.win, j0 + 3 + d.oy - 4, k0 + 3 - RZ, ib + XLO + wo + 3, 0, bar + slot);
+      wn++;
+      if (++wo == ie - ib + 4) { wo = 0; wu += G; }
+    }
+    while (pu < sc.nunits && pn < relP + NP) {
+      int tc = pu / ntile, r = pu % ntile;
+      int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
+      int j0 = sc.lo_y + (r % sc.ntj) * TJ, k0 = sc.lo_z + (r / sc.ntj) * TK;
+      int slot = (int)(pn % NP);
+      uint64_t* b = bar + NS + slot;
+      float* dst = pw + slot * PSLOT;
+      int c0 = j0 + 3 + d.oy, c1 = k0 + 3, c2 = ib + po + 3;
+      mbar_expect_tx(b, ptx);
+      tma_load4(dst, &mp.m9, c0, c1, c2, 0, b);
+      tma_load4(dst + 9 * PB, &mp.m3, c0, c1, c2, 10, b);
+      if (needW0) tma_load4(dst + 12 * PB, &mp.w0, c0, c1, c2, 0, b);
+      if (needT) tma_load4(dst + 21 * PB, &mp.t, c0, c1, c2, 0, b);
+      pn++;
+      if (++po == ie - ib) { po = 0; pu += G; }
+    }
+  };
+  if (tid == 0) produce();
+
+  const long long n = d.nxyz;
+  const float r = a.rDH;
+  const int hc = (ty + RZ) * HW + tx + 4;  // node inside a halo field box
+  const int pc = ty * TJ + tx;             // node inside a pointwise field box
+  long long wbase = 0, waited = 0, step = 0;
+  int bad = 0;
+  for (int u = blockIdx.x; u < sc.nunits; u += G) {
+    const int tc = u / ntile, ru = u % ntile;
+    const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
+    const int j = sc.lo_y + (ru % sc.ntj) * TJ + tx, k = sc.lo_z + (ru / sc.ntj) * TK + ty;
+    const bool active = j < sc.hi_y && k < sc.hi_z;
+    const bool band = active && a.united && !a.united[j + k * d.nj];
+    float dyz = 1.0f;
+    if (active && a.dampx) dyz = fminf(__ldg(a.dampy + j + 3), __ldg(a.dampz + k + 3));
+    const long long qyz = idx3(d, 0, j + 3, k + 3);
+    const int nst = ie - ib;
+    for (int s = 0; s < nst; s++) {
+      for (const long long top = wbase + s + 4; waited <= top; waited++)
+        bad |= !mbar_wait(bar + (int)(waited % NS), (unsigned)((waited / NS) & 1));
+      bad |= !mbar_wait(bar + NS + (int)(step % NP), (unsigned)((step / NP) & 1));
+      const int i = ib + s;
+      if (active && !bad && !(band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3)) {
+        const float* xs0 = win + (int)((wbase + s) % NS) * HSLOT + hc;
+        const float* xs1 = win + (int)((wbase + s + 1) % NS) * HSLOT + hc;
+        const float* xs2 = win + (int)((wbase + s + 2) % NS) * HSLOT + hc;
+        const float* xs3 = win + (int)((wbase + s + 3) % NS) * HSLOT + hc;
+        const float* xs4 = win + (int)((wbase + s + 4) % NS) * HSLOT + hc;
+        const float* cur = FX == 1 ? xs1 : xs3;  // plane x itself
+        const float* P = pw + (int)(step % NP) * PSLOT + pc;
+        const float lam = P[9 * PB], mu = P[10 * PB];
+        const float rrho = 1.0f / P[11 * PB];
+        const float l2m = lam + 2.0f * mu;
+        float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f, h8 = 0.f;
+#define DFD_TAXIS(DER, MO)                                                                          \
+  {                                                                                                 \
+    const float e0 = P[(MO) * PB], e1 = P[((MO) + 1) * PB], e2 = P[((MO) + 2) * PB];                 \
+    float dv;                                                                                       \
+    dv = DER(0) * r;                                                                                \
+    h3 += dv * e0 * l2m; h4 += dv * e0 * lam; h5 += dv * e0 * lam; h6 += dv * e1 * mu; h7 += dv * e2 * mu; \
+    dv = DER(1) * r;                                                                                \
+    h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h6 += dv * e0 * mu; h8 += dv * e2 * mu; \
+    dv = DER(2) * r;                                                                                \
+    h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h7 += dv * e0 * mu; h8 += dv * e1 * mu; \
+    const float er0 = e0 * rrho, er1 = e1 * rrho, er2 = e2 * rrho;                                  \
+    dv = DER(3) * r; h0 += dv * er0;                                                                \
+    dv = DER(4) * r; h1 += dv * er1;                                                                \
+    dv = DER(5) * r; h2 += dv * er2;                                                                \
+    dv = DER(6) * r; h0 += dv * er1; h1 += dv * er0;                                                \
+    dv = DER(7) * r; h0 += dv * er2; h2 += dv * er0;                                                \
+    dv = DER(8) * r; h1 += dv * er2; h2 += dv * er1;                                                \
+  }
+#define DFD_DERX(f) DFD_DX(FX, (f) * HBOX)
+#define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HBOX)
+#define DFD_DERZ(f) d5s<FZ, HW>(cur + (f) * HBOX)
+        DFD_TAXIS(DFD_DERX, 0)
+        DFD_TAXIS(DFD_DERY, 3)
+        DFD_TAXIS(DFD_DERZ, 6)
+#undef DFD_DERX
+#undef DFD_DERY
+#undef DFD_DERZ
+#undef DFD_TAXIS
+        const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
+        const float hv[9] = {h0, h1, h2, h3, h4, h5, h6, h7, h8};
+        const long long q = qyz + (long long)(i + 3) * d.sx;
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+          const long long x = f * n + q;
+          float w;
+          if (irk == 0) {
+            const float w0 = cur[f * HBOX];
+            a.T[x] = fmaf(a.rkb, hv[f], w0);
+            w = fmaf(a.rka, hv[f], w0);
+          } else if (irk < 3) {
+            a.T[x] = fmaf(a.rkb, hv[f], P[(21 + f) * PB]);
+            w = fmaf(a.rka, hv[f], P[(12 + f) * PB]);
+          } else {
+            w = fmaf(a.rkb, hv[f], P[(21 + f) * PB]);
+          }
+          a.Wout[x] = w * damp;
+        }
+      }
+      if (__syncthreads_or(bad)) {
+        // a copy did not arrive in time: flag it, let the copies in flight land, leave
+        if (tid == 0) {
+          atomicExch(err, 1);
+          for (int sl = 0; sl < NS; sl++) {
+            long long last = wn - 1 - ((wn - 1 - sl) % NS + NS) % NS;  // newest load into slot sl
+            if (last >= 0 && last % NS == sl) mbar_wait(bar + sl, (unsigned)((last / NS) & 1));
+          }
+          for (int sl = 0; sl < NP; sl++) {
+            long long last = pn - 1 - ((pn - 1 - sl) % NP + NP) % NP;
+            if (last >= 0 && last % NP == sl) mbar_wait(bar + NS + sl, (unsigned)((last / NP) & 1));
+          }
+        }
+        return;
+      }
+      relW = (s == nst - 1) ? wbase + nst + 4 : wbase + s + 1;
+      relP = ++step;
+      if (tid == 0) {
+        fence_async_shared();
+        produce();
+      }
+    }
+    wbase += nst + 4;
+  }
+}
+#undef DFD_DX
+
+// ---------------- host side
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 4-D map over nf fields of the volume layout (py, nz, nx, nf) with box (bw, bh, 1, bf)
+static bool make_map(CUtensorMap* m, const Dims& d, const float* base, int nf, int bw, int bh, int bf) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[4] = {(cuuint64_t)d.py, (cuuint64_t)d.nz, (cuuint64_t)d.nx, (cuuint64_t)nf};
+  cuuint64_t strides[3] = {(cuuint64_t)d.py * 4, (cuuint64_t)d.sx * 4, (cuuint64_t)d.nxyz * 4};
+  cuuint32_t box[4] = {(cuuint32_t)bw, (cuuint32_t)bh, 1, (cuuint32_t)bf};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int FX, int FY, int FZ>
+static bool set_smem() {
+  return cudaFuncSetAttribute(volume_tile_kernel<FX, FY, FZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)SMEM_BYTES) == cudaSuccess;
+}
+
+bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* M, int* err, int device) {
+  tc->ok = false;
+  tc->err = err;
+  if (cudaDeviceGetAttribute(&tc->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return false;
+  // the tile's halo box must start on a 16-byte boundary: (first interior row node) % 4 == 0
+  bool ok = true;
+  for (int b = 0; b < 4 && ok; b++) {
+    ok = make_map(&tc->halo[b], d, W[b], 9, HW, HH, 9);
+    ok = ok && make_map(&tc->centre[b], d, W[b], 9, TJ, TK, 9);
+  }
+  ok = ok && make_map(&tc->m9, d, M, 13, TJ, TK, 9);
+  ok = ok && make_map(&tc->m3, d, M, 13, TJ, TK, 3);
+  ok = ok && set_smem<-1, -1, -1>() && set_smem<-1, -1, 1>() && set_smem<-1, 1, -1>() && set_smem<-1, 1, 1>();
+  ok = ok && set_smem<1, -1, -1>() && set_smem<1, -1, 1>() && set_smem<1, 1, -1>() && set_smem<1, 1, 1>();
+  tc->ok = ok;
+  cudaGetLastError();  // a failed attribute call leaves no sticky error; clear it
+  return ok;
+}
+
+// Chunking of the x range: minimise the busiest CTA's plane loads, ceil(units / grid) x
+// (planes per chunk + 4 halo planes).
+static TileSched plan(const Dims& d, int3 lo, int3 hi, int nsm, int* grid) {
+  TileSched s;
+  s.lo_x = lo.x; s.lo_y = lo.y; s.lo_z = lo.z; s.hi_x = hi.x; s.hi_y = hi.y; s.hi_z = hi.z;
+  s.ntj = (hi.y - lo.y + TJ - 1) / TJ;
+  s.ntk = (hi.z - lo.z + TK - 1) / TK;
+  int nx = hi.x - lo.x, ntile = s.ntj * s.ntk;
+  long long best = -1;
+  for (int nch = 1; nch <= 64 && nch <= nx; nch++) {
+    int ci = (nx + nch - 1) / nch;
+    int nchr = (nx + ci - 1) / ci;
+    long long units = (long long)ntile * nchr;
+    long long g = std::min<long long>(units, nsm);
+    long long cost = (units + g - 1) / g * (ci + 4);
+    if (best < 0 || cost < best) { best = cost; s.ci = ci; s.nunits = (int)units; *grid = (int)g; }
+  }
+  (void)d;
+  return s;
+}
+
+template <int FX, int FY, int FZ>
+static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
+  TileMaps mp;
+  mp.win = tc.halo[bin];
+  mp.w0 = tc.centre[0];
+  mp.t = tc.centre[3];
+  mp.m9 = tc.m9;
+  mp.m3 = tc.m3;
+  int grid = 0;
+  TileSched sc = plan(a.d, lo, hi, tc.nsm, &grid);
+  volume_tile_kernel<FX, FY, FZ><<<grid, NTHR, SMEM_BYTES, s>>>(mp, a, sc, tc.err);
+}
+
+// true when the tiled kernel took the interior box
+bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi,
+                 cudaStream_t s) {
+  if (!tc || !tc->ok) return false;
+  if ((lo.y + 3 + a.d.oy) % 4 != 0 || lo.z < 0 || hi.x <= lo.x || hi.y <= lo.y || hi.z <= lo.z) return false;
+  int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: launch_t<-1, -1, -1>(*tc, a, bin, lo, hi, s); break;
+    case 1: launch_t<-1, -1, 1>(*tc, a, bin, lo, hi, s); break;
+    case 2: launch_t<-1, 1, -1>(*tc, a, bin, lo, hi, s); break;
+    case 3: launch_t<-1, 1, 1>(*tc, a, bin, lo, hi, s); break;
+    case 4: launch_t<1, -1, -1>(*tc, a, bin, lo, hi, s); break;
+    case 5: launch_t<1, -1, 1>(*tc, a, bin, lo, hi, s); break;
+    case 6: launch_t<1, 1, -1>(*tc, a, bin, lo, hi, s); break;
+    default: launch_t<1, 1, 1>(*tc, a, bin, lo, hi, s); break;
+  }
+  return true;
+}
+
+}  // namespace dfd

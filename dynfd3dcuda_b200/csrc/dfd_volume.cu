@@ -123,7 +123,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 
   // ---- x ----
 #pragma unroll
-  for (int f = 0; f < 9; f++) dv[f] = d5<FX>(W + f * n, q, d.nyz) * a.rDH;
+  for (int f = 0; f < 9; f++) dv[f] = d5<FX>(W + f * n, q, d.sx) * a.rDH;
   dxv[0] = dv[0]; dxv[1] = dv[1]; dxv[2] = dv[2];
   axis_terms(dv, __ldg(M + q), __ldg(M + n + q), __ldg(M + 2 * n + q), lam, mu, rrho, D);
 #pragma unroll
@@ -163,7 +163,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
   }
   // ---- z ----
 #pragma unroll
-  for (int f = 0; f < 9; f++) dv[f] = d5<FZ>(W + f * n, q, d.ny) * a.rDH;
+  for (int f = 0; f < 9; f++) dv[f] = d5<FZ>(W + f * n, q, d.py) * a.rDH;
   float Dz_plain[9];
   axis_terms(dv, ez0, ez1, ez2, lam, mu, rrho, Dz_plain);
 #pragma unroll
@@ -182,14 +182,14 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 #pragma unroll
       for (int r = 0; r < 3; r++) {
         const float* v = W + r * n;
-        dz[r] = (FZ == 1 ? (__ldg(v + q + d.ny) - __ldg(v + q)) : (__ldg(v + q) - __ldg(v + q - d.ny))) * a.rDH;
+        dz[r] = (FZ == 1 ? (__ldg(v + q + d.py) - __ldg(v + q)) : (__ldg(v + q) - __ldg(v + q - d.py))) * a.rDH;
       }
     } else {
 #pragma unroll
       for (int r = 0; r < 3; r++) {
         const float* v = W + r * n;
-        dz[r] = (FZ == 1 ? (-DFD_C24_1 * __ldg(v + q) + DFD_C24_2 * __ldg(v + q + d.ny) - DFD_C24_3 * __ldg(v + q + 2 * d.ny))
-                         : (DFD_C24_3 * __ldg(v + q - 2 * d.ny) - DFD_C24_2 * __ldg(v + q - d.ny) + DFD_C24_1 * __ldg(v + q))) *
+        dz[r] = (FZ == 1 ? (-DFD_C24_1 * __ldg(v + q) + DFD_C24_2 * __ldg(v + q + d.py) - DFD_C24_3 * __ldg(v + q + 2 * d.py))
+                         : (DFD_C24_3 * __ldg(v + q - 2 * d.py) - DFD_C24_2 * __ldg(v + q - d.py) + DFD_C24_1 * __ldg(v + q))) *
                 a.rDH;
       }
     }
@@ -217,9 +217,9 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
     float v1[3][7], v2[3][7], v3[3][7];
 #pragma unroll
     for (int l = 0; l < 7; l++) {
-      traction(W, M, n, q + (l - 3) * d.nyz, 0, v1[0][l], v1[1][l], v1[2][l]);
+      traction(W, M, n, q + (l - 3) * d.sx, 0, v1[0][l], v1[1][l], v1[2][l]);
       traction(W, M, n, q + (l - 3), 3, v2[0][l], v2[1][l], v2[2][l]);
-      traction(W, M, n, q + (long long)(l - 3) * d.ny, 6, v3[0][l], v3[1][l], v3[2][l]);
+      traction(W, M, n, q + (long long)(l - 3) * d.py, 6, v3[0][l], v3[1][l], v3[2][l]);
     }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -256,10 +256,14 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 
 
 // Shell kernel: the general update on up to six boxes (PML slabs, free-surface rows) that
-// surround the interior box; one 1-D grid of (32, 4, 2) blocks is split over the boxes.
+// surround the interior box; one 1-D grid of 256-thread blocks is split over the boxes.
+// A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z, 2 x) per block; a
+// thinner box (the y slabs of the PML, the free-surface rows) is flattened over (y, z) with y fastest, so that no thread
+// idles and the y-face PML state (y fastest over N nodes, then z) is read contiguously.
 struct Boxes {
   int n;
   int lo[6][3], hi[6][3];  // (i, j, k) interior-index bounds, half open
+  int thin[6];             // flattened (y, z) mapping
   int start[7];            // first block of each box
 };
 
@@ -269,10 +273,22 @@ __global__ void __launch_bounds__(256, 2) volume_shell_kernel(VolArgs a, Boxes b
   while (b + 1 < bx.n && (int)blockIdx.x >= bx.start[b + 1]) b++;
   int loc = blockIdx.x - bx.start[b];
   int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
-  int gj = (nj + 31) / 32, gk = (nk + 3) / 4;
-  int bj = loc % gj, bk = (loc / gj) % gk, bi = loc / (gj * gk);
-  int j = bj * 32 + threadIdx.x, k = bk * 4 + threadIdx.y, i = bi * 2 + threadIdx.z;
-  if (i >= ni || j >= nj || k >= nk) return;
+  int i, j, k;
+  if (bx.thin[b]) {
+    int gyz = (nj * nk + 255) / 256;
+    int t = (loc % gyz) * 256 + threadIdx.x;
+    i = loc / gyz;
+    j = t % nj;
+    k = t / nj;
+    if (k >= nk) return;
+  } else {
+    int gj = (nj + 31) / 32, gk = (nk + 3) / 4;
+    int bj = loc % gj, bk = (loc / gj) % gk, bi = loc / (gj * gk);
+    j = bj * 32 + (threadIdx.x & 31);
+    k = bk * 4 + ((threadIdx.x >> 5) & 3);
+    i = bi * 2 + (threadIdx.x >> 7);
+    if (i >= ni || j >= nj || k >= nk) return;
+  }
   volume_point_general<FX, FY, FZ>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
 }
 
@@ -308,9 +324,9 @@ __device__ __forceinline__ void interior_point(const VolArgs& a, long long q, fl
     dv = d5<F>(W + 7 * n, q, S) * r; h0 += dv * er2; h2 += dv * er0;                               \
     dv = d5<F>(W + 8 * n, q, S) * r; h1 += dv * er2; h2 += dv * er1;                               \
   }
-  DFD_AXIS(FX, a.d.nyz, 0)
+  DFD_AXIS(FX, a.d.sx, 0)
   DFD_AXIS(FY, 1, 3)
-  DFD_AXIS(FZ, a.d.ny, 6)
+  DFD_AXIS(FZ, a.d.py, 6)
 #undef DFD_AXIS
   float hv[9] = {h0, h1, h2, h3, h4, h5, h6, h7, h8};
 #pragma unroll
@@ -342,7 +358,7 @@ __global__ void __launch_bounds__(256, 3) volume_interior_kernel(VolArgs a, int3
   float dyz = 1.0f;
   if (a.dampx) dyz = fminf(__ldg(a.dampy + j + 3), __ldg(a.dampz + k + 3));
   long long q = idx3(d, ib + 3, j + 3, k + 3);
-  for (int i = ib; i < ie; i++, q += d.nyz) {
+  for (int i = ib; i < ie; i++, q += d.sx) {
     if (band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3) continue;
     float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
     interior_point<FX, FY, FZ>(a, q, damp);
@@ -350,7 +366,7 @@ __global__ void __launch_bounds__(256, 3) volume_interior_kernel(VolArgs a, int3
 }
 
 template <int FX, int FY, int FZ>
-static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell) {
+static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin) {
   const Dims& d = a.d;
   // interior box: outside every PML slab and below the free-surface rows
   int nx0 = a.aux[0] ? d.N : 0, nx1 = a.aux[1] ? d.N : 0;
@@ -358,7 +374,7 @@ static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell)
   int nz0 = a.aux[4] ? d.N : 0, nz1 = a.aux[5] ? d.N : (a.freenode ? 3 : 0);
   int3 lo = make_int3(nx0, ny0, nz0), hi = make_int3(d.ni - nx1, d.nj - ny1, d.nk - nz1);
   const int chunk = 8;
-  if (hi.x > lo.x && hi.y > lo.y && hi.z > lo.z) {
+  if (hi.x > lo.x && hi.y > lo.y && hi.z > lo.z && !launch_tile(tc, a, FX, FY, FZ, bin, lo, hi, s)) {
     dim3 block(32, 8, 1);
     dim3 grid((hi.y - lo.y + 31) / 32, (hi.z - lo.z + 7) / 8, (hi.x - lo.x + chunk - 1) / chunk);
     volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, lo, hi, chunk);
@@ -381,23 +397,25 @@ static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell)
   for (int b = 0; b < bx.n; b++) {
     bx.start[b] = tot;
     int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
-    tot += ((nj + 31) / 32) * ((nk + 3) / 4) * ((ni + 1) / 2);
+    bx.thin[b] = nj < 32 || nk < 4;
+    tot += bx.thin[b] ? ((nj * nk + 255) / 256) * ni : ((nj + 31) / 32) * ((nk + 3) / 4) * ((ni + 1) / 2);
   }
   bx.start[bx.n] = tot;
-  if (tot > 0) volume_shell_kernel<FX, FY, FZ><<<tot, dim3(32, 4, 2), 0, s_shell>>>(a, bx);
+  if (tot > 0) volume_shell_kernel<FX, FY, FZ><<<tot, 256, 0, s_shell>>>(a, bx);
 }
 
-void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell) {
+void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
+                         const TileCtx* tc, int bin) {
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: launch_flags<-1, -1, -1>(a, s, s_shell); break;
-    case 1: launch_flags<-1, -1, 1>(a, s, s_shell); break;
-    case 2: launch_flags<-1, 1, -1>(a, s, s_shell); break;
-    case 3: launch_flags<-1, 1, 1>(a, s, s_shell); break;
-    case 4: launch_flags<1, -1, -1>(a, s, s_shell); break;
-    case 5: launch_flags<1, -1, 1>(a, s, s_shell); break;
-    case 6: launch_flags<1, 1, -1>(a, s, s_shell); break;
-    default: launch_flags<1, 1, 1>(a, s, s_shell); break;
+    case 0: launch_flags<-1, -1, -1>(a, s, s_shell, tc, bin); break;
+    case 1: launch_flags<-1, -1, 1>(a, s, s_shell, tc, bin); break;
+    case 2: launch_flags<-1, 1, -1>(a, s, s_shell, tc, bin); break;
+    case 3: launch_flags<-1, 1, 1>(a, s, s_shell, tc, bin); break;
+    case 4: launch_flags<1, -1, -1>(a, s, s_shell, tc, bin); break;
+    case 5: launch_flags<1, -1, 1>(a, s, s_shell, tc, bin); break;
+    case 6: launch_flags<1, 1, -1>(a, s, s_shell, tc, bin); break;
+    default: launch_flags<1, 1, 1>(a, s, s_shell, tc, bin); break;
   }
 }
 
