@@ -174,10 +174,9 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   d.nx = q.NX + 6; d.ny = q.NY + 6; d.nz = q.NZ + 6;
   d.i0 = d.nx / 2;
   d.N = q.PML_N;
-  // row offset: the first interior-box row node (3 ghost nodes + the low y PML slab) on a
-  // 16-byte boundary; pitch a multiple of 8 elements
-  int ylo = 3 + (q.use_pml ? q.PML_N : 0);
-  d.oy = (4 - ylo % 4) % 4;
+  // row offset 1: the first interior node (after 3 ghost nodes) of every row on a 16-byte
+  // boundary; pitch a multiple of 8 elements
+  d.oy = 1;
   d.py = (d.ny + d.oy + 7) / 8 * 8;
   d.sx = (long long)d.py * d.nz;
   d.nxyz = d.sx * d.nx;
@@ -236,9 +235,13 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->guess_net, 1232);
   if (!rc) rc = dalloc(ctx, &ctx->tile_err, 1);
   if (rc) { dfd_destroy(ctx); return rc; }
-  // interior box through the TMA-tiled kernel unless DFD_TILE=0 selects the plain kernel
+  // volume kernels: DFD_TILE=0 plain interior kernel + general shell kernel;
+  // 1 (default) TMA-tiled interior box + general shell kernel; 2 TMA tiles also over the
+  // PML slabs
   const char* tv = getenv("DFD_TILE");
-  ctx->use_tile = !(tv && tv[0] == '0') && tile_setup(&ctx->tile, d, ctx->W, ctx->M, ctx->tile_err, device);
+  int mode = tv && tv[0] >= '0' && tv[0] <= '2' ? tv[0] - '0' : 1;
+  ctx->use_tile = mode > 0 && tile_setup(&ctx->tile, d, ctx->W, ctx->M, ctx->tile_err, device);
+  ctx->tile.pml = mode == 2;
   *out = ctx;
   return DFD_OK;
 }

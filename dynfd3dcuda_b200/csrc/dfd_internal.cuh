@@ -46,9 +46,9 @@ enum Tab {
 enum TabF { TF_VX2VZ1 = 0, TF_VY2VZ1, TF_VX2VZ2, TF_VY2VZ2, TF_P2M1, TF_P2M2, TF_P2M3, TF_M2P1, TF_M2P2, TF_M2P3, NTABF };
 
 // Volume fields are stored with a padded row pitch: node (i, j, k) (padded indices, 3 ghost
-// nodes per side) of a field sits at element (j + oy) + k*py + i*sx.  The row offset oy puts
-// the first node of the interior box (outside the PML) on a 16-byte boundary and the pitch
-// py >= ny + oy is a multiple of 8, as tiled TMA loads need.  Fault-plane arrays keep the
+// nodes per side) of a field sits at element (j + oy) + k*py + i*sx.  The row offset oy = 1
+// puts the first interior node of every row (j = 3) on a 16-byte boundary and the pitch
+// py >= ny + 1 is a multiple of 8, as tiled TMA loads need.  Fault-plane arrays keep the
 // dense (nz, ny) layout.
 struct Dims {
   int ni, nj, nk;       // interior sizes NX NY NZ
@@ -168,6 +168,7 @@ struct TileCtx {
   CUtensorMap m9, m3;
   int* err = nullptr;
   int nsm = 0;
+  int pml = 0;  // 1: the tiles also cover the PML slabs
   bool ok = false;
 };
 bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* M, int* err, int device);

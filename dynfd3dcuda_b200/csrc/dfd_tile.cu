@@ -1,29 +1,32 @@
-// Interior volume stage staged through shared memory by TMA.
+// Volume stage staged through shared memory by TMA (interior box, and optionally the PML
+// slabs too).
 //
-// The interior box (outside every PML slab, below the free-surface rows) is cut into
-// tiles of 32 (y) x 8 (z) nodes; a CTA owns one tile column and marches along x over a
-// chunk of planes.  Per plane it needs
+// The box is cut into tiles of 32 (y) x 8 (z) nodes; a CTA owns one tile column and
+// marches along x over a chunk of planes.  Per plane it needs
 //   - the stencil input (9 fields) of the planes x-1..x+3 (forward x operator) or
 //     x-3..x+1 (backward), with a y/z halo on the current plane: one 4-D TMA box
 //     (40 y, 12 z, 1 x, 9 fields) per plane, held in a ring of NS plane slots;
 //   - the pointwise streams of the node: 12 metric/media fields, and the RK registers
 //     W0 (stages 1, 2) and T (stages 1..3): TMA boxes (32, 8, 1, n) in a ring of NP slots.
-// One elected thread issues the copies ahead of the consumers (mbarrier completion), so
-// HBM traffic is in flight while the 8 warps evaluate the stencils from shared memory
-// with immediate offsets.  Outputs (Wout, T) are written straight from registers.
+// A dedicated warp issues the copies ahead of the eight computing warps (full/empty
+// mbarrier pairs per slot, no block-wide barrier in the loop), so HBM traffic stays in
+// flight while the stencils are evaluated from shared memory with immediate offsets.
+// Nodes inside a PML slab take the general path (per-axis 1/beta and the ADE auxiliary
+// state, read and written in global memory); the others the lean interior path.  Outputs
+// (Wout, T) are written straight from registers.
 //
 // The kernel is persistent: one CTA per SM walks its units (tile column x chunk) and the
 // copy stream runs across unit boundaries, so the next unit's planes arrive while the
 // current one finishes.
 //
-// The right-hand side is the one of the interior kernel in dfd_volume.cu (reference
-// wave.cu:8-204 with rk4.cu:20-33): same operators, metric terms and RK update.
+// The right-hand side follows the reference's wave.cu:8-204, pmlx.cu / pmly.cu / pmlz.cu
+// and rk4.cu:20-33, as the general kernel in dfd_volume.cu does.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
 
-#include "dfd_internal.cuh"
+#include "dfd_stencil.cuh"
 
 namespace dfd {
 
@@ -36,7 +39,7 @@ constexpr int HSLOT = 9 * HBOX;      // floats per stencil plane slot
 constexpr int PB = TJ * TK;          // floats per field of a pointwise box
 constexpr int PSLOT = 30 * PB;       // metric 9 + lam mu rho + W0 9 + T 9
 constexpr int NS = 7, NP = 3;        // ring depths (stencil planes, pointwise planes)
-constexpr size_t SMEM_BYTES = (size_t)(NS * HSLOT + NP * PSLOT) * 4 + (NS + NP) * 8;
+constexpr size_t SMEM_BYTES = (size_t)(NS * HSLOT + NP * PSLOT) * 4 + 2 * (NS + NP) * 8;
 constexpr long long WAIT_LIMIT = 1LL << 22;  // polls of one mbarrier before giving up
 static_assert(SMEM_BYTES <= 232448, "tile ring exceeds the shared memory of one CTA");
 static_assert((HSLOT * 4) % 128 == 0 && (PSLOT * 4) % 128 == 0 && (PB * 4) % 128 == 0, "slot alignment");
@@ -91,104 +94,216 @@ __device__ __forceinline__ float d5s(const float* p) {
 }
 
 struct TileSched {
-  int lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;  // interior box, interior indices, half open
+  int lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;  // tiled box, interior indices, half open
   int ntj, ntk, ci, nunits;               // tiles in y and z, planes per chunk, units
 };
 
-// x derivative of field f (offset o inside the plane slots)
-#define DFD_DX(F_, o) d5v<F_>(xs0[o], xs1[o], xs2[o], xs3[o], xs4[o])
+constexpr int NCW = NTHR / 32;   // computing warps, one node per thread
+constexpr int NTOT = NTHR + 32;  // plus one copy-issuing warp
 
-// 256 threads with at most 128 registers, so that a block of the shell kernel fits beside
-// the CTA on its SM
+// slot / phase-parity cursor over a ring of N mbarrier-guarded slots
+struct Ring {
+  int slot = 0, phase = 0;
+  template <int N>
+  __device__ __forceinline__ void next() {
+    if (++slot == N) { slot = 0; phase ^= 1; }
+  }
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+// Right-hand side of a node inside at least one PML slab: every axis with its 1/beta and
+// the ADE auxiliary update of the faces the node lies in (reference wave.cu:8-204 with
+// pmlx.cu / pmly.cu / pmlz.cu).  xv[m] are the five x-stencil planes, cur the plane x.
 template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(NTHR, 2)
+__device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* const* xv, const float* cur,
+                                               const float* P, int i, int j, int k, float* hv) {
+  const Dims& d = a.d;
+  const float r = a.rDH;
+  const float lam = P[9 * PB], mu = P[10 * PB], rrho = 1.0f / P[11 * PB];
+  const float rb1 = __ldg(a.rBx + i), rb2 = __ldg(a.rBy + j), rb3 = __ldg(a.rBz + k);
+  float p[9], D[9], dv[9];
+#pragma unroll
+  for (int f = 0; f < 9; f++) p[f] = 0.0f;
+  // x
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    const int o = f * HBOX;
+    dv[f] = d5v<FX>(xv[0][o], xv[1][o], xv[2][o], xv[3][o], xv[4][o]) * r;
+  }
+  axis_terms(dv, P[0], P[PB], P[2 * PB], lam, mu, rrho, D);
+#pragma unroll
+  for (int f = 0; f < 9; f++) hv[f] = D[f] * rb1;
+  const bool px1 = a.aux[0] && i < d.N, px2 = a.aux[1] && i >= d.ni - d.N;
+  if (px1 || px2) {
+    long long st = (long long)d.N * d.nj * d.nk;
+    int ia = px1 ? i : i - (d.ni - d.N);
+    long long qa = j + (long long)k * d.nj + (long long)ia * d.nj * d.nk;
+    pml_face(a, px1 ? 0 : 1, qa, st, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D, nullptr, 0.f,
+             0.f, 0.f, lam, mu, p);
+  }
+  // y
+#pragma unroll
+  for (int f = 0; f < 9; f++) dv[f] = d5s<FY, 1>(cur + f * HBOX) * r;
+  axis_terms(dv, P[3 * PB], P[4 * PB], P[5 * PB], lam, mu, rrho, D);
+#pragma unroll
+  for (int f = 0; f < 9; f++) hv[f] += D[f] * rb2;
+  const bool py1 = a.aux[2] && j < d.N, py2 = a.aux[3] && j >= d.nj - d.N;
+  if (py1 || py2) {
+    long long st = (long long)d.N * d.nk * d.ni;
+    int ja = py1 ? j : j - (d.nj - d.N);
+    long long qa = ja + (long long)k * d.N + (long long)i * d.N * d.nk;
+    pml_face(a, py1 ? 2 : 3, qa, st, rb2, __ldg(a.By + j), __ldg(a.Dpy + j), __ldg(a.Apy + j), D, nullptr, 0.f,
+             0.f, 0.f, lam, mu, p);
+  }
+  // z
+#pragma unroll
+  for (int f = 0; f < 9; f++) dv[f] = d5s<FZ, HW>(cur + f * HBOX) * r;
+  axis_terms(dv, P[6 * PB], P[7 * PB], P[8 * PB], lam, mu, rrho, D);
+#pragma unroll
+  for (int f = 0; f < 9; f++) hv[f] += D[f] * rb3;
+  const bool pz1 = a.aux[4] && k < d.N, pz2 = a.aux[5] && k >= d.nk - d.N;
+  if (pz1 || pz2) {
+    long long st = (long long)d.N * d.ni * d.nj;
+    int ka = pz1 ? k : k - (d.nk - d.N);
+    long long qa = j + (long long)ka * d.nj + (long long)i * d.nj * d.N;
+    pml_face(a, pz1 ? 4 : 5, qa, st, rb3, __ldg(a.Bz + k), __ldg(a.Dpz + k), __ldg(a.Apz + k), D, nullptr, 0.f,
+             0.f, 0.f, lam, mu, p);
+  }
+#pragma unroll
+  for (int f = 0; f < 9; f++) hv[f] += p[f];
+}
+
+// Warp NCW issues the copies; warps 0..NCW-1 compute one node each per plane.  Each ring
+// slot has a "full" barrier (completed by the copy's transaction bytes) and an "empty"
+// barrier (one arrival per computing warp once it has finished reading the slot).  At
+// most 160 registers, so that a block of the fault band kernel fits beside the CTA.
+template <int FX, int FY, int FZ>
+__global__ void __maxnreg__(160)
     volume_tile_kernel(const __grid_constant__ TileMaps mp, const VolArgs a, const TileSched sc, int* err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   float* win = reinterpret_cast<float*>(smraw);
   float* pw = win + NS * HSLOT;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(pw + NP * PSLOT);
+  uint64_t* full_w = reinterpret_cast<uint64_t*>(pw + NP * PSLOT);
+  uint64_t* empty_w = full_w + NS;
+  uint64_t* full_p = empty_w + NS;
+  uint64_t* empty_p = full_p + NP;
   const Dims& d = a.d;
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int XLO = FX == 1 ? -1 : -3;  // first stencil plane relative to x
   constexpr int RZ = FZ == 1 ? 1 : 3;     // row of the tile's first z node inside the halo box
   const int irk = a.irk;
-  const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1;
-  const unsigned ptx = (12 + (needW0 ? 9 : 0) + (needT ? 9 : 0)) * PB * 4;
   const int ntile = sc.ntj * sc.ntk;
   const int G = gridDim.x;
 
-  if (tid == 0) {
-    for (int s = 0; s < NS + NP; s++) mbar_init(bar + s, 1);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS; s++) { mbar_init(full_w + s, 1); mbar_init(empty_w + s, NCW); }
+    for (int s = 0; s < NP; s++) { mbar_init(full_p + s, 1); mbar_init(empty_p + s, NCW); }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fence_async_shared();
   }
   __syncthreads();
 
-  // copy-issue state (used by thread 0 only)
-  int wu = blockIdx.x, wo = 0, pu = blockIdx.x, po = 0;
-  long long wn = 0, pn = 0, relW = 0, relP = 0;
-  auto produce = [&]() {
-    while (wu < sc.nunits && wn < relW + NS) {
-      int tc = wu / ntile, r = wu % ntile;
-      int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
-      int j0 = sc.lo_y + (r % sc.ntj) * TJ, k0 = sc.lo_z + (r / sc.ntj) * TK;
-      int slot = (int)(wn % NS);
-      mbar_expect_tx(bar + slot, HSLOT * 4);
-      tma_load4(win + slot * HSLOT, &mp.win, j0 + 3 + d.oy - 4, k0 + 3 - RZ, ib + XLO + wo + 3, 0, bar + slot);
-      wn++;
-      if (++wo == ie - ib + 4) { wo = 0; wu += G; }
+  if (warp == NCW) {
+    // ---------------- copy-issuing warp (one lane)
+    if (lane != 0) return;
+    const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1;
+    const unsigned ptx = (12 + (needW0 ? 9 : 0) + (needT ? 9 : 0)) * PB * 4;
+    Ring wr, pr;
+    int wcount = 0, pcount = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; u < sc.nunits && ok; u += G) {
+      const int tc = u / ntile, ru = u % ntile;
+      const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
+      const int j0 = sc.lo_y + (ru % sc.ntj) * TJ, k0 = sc.lo_z + (ru / sc.ntj) * TK;
+      const int cw0 = j0 + 3 + d.oy - 4, cw1 = k0 + 3 - RZ, cp0 = j0 + 3 + d.oy, cp1 = k0 + 3;
+      const int nst = ie - ib;
+      for (int m = 0; m < nst + 4 && ok; m++) {
+        // stencil plane m of the unit (first needed by step m - 4)
+        if (wcount >= NS && !(ok = mbar_wait(empty_w + wr.slot, wr.phase ^ 1))) break;
+        mbar_expect_tx(full_w + wr.slot, HSLOT * 4);
+        tma_load4(win + wr.slot * HSLOT, &mp.win, cw0, cw1, ib + XLO + m + 3, 0, full_w + wr.slot);
+        wr.next<NS>();
+        wcount++;
+        if (m < 4) continue;
+        // pointwise streams of step m - 4
+        if (pcount >= NP && !(ok = mbar_wait(empty_p + pr.slot, pr.phase ^ 1))) break;
+        uint64_t* b = full_p + pr.slot;
+        float* dst = pw + pr.slot * PSLOT;
+        const int cp2 = ib + (m - 4) + 3;
+        mbar_expect_tx(b, ptx);
+        tma_load4(dst, &mp.m9, cp0, cp1, cp2, 0, b);
+        tma_load4(dst + 9 * PB, &mp.m3, cp0, cp1, cp2, 10, b);
+        if (needW0) tma_load4(dst + 12 * PB, &mp.w0, cp0, cp1, cp2, 0, b);
+        if (needT) tma_load4(dst + 21 * PB, &mp.t, cp0, cp1, cp2, 0, b);
+        pr.next<NP>();
+        pcount++;
+      }
     }
-    while (pu < sc.nunits && pn < relP + NP) {
-      int tc = pu / ntile, r = pu % ntile;
-      int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
-      int j0 = sc.lo_y + (r % sc.ntj) * TJ, k0 = sc.lo_z + (r / sc.ntj) * TK;
-      int slot = (int)(pn % NP);
-      uint64_t* b = bar + NS + slot;
-      float* dst = pw + slot * PSLOT;
-      int c0 = j0 + 3 + d.oy, c1 = k0 + 3, c2 = ib + po + 3;
-      mbar_expect_tx(b, ptx);
-      tma_load4(dst, &mp.m9, c0, c1, c2, 0, b);
-      tma_load4(dst + 9 * PB, &mp.m3, c0, c1, c2, 10, b);
-      if (needW0) tma_load4(dst + 12 * PB, &mp.w0, c0, c1, c2, 0, b);
-      if (needT) tma_load4(dst + 21 * PB, &mp.t, c0, c1, c2, 0, b);
-      pn++;
-      if (++po == ie - ib) { po = 0; pu += G; }
+    if (!ok) {
+      // a slot was not released in time: flag it and let the copies in flight land
+      atomicExch(err, 1);
+      for (int c = max(0, wcount - NS); c < wcount; c++) mbar_wait(full_w + c % NS, (c / NS) & 1);
+      for (int c = max(0, pcount - NP); c < pcount; c++) mbar_wait(full_p + c % NP, (c / NP) & 1);
     }
-  };
-  if (tid == 0) produce();
+    return;
+  }
 
+  // ---------------- computing warps: thread (lane, warp) owns node (y = lane, z = warp)
   const long long n = d.nxyz;
   const float r = a.rDH;
-  const int hc = (ty + RZ) * HW + tx + 4;  // node inside a halo field box
-  const int pc = ty * TJ + tx;             // node inside a pointwise field box
-  long long wbase = 0, waited = 0, step = 0;
-  int bad = 0;
+  const int hc = (warp + RZ) * HW + lane + 4;  // node inside a halo field box
+  const int pc = warp * TJ + lane;             // node inside a pointwise field box
+  Ring wr, pr;  // next stencil plane to wait for; pointwise slot of the step
+  int sb = 0;   // slot of the step's first stencil plane
   for (int u = blockIdx.x; u < sc.nunits; u += G) {
     const int tc = u / ntile, ru = u % ntile;
     const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
-    const int j = sc.lo_y + (ru % sc.ntj) * TJ + tx, k = sc.lo_z + (ru / sc.ntj) * TK + ty;
+    const int j = sc.lo_y + (ru % sc.ntj) * TJ + lane, k = sc.lo_z + (ru / sc.ntj) * TK + warp;
     const bool active = j < sc.hi_y && k < sc.hi_z;
     const bool band = active && a.united && !a.united[j + k * d.nj];
+    const bool pml_yz = (a.aux[2] && j < d.N) || (a.aux[3] && j >= d.nj - d.N) || (a.aux[4] && k < d.N) ||
+                        (a.aux[5] && k >= d.nk - d.N);
     float dyz = 1.0f;
     if (active && a.dampx) dyz = fminf(__ldg(a.dampy + j + 3), __ldg(a.dampz + k + 3));
     const long long qyz = idx3(d, 0, j + 3, k + 3);
     const int nst = ie - ib;
     for (int s = 0; s < nst; s++) {
-      for (const long long top = wbase + s + 4; waited <= top; waited++)
-        bad |= !mbar_wait(bar + (int)(waited % NS), (unsigned)((waited / NS) & 1));
-      bad |= !mbar_wait(bar + NS + (int)(step % NP), (unsigned)((step / NP) & 1));
+      bool ok = true;
+      for (int c = s == 0 ? 5 : 1; c > 0; c--) {
+        ok = ok && mbar_wait(full_w + wr.slot, wr.phase);
+        wr.next<NS>();
+      }
+      ok = ok && mbar_wait(full_p + pr.slot, pr.phase);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicExch(err, 1);
+        return;
+      }
       const int i = ib + s;
-      if (active && !bad && !(band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3)) {
-        const float* xs0 = win + (int)((wbase + s) % NS) * HSLOT + hc;
-        const float* xs1 = win + (int)((wbase + s + 1) % NS) * HSLOT + hc;
-        const float* xs2 = win + (int)((wbase + s + 2) % NS) * HSLOT + hc;
-        const float* xs3 = win + (int)((wbase + s + 3) % NS) * HSLOT + hc;
-        const float* xs4 = win + (int)((wbase + s + 4) % NS) * HSLOT + hc;
+      const float* P = pw + pr.slot * PSLOT + pc;
+      if (active && !(band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3)) {
+        const int s1 = sb + 1 == NS ? 0 : sb + 1;
+        const int s2 = s1 + 1 == NS ? 0 : s1 + 1;
+        const int s3 = s2 + 1 == NS ? 0 : s2 + 1;
+        const int s4 = s3 + 1 == NS ? 0 : s3 + 1;
+        const float* xs0 = win + sb * HSLOT + hc;
+        const float* xs1 = win + s1 * HSLOT + hc;
+        const float* xs2 = win + s2 * HSLOT + hc;
+        const float* xs3 = win + s3 * HSLOT + hc;
+        const float* xs4 = win + s4 * HSLOT + hc;
         const float* cur = FX == 1 ? xs1 : xs3;  // plane x itself
-        const float* P = pw + (int)(step % NP) * PSLOT + pc;
-        const float lam = P[9 * PB], mu = P[10 * PB];
-        const float rrho = 1.0f / P[11 * PB];
-        const float l2m = lam + 2.0f * mu;
-        float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f, h8 = 0.f;
+        const bool pml = pml_yz || (a.aux[0] && i < d.N) || (a.aux[1] && i >= d.ni - d.N);
+        float hv[9];
+        if (pml) {
+          const float* xv[5] = {xs0, xs1, xs2, xs3, xs4};
+          tile_pml_point<FX, FY, FZ>(a, xv, cur, P, i, j, k, hv);
+        } else {
+          const float lam = P[9 * PB], mu = P[10 * PB];
+          const float rrho = 1.0f / P[11 * PB];
+          const float l2m = lam + 2.0f * mu;
+          float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f, h8 = 0.f;
 #define DFD_TAXIS(DER, MO)                                                                          \
   {                                                                                                 \
     const float e0 = P[(MO) * PB], e1 = P[((MO) + 1) * PB], e2 = P[((MO) + 2) * PB];                 \
@@ -207,18 +322,21 @@ __global__ void __launch_bounds__(NTHR, 2)
     dv = DER(7) * r; h0 += dv * er2; h2 += dv * er0;                                                \
     dv = DER(8) * r; h1 += dv * er2; h2 += dv * er1;                                                \
   }
-#define DFD_DERX(f) DFD_DX(FX, (f) * HBOX)
+#define DFD_DERX(f) d5v<FX>(xs0[(f) * HBOX], xs1[(f) * HBOX], xs2[(f) * HBOX], xs3[(f) * HBOX], xs4[(f) * HBOX])
 #define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HBOX)
 #define DFD_DERZ(f) d5s<FZ, HW>(cur + (f) * HBOX)
-        DFD_TAXIS(DFD_DERX, 0)
-        DFD_TAXIS(DFD_DERY, 3)
-        DFD_TAXIS(DFD_DERZ, 6)
+          DFD_TAXIS(DFD_DERX, 0)
+          DFD_TAXIS(DFD_DERY, 3)
+          DFD_TAXIS(DFD_DERZ, 6)
 #undef DFD_DERX
 #undef DFD_DERY
 #undef DFD_DERZ
 #undef DFD_TAXIS
+          hv[0] = h0; hv[1] = h1; hv[2] = h2; hv[3] = h3; hv[4] = h4;
+          hv[5] = h5; hv[6] = h6; hv[7] = h7; hv[8] = h8;
+        }
+        // RK4 registers and Cerjan sponge (rk4.cu:20-33, cerjan.cu:166-200)
         const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
-        const float hv[9] = {h0, h1, h2, h3, h4, h5, h6, h7, h8};
         const long long q = qyz + (long long)(i + 3) * d.sx;
 #pragma unroll
         for (int f = 0; f < 9; f++) {
@@ -237,32 +355,22 @@ __global__ void __launch_bounds__(NTHR, 2)
           a.Wout[x] = w * damp;
         }
       }
-      if (__syncthreads_or(bad)) {
-        // a copy did not arrive in time: flag it, let the copies in flight land, leave
-        if (tid == 0) {
-          atomicExch(err, 1);
-          for (int sl = 0; sl < NS; sl++) {
-            long long last = wn - 1 - ((wn - 1 - sl) % NS + NS) % NS;  // newest load into slot sl
-            if (last >= 0 && last % NS == sl) mbar_wait(bar + sl, (unsigned)((last / NS) & 1));
-          }
-          for (int sl = 0; sl < NP; sl++) {
-            long long last = pn - 1 - ((pn - 1 - sl) % NP + NP) % NP;
-            if (last >= 0 && last % NP == sl) mbar_wait(bar + NS + sl, (unsigned)((last / NP) & 1));
-          }
+      // release the slots this warp has finished with
+      __syncwarp();
+      if (lane == 0) {
+        if (s + 1 < nst) {
+          mbar_arrive(empty_w + sb);
+        } else {
+          for (int m = 0, sl = sb; m < 5; m++, sl = sl + 1 == NS ? 0 : sl + 1) mbar_arrive(empty_w + sl);
         }
-        return;
+        mbar_arrive(empty_p + pr.slot);
       }
-      relW = (s == nst - 1) ? wbase + nst + 4 : wbase + s + 1;
-      relP = ++step;
-      if (tid == 0) {
-        fence_async_shared();
-        produce();
-      }
+      pr.next<NP>();
+      sb += s + 1 < nst ? 1 : 5;
+      if (sb >= NS) sb -= NS;
     }
-    wbase += nst + 4;
   }
 }
-#undef DFD_DX
 
 // ---------------- host side
 
@@ -348,7 +456,7 @@ static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3
   mp.m3 = tc.m3;
   int grid = 0;
   TileSched sc = plan(a.d, lo, hi, tc.nsm, &grid);
-  volume_tile_kernel<FX, FY, FZ><<<grid, NTHR, SMEM_BYTES, s>>>(mp, a, sc, tc.err);
+  volume_tile_kernel<FX, FY, FZ><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err);
 }
 
 // true when the tiled kernel took the interior box

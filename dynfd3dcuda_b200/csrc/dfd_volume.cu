@@ -10,7 +10,7 @@
 // Nodes of the seven x-layers around the fault whose (j,k) is not "united" are left
 // to the band kernel (dfd_fault.cu), exactly the nodes whose right-hand side the
 // reference overwrites in fault_dvelo / fault_dstrs.
-#include "dfd_internal.cuh"
+#include "dfd_stencil.cuh"
 
 namespace dfd {
 
@@ -29,22 +29,6 @@ __device__ __forceinline__ float d5a(const float* v, int c) {  // on a 7-point r
   else return -DFD_C5 * v[c - 3] + DFD_C4 * v[c - 2] - DFD_C3 * v[c - 1] + DFD_C2 * v[c] + DFD_C1 * v[c + 1];
 }
 
-// axis contribution of the velocity-stress system for one set of derivatives d[9]
-// (Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz) and metric row e (wave.cu:133-141)
-__device__ __forceinline__ void axis_terms(const float* d, float e0, float e1, float e2, float lam, float mu,
-                                           float rrho, float* D) {
-  float l2m = lam + 2.0f * mu;
-  D[0] = (d[3] * e0 + d[6] * e1 + d[7] * e2) * rrho;
-  D[1] = (d[6] * e0 + d[4] * e1 + d[8] * e2) * rrho;
-  D[2] = (d[7] * e0 + d[8] * e1 + d[5] * e2) * rrho;
-  D[3] = d[0] * e0 * l2m + d[1] * e1 * lam + d[2] * e2 * lam;
-  D[4] = d[0] * e0 * lam + d[1] * e1 * l2m + d[2] * e2 * lam;
-  D[5] = d[0] * e0 * lam + d[1] * e1 * lam + d[2] * e2 * l2m;
-  D[6] = (d[0] * e1 + d[1] * e0) * mu;
-  D[7] = (d[0] * e2 + d[2] * e0) * mu;
-  D[8] = (d[1] * e2 + d[2] * e1) * mu;
-}
-
 // traction vector jac * e_axis . sigma at node q
 __device__ __forceinline__ void traction(const float* __restrict__ W, const float* __restrict__ M, long long n,
                                          long long q, int mo, float& t1, float& t2, float& t3) {
@@ -55,45 +39,6 @@ __device__ __forceinline__ void traction(const float* __restrict__ W, const floa
   t1 = (e0 * txx + e1 * txy + e2 * txz) * jac;
   t2 = (e0 * txy + e1 * tyy + e2 * tyz) * jac;
   t3 = (e0 * txz + e1 * tyz + e2 * tzz) * jac;
-}
-
-// PML auxiliary update of one face for this node: accumulates -aux/beta into p[] and
-// advances aux in place with the RK4 registers (pmlx.cu:165-208, rk4.cu:208-255).
-__device__ __forceinline__ void pml_face(const VolArgs& a, int face, long long qa, long long st, float rb, float b,
-                                         float dd, float al, const float* Dv, const float* dzv, float ez0,
-                                         float ez1, float ez2, float lam, float mu, float* p) {
-  float* aux = a.aux[face];
-  float* aux0 = a.aux0[face];
-  float* auxT = a.auxT[face];
-  float ad = -(al + dd);
-  float add[6];
-  if (dzv) {
-    float l2m = lam + 2.0f * mu, c = dd * b;
-    add[0] = c * (l2m * ez0 * dzv[0] + lam * ez1 * dzv[1] + lam * ez2 * dzv[2]);
-    add[1] = c * (lam * ez0 * dzv[0] + l2m * ez1 * dzv[1] + lam * ez2 * dzv[2]);
-    add[2] = c * (lam * ez0 * dzv[0] + lam * ez1 * dzv[1] + l2m * ez2 * dzv[2]);
-    add[3] = c * mu * (ez1 * dzv[0] + ez0 * dzv[1]);
-    add[4] = c * mu * (ez2 * dzv[0] + ez0 * dzv[2]);
-    add[5] = c * mu * (ez2 * dzv[1] + ez1 * dzv[2]);
-  }
-#pragma unroll
-  for (int f = 0; f < 9; f++) {
-    long long x = f * st + qa;
-    float w = aux[x];
-    p[f] += -w * rb;
-    float h = ad * w + dd * Dv[f];
-    if (dzv && f >= 3) h += add[f - 3];
-    if (a.irk == 0) {
-      aux0[x] = w;
-      auxT[x] = fmaf(a.rkb, h, w);
-      aux[x] = fmaf(a.rka, h, w);
-    } else if (a.irk < 3) {
-      auxT[x] = fmaf(a.rkb, h, auxT[x]);
-      aux[x] = fmaf(a.rka, h, aux0[x]);
-    } else {
-      aux[x] = fmaf(a.rkb, h, auxT[x]);
-    }
-  }
 }
 
 // General node update: every boundary treatment (PML faces, free-surface rows and
@@ -235,31 +180,16 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
   // ---- RK4 registers and Cerjan sponge
   float damp = 1.0f;
   if (a.dampx) damp = fminf(fminf(__ldg(a.dampx + i1), __ldg(a.dampy + j1)), __ldg(a.dampz + k1));
-#pragma unroll
-  for (int f = 0; f < 9; f++) {
-    float hf = h[f] + p[f];
-    long long x = f * n + q;
-    float w;
-    if (a.irk == 0) {
-      float w0 = __ldg(W + x);
-      a.T[x] = fmaf(a.rkb, hf, w0);
-      w = fmaf(a.rka, hf, w0);
-    } else if (a.irk < 3) {
-      a.T[x] = fmaf(a.rkb, hf, a.T[x]);
-      w = fmaf(a.rka, hf, __ldg(a.W0 + x));
-    } else {
-      w = fmaf(a.rkb, hf, a.T[x]);
-    }
-    a.Wout[x] = w * damp;
-  }
+  rk_store(a, q, h, p, damp);
 }
 
 
 // Shell kernel: the general update on up to six boxes (PML slabs, free-surface rows) that
 // surround the interior box; one 1-D grid of 256-thread blocks is split over the boxes.
 // A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z, 2 x) per block; a
-// thinner box (the y slabs of the PML, the free-surface rows) is flattened over (y, z) with y fastest, so that no thread
-// idles and the y-face PML state (y fastest over N nodes, then z) is read contiguously.
+// thinner box (the y slabs of the PML, the free-surface rows) is flattened over (y, z)
+// with y fastest, so that no thread idles and the y-face PML state (y fastest over N
+// nodes, then z) is read contiguously.
 struct Boxes {
   int n;
   int lo[6][3], hi[6][3];  // (i, j, k) interior-index bounds, half open
@@ -328,23 +258,8 @@ __device__ __forceinline__ void interior_point(const VolArgs& a, long long q, fl
   DFD_AXIS(FY, 1, 3)
   DFD_AXIS(FZ, a.d.py, 6)
 #undef DFD_AXIS
-  float hv[9] = {h0, h1, h2, h3, h4, h5, h6, h7, h8};
-#pragma unroll
-  for (int f = 0; f < 9; f++) {
-    long long x = f * n + q;
-    float w;
-    if (a.irk == 0) {
-      float w0 = __ldg(W + x);
-      a.T[x] = fmaf(a.rkb, hv[f], w0);
-      w = fmaf(a.rka, hv[f], w0);
-    } else if (a.irk < 3) {
-      a.T[x] = fmaf(a.rkb, hv[f], a.T[x]);
-      w = fmaf(a.rka, hv[f], __ldg(a.W0 + x));
-    } else {
-      w = fmaf(a.rkb, hv[f], a.T[x]);
-    }
-    a.Wout[x] = w * damp;
-  }
+  const float hv[9] = {h0, h1, h2, h3, h4, h5, h6, h7, h8};
+  rk_store(a, q, hv, nullptr, damp);
 }
 
 template <int FX, int FY, int FZ>
@@ -368,17 +283,6 @@ __global__ void __launch_bounds__(256, 3) volume_interior_kernel(VolArgs a, int3
 template <int FX, int FY, int FZ>
 static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin) {
   const Dims& d = a.d;
-  // interior box: outside every PML slab and below the free-surface rows
-  int nx0 = a.aux[0] ? d.N : 0, nx1 = a.aux[1] ? d.N : 0;
-  int ny0 = a.aux[2] ? d.N : 0, ny1 = a.aux[3] ? d.N : 0;
-  int nz0 = a.aux[4] ? d.N : 0, nz1 = a.aux[5] ? d.N : (a.freenode ? 3 : 0);
-  int3 lo = make_int3(nx0, ny0, nz0), hi = make_int3(d.ni - nx1, d.nj - ny1, d.nk - nz1);
-  const int chunk = 8;
-  if (hi.x > lo.x && hi.y > lo.y && hi.z > lo.z && !launch_tile(tc, a, FX, FY, FZ, bin, lo, hi, s)) {
-    dim3 block(32, 8, 1);
-    dim3 grid((hi.y - lo.y + 31) / 32, (hi.z - lo.z + 7) / 8, (hi.x - lo.x + chunk - 1) / chunk);
-    volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, lo, hi, chunk);
-  }
   Boxes bx;
   bx.n = 0;
   auto add = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
@@ -387,12 +291,40 @@ static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell,
     bx.hi[bx.n][0] = i1; bx.hi[bx.n][1] = j1; bx.hi[bx.n][2] = k1;
     bx.n++;
   };
-  add(0, lo.x, 0, d.nj, 0, d.nk);
-  add(hi.x, d.ni, 0, d.nj, 0, d.nk);
-  add(lo.x, hi.x, 0, lo.y, 0, d.nk);
-  add(lo.x, hi.x, hi.y, d.nj, 0, d.nk);
-  add(lo.x, hi.x, lo.y, hi.y, 0, lo.z);
-  add(lo.x, hi.x, lo.y, hi.y, hi.z, d.nk);
+  // interior box: outside every PML slab, below the free-surface rows
+  int nx0 = a.aux[0] ? d.N : 0, nx1 = a.aux[1] ? d.N : 0;
+  int ny0 = a.aux[2] ? d.N : 0, ny1 = a.aux[3] ? d.N : 0;
+  int nz0 = a.aux[4] ? d.N : 0, nz1 = a.aux[5] ? d.N : (a.freenode ? 3 : 0);
+  int3 lo = make_int3(nx0, ny0, nz0), hi = make_int3(d.ni - nx1, d.nj - ny1, d.nk - nz1);
+  const int ktop = a.freenode ? d.nk - 3 : d.nk;
+  if (tc && tc->ok && tc->pml &&
+      launch_tile(tc, a, FX, FY, FZ, bin, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop), s)) {
+    // TMA-tiled kernel over every node below the free-surface rows; the general kernel
+    // takes the free-surface rows
+    add(0, d.ni, 0, d.nj, ktop, d.nk);
+  } else {
+    // interior box by the TMA-tiled kernel (or the plain interior kernel), the shell
+    // around it by the general kernel.  The tiles start on a 16-byte boundary in y: the
+    // box is widened down to it (the few PML columns this adds take the tile kernel's
+    // PML path).
+    int3 tlo = lo;
+    tlo.y -= (lo.y + 3 + d.oy) % 4;
+    const bool some = hi.x > lo.x && hi.y > lo.y && hi.z > lo.z;
+    if (some && tlo.y >= 0 && launch_tile(tc, a, FX, FY, FZ, bin, tlo, hi, s)) {
+      lo = tlo;
+    } else if (some) {
+      const int chunk = 8;
+      dim3 block(32, 8, 1);
+      dim3 grid((hi.y - lo.y + 31) / 32, (hi.z - lo.z + 7) / 8, (hi.x - lo.x + chunk - 1) / chunk);
+      volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, lo, hi, chunk);
+    }
+    add(0, lo.x, 0, d.nj, 0, d.nk);
+    add(hi.x, d.ni, 0, d.nj, 0, d.nk);
+    add(lo.x, hi.x, 0, lo.y, 0, d.nk);
+    add(lo.x, hi.x, hi.y, d.nj, 0, d.nk);
+    add(lo.x, hi.x, lo.y, hi.y, 0, lo.z);
+    add(lo.x, hi.x, lo.y, hi.y, hi.z, d.nk);
+  }
   int tot = 0;
   for (int b = 0; b < bx.n; b++) {
     bx.start[b] = tot;

@@ -114,13 +114,15 @@ def test_run_many_steps_equals_single_steps():
     assert np.array_equal(a.fault("State"), b.fault("State"))
 
 
+@pytest.mark.parametrize("mode", ["1", "2"])
 @pytest.mark.parametrize("name", ["vol_curved", "sw_curved"])
-def test_tiled_interior_matches_plain_kernel(monkeypatch, name):
-    """The TMA-tiled interior kernel (default) and the plain interior kernel (DFD_TILE=0)
+def test_tiled_interior_matches_plain_kernel(monkeypatch, name, mode):
+    """The TMA-tiled kernel over the interior box (DFD_TILE=1, default) or over the PML
+    slabs too (2) and the plain interior kernel with the general shell kernel (0)
     evaluate the same stencils; after 12 steps they agree to FP32 rounding."""
     monkeypatch.setenv("DFD_TILE", "0")
     plain, *_ = make_sim(name)
-    monkeypatch.setenv("DFD_TILE", "1")
+    monkeypatch.setenv("DFD_TILE", mode)
     tiled, *_ = make_sim(name)
     for it in range(12):
         plain.run(it, 1)
