@@ -86,6 +86,7 @@ def lib():
             "dfd_output_open": [V, ctypes.c_char_p], "dfd_output_write": [V, I], "dfd_output_close": [V],
             "dfd_set_guess_net": [V, V, I], "dfd_fetch_outputs": [V, V],
             "dfd_run_timed": [V, I, I, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)],
+            "dfd_interior_stats": [V, P(ctypes.c_float), P(ctypes.c_longlong)],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)
@@ -239,6 +240,12 @@ class Simulation:
         t, v, f = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         self._check(lib().dfd_run_timed(self.h, it0, nsteps, ctypes.byref(t), ctypes.byref(v), ctypes.byref(f)))
         return t.value, v.value, f.value
+
+    def interior_stats(self):
+        """(ms, nodes): interior-kernel device time of the last run_timed and nodes per stage."""
+        ms, nodes = ctypes.c_float(), ctypes.c_longlong()
+        self._check(lib().dfd_interior_stats(self.h, ctypes.byref(ms), ctypes.byref(nodes)))
+        return ms.value, nodes.value
 
     def set_guess_net(self, w):
         a = np.ascontiguousarray(w, np.float32).ravel()

@@ -12,8 +12,8 @@
 #include "dfd_internal.cuh"
 
 namespace dfd {
-void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
-                         const TileCtx* tc, int bin);
+long long launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
+                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke);
 void launch_fault_node(const FaultArgs& a, cudaStream_t s);
 void launch_fault_band(const FaultArgs& a, cudaStream_t s);
 void launch_fault_coef(const Dims& d, const float* M, float* tab, float* tabf, float* vecn, float* vecs1,
@@ -80,6 +80,9 @@ struct dfd_ctx {
   TileCtx tile;                    // tiled interior kernel (TMA maps)
   int* tile_err = nullptr;
   bool use_tile = true;
+  long long interior_nodes = 0;   // nodes the interior kernel updates per stage
+  long long n_band_columns = 0;   // non-united (j, k) fault columns
+  float interior_ms = 0;          // interior kernel time of the last dfd_run_timed
   // host-side inputs
   std::vector<float> fxyz, planes, layers;
   std::vector<double> xl, fx, fy, fz;
@@ -404,6 +407,8 @@ int dfd_precompute(dfd_ctx* ctx) {
       CK(cudaMemcpyAsync(ctx->pl + u.plane * nf, u.v->data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
     struct { int plane; std::vector<int>* v; } iup[] = {
         {I_UNITED, &h.united}, {I_FAULTGRID, &h.faultgrid}, {I_RUPY, &h.rupy}, {I_RUPZ, &h.rupz}};
+    ctx->n_band_columns = 0;
+    for (int v : h.united) ctx->n_band_columns += v == 0;
     for (auto& u : iup)
       CK(cudaMemcpyAsync(ctx->ipl + u.plane * nf, u.v->data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s));
     for (int b = 0; b < 2; b++) CK(cudaMemsetAsync(ctx->FW[b], 0, sizeof(float) * 18 * d.nyz, s));
@@ -437,7 +442,8 @@ static const int kFlags[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1
                                  {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
 
 // enqueue one stage on the context streams (no synchronisation)
-static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr) {
+static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr,
+                         cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr) {
   const dfd_params& p = ctx->p;
   const Dims& d = ctx->d;
   int sg = (irk % 2) ? -1 : 1;
@@ -509,7 +515,9 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   va.united = p.rupture ? ctx->ipl + I_UNITED * nf : nullptr;
   va.rDH = (float)(1.0 / p.DH); va.rka = rka; va.rkb = rkb;
   va.irk = irk; va.freenode = p.free_surface;
-  launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk]);
+  long long nodes =
+      launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke);
+  ctx->interior_nodes = nodes - (p.rupture ? 7LL * ctx->n_band_columns : 0);
   cudaEventRecord(ctx->ev_join2, ctx->s2);
   if (p.rupture) cudaStreamWaitEvent(ctx->s0, ctx->ev_join, 0);
   cudaStreamWaitEvent(ctx->s0, ctx->ev_join2, 0);
@@ -728,33 +736,45 @@ int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* vol
   if (!ctx->ready || ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "not ready for a step");
   cudaSetDevice(ctx->device);
   int nev = 8 * nsteps + 2;
-  std::vector<cudaEvent_t> ev(nev);
+  std::vector<cudaEvent_t> ev(nev), kev(8 * nsteps);
   for (auto& e : ev) CK(cudaEventCreate(&e));
+  for (auto& e : kev) CK(cudaEventCreate(&e));
   CK(cudaEventRecord(ev[0], ctx->s0));
   int k = 1;
   for (int s = 0; s < nsteps; s++) {
     int it = it0 + s;
     dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it);
     for (int irk = 0; irk < 4; irk++) {
-      int r = enqueue_stage(ctx, ((it % 8) + 8) % 8, irk, &ev[k], &ev[k + 1]);
+      int r = enqueue_stage(ctx, ((it % 8) + 8) % 8, irk, &ev[k], &ev[k + 1], &kev[k - 1], &kev[k]);
       if (r) return r;
       k += 2;
     }
   }
   CK(cudaEventRecord(ev[nev - 1], ctx->s0));
   CK(cudaEventSynchronize(ev[nev - 1]));
-  float tot = 0, vol = 0;
+  float tot = 0, vol = 0, inner = 0;
   CK(cudaEventElapsedTime(&tot, ev[0], ev[nev - 1]));
   for (int i = 1; i + 1 < nev - 1; i += 2) {
     float m = 0;
     CK(cudaEventElapsedTime(&m, ev[i], ev[i + 1]));
     vol += m;
+    CK(cudaEventElapsedTime(&m, kev[i - 1], kev[i]));
+    inner += m;
   }
   for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& e : kev) cudaEventDestroy(e);
+  ctx->interior_ms = inner;
   if (total_ms) *total_ms = tot;
   if (volume_ms) *volume_ms = vol;
   if (fault_ms) *fault_ms = tot - vol;
   return tile_status(ctx);
+}
+
+int dfd_interior_stats(dfd_ctx* ctx, float* ms, long long* nodes) {
+  if (!ctx) return DFD_ERR_PARAM;
+  if (ms) *ms = ctx->interior_ms;
+  if (nodes) *nodes = ctx->interior_nodes;
+  return DFD_OK;
 }
 
 int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {

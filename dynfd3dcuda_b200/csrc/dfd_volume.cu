@@ -281,7 +281,8 @@ __global__ void __launch_bounds__(256, 3) volume_interior_kernel(VolArgs a, int3
 }
 
 template <int FX, int FY, int FZ>
-static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin) {
+static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin,
+                              cudaEvent_t* kb, cudaEvent_t* ke) {
   const Dims& d = a.d;
   Boxes bx;
   bx.n = 0;
@@ -297,10 +298,13 @@ static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell,
   int nz0 = a.aux[4] ? d.N : 0, nz1 = a.aux[5] ? d.N : (a.freenode ? 3 : 0);
   int3 lo = make_int3(nx0, ny0, nz0), hi = make_int3(d.ni - nx1, d.nj - ny1, d.nk - nz1);
   const int ktop = a.freenode ? d.nk - 3 : d.nk;
+  long long nodes = 0;  // nodes of the box the interior (or tiled) kernel covers
+  if (kb) cudaEventRecord(*kb, s);
   if (tc && tc->ok && tc->pml &&
       launch_tile(tc, a, FX, FY, FZ, bin, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop), s)) {
     // TMA-tiled kernel over every node below the free-surface rows; the general kernel
     // takes the free-surface rows
+    nodes = (long long)d.ni * d.nj * ktop;
     add(0, d.ni, 0, d.nj, ktop, d.nk);
   } else {
     // interior box by the TMA-tiled kernel (or the plain interior kernel), the shell
@@ -318,6 +322,7 @@ static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell,
       dim3 grid((hi.y - lo.y + 31) / 32, (hi.z - lo.z + 7) / 8, (hi.x - lo.x + chunk - 1) / chunk);
       volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, lo, hi, chunk);
     }
+    if (some) nodes = (long long)(hi.x - lo.x) * (hi.y - lo.y) * (hi.z - lo.z);
     add(0, lo.x, 0, d.nj, 0, d.nk);
     add(hi.x, d.ni, 0, d.nj, 0, d.nk);
     add(lo.x, hi.x, 0, lo.y, 0, d.nk);
@@ -333,21 +338,26 @@ static void launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell,
     tot += bx.thin[b] ? ((nj * nk + 255) / 256) * ni : ((nj + 31) / 32) * ((nk + 3) / 4) * ((ni + 1) / 2);
   }
   bx.start[bx.n] = tot;
+  if (ke) cudaEventRecord(*ke, s);
   if (tot > 0) volume_shell_kernel<FX, FY, FZ><<<tot, 256, 0, s_shell>>>(a, bx);
+  return nodes;
 }
 
-void launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
-                         const TileCtx* tc, int bin) {
+// Launches the volume kernels of one stage; kb/ke (optional) are recorded on s right
+// before and after the interior (tiled) kernel.  Returns the nodes of the box that kernel
+// covers.
+long long launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
+                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke) {
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: launch_flags<-1, -1, -1>(a, s, s_shell, tc, bin); break;
-    case 1: launch_flags<-1, -1, 1>(a, s, s_shell, tc, bin); break;
-    case 2: launch_flags<-1, 1, -1>(a, s, s_shell, tc, bin); break;
-    case 3: launch_flags<-1, 1, 1>(a, s, s_shell, tc, bin); break;
-    case 4: launch_flags<1, -1, -1>(a, s, s_shell, tc, bin); break;
-    case 5: launch_flags<1, -1, 1>(a, s, s_shell, tc, bin); break;
-    case 6: launch_flags<1, 1, -1>(a, s, s_shell, tc, bin); break;
-    default: launch_flags<1, 1, 1>(a, s, s_shell, tc, bin); break;
+    case 0: return launch_flags<-1, -1, -1>(a, s, s_shell, tc, bin, kb, ke);
+    case 1: return launch_flags<-1, -1, 1>(a, s, s_shell, tc, bin, kb, ke);
+    case 2: return launch_flags<-1, 1, -1>(a, s, s_shell, tc, bin, kb, ke);
+    case 3: return launch_flags<-1, 1, 1>(a, s, s_shell, tc, bin, kb, ke);
+    case 4: return launch_flags<1, -1, -1>(a, s, s_shell, tc, bin, kb, ke);
+    case 5: return launch_flags<1, -1, 1>(a, s, s_shell, tc, bin, kb, ke);
+    case 6: return launch_flags<1, 1, -1>(a, s, s_shell, tc, bin, kb, ke);
+    default: return launch_flags<1, 1, 1>(a, s, s_shell, tc, bin, kb, ke);
   }
 }
 

@@ -125,6 +125,11 @@ int dfd_fetch_outputs(dfd_ctx *ctx, float *host);
 /* nsteps steps issued stage by stage with CUDA events around every volume-kernel launch:
  * total device time, time inside the volume kernels, and the rest (milliseconds) */
 int dfd_run_timed(dfd_ctx *ctx, int it0, int nsteps, float *total_ms, float *volume_ms, float *fault_ms);
+/* device time spent in the interior (TMA-tiled) volume kernel during the last
+ * dfd_run_timed (CUDA events on its stream, summed over all stages), and the nodes that
+ * kernel updates per stage (the interior box minus the fault band); a measurement aid
+ * with no counterpart in the reference */
+int dfd_interior_stats(dfd_ctx *ctx, float *ms, long long *nodes);
 /* The same slice as dfd_get_slice, gathered into a static device array instead of a
  * temporary allocation; this entry has no counterpart in the reference.  It is for callers
  * that must not allocate or free device memory while they run (fixed memory budget, or no
