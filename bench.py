@@ -251,6 +251,63 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def active_fault_nodes(job):
+    """Fault nodes that run the friction solve: the non-united ones (init.cu:806-816)."""
+    NY, NZ = job["NY"], job["NZ"]
+    nj = sum(1 for j in range(NY) if 30 < j + 1 < NY - 30)
+    free = job.get("FreeSurface", 1)
+    nk = sum(1 for k in range(NZ) if k + 1 > 30 and (free or k + 1 < NZ - 30))
+    return nj * nk
+
+
+def learned_rs(dfd, steps=600, every=7, epochs=4, device=0):
+    """The learned Newton guess on the rate-and-state rough-fault configuration
+    (300 x 200 x 150, slip law): record plain-solver samples on one seed, train the MLP on
+    the GPU, then run another seed with the plain and with the learned guess and compare
+    the fault node kernel time, Newton iterations per solve and the final slip."""
+    import cases
+
+    job, fx, st, _, _, _ = cases.rs_rough_case(300, 200, 150, seed=11, steps=steps)
+    sim = dfd.Simulation(job, fx, st, None, device=device)
+    sim.newton_record(12_000_000, every)
+    sim.run(0, steps)
+    samples = sim.newton_samples(12_000_000)
+    sim.close()
+    t0 = time.perf_counter()
+    w, hist = dfd.train_guess_net(samples, epochs=epochs, batch=8192, lr=3e-3, seed=1)
+    train_s = time.perf_counter() - t0
+    job, fx, st, _, _, _ = cases.rs_rough_case(300, 200, 150, seed=23, steps=steps)
+    nact = active_fault_nodes(job)
+    out = {"config": "rate-and-state slip law, self-similar rough fault 300x200x150 (strike x normal x depth), "
+                     f"dh=100 m, a log-uniform 0.01-0.02, {steps} steps; trained on seed 11, run on seed 23",
+           "train_samples": int(len(samples)), "epochs": epochs, "train_s": train_s,
+           "loss_per_epoch": [float(v) for v in hist]}
+    slips = {}
+    for name, net in (("plain", None), ("learned", w)):
+        sim = dfd.Simulation(job, fx, st, None, device=device)
+        if net is not None:
+            sim.set_guess_net(net)
+        sim.run(0, 5)
+        sim.synchronize()
+        it0, cap0 = sim.newton_stats()
+        total_ms, vol_ms, _ = sim.run_timed(5, steps - 5)
+        node_ms = sim.fault_node_ms()
+        it1, cap1 = sim.newton_stats()
+        solves = nact * 4 * (steps - 5)
+        slips[name] = sim.fault("slip").astype(np.float64)
+        out[name] = {"node_kernel_us_per_stage": 1e3 * node_ms / (4 * (steps - 5)),
+                     "newton_iterations_per_solve": (it1 - it0) / solves,
+                     "unconverged_solves": int(cap1 - cap0), "step_ms": total_ms / (steps - 5)}
+        sim.close()
+    p, l = out["plain"], out["learned"]
+    out["speedup_node_kernel"] = p["node_kernel_us_per_stage"] / l["node_kernel_us_per_stage"]
+    out["speedup_newton_iterations"] = p["newton_iterations_per_solve"] / l["newton_iterations_per_solve"]
+    s0 = np.abs(slips["plain"]).max()
+    out["final_slip_max_m"] = float(s0)
+    out["slip_rel_diff_learned_vs_plain"] = float(np.abs(slips["learned"] - slips["plain"]).max() / max(s0, 1e-30))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -259,6 +316,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="curved", choices=["curved", "flat", "profile", "large"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned Newton-guess comparison")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -351,6 +409,8 @@ def main():
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,
         "clocks": clocks,
     }
+    if rank == 0 and world == 1 and not args.no_learned:
+        line["learned_rs"] = learned_rs(dfd, device=local)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(job, fx, st, layers)
     if dist:

@@ -28,6 +28,65 @@ STATUS = {0: "ok", 1: "bad or unsupported parameter", 2: "CUDA error", 3: "file 
           7: "Newton solve hit its iteration cap"}
 
 
+# parameter vector of the learned Newton guess (DFD_MLP_PARAMS, DFD_MLP_TRAINABLE)
+MLP_PARAMS = 1259
+MLP_TRAINABLE = 1249
+
+
+def _check(r):
+    if r:
+        raise DfdError(r)
+
+
+def mlp_init(seed, x_mean, x_scale, y_mean, y_scale):
+    """Initial parameter vector: Xavier weights from seed, standardisation constants."""
+    w = np.zeros(MLP_PARAMS, np.float32)
+    xm = np.ascontiguousarray(x_mean, np.float32)
+    xs = np.ascontiguousarray(x_scale, np.float32)
+    _check(lib().dfd_mlp_init(w.ctypes.data, int(seed), xm.ctypes.data, xs.ctypes.data, float(y_mean), float(y_scale)))
+    return w
+
+
+def mlp_forward(w, x):
+    """Residual predicted by the network for inputs x (n, 4), on the GPU."""
+    w = np.ascontiguousarray(w, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.empty(len(x), np.float32)
+    _check(lib().dfd_mlp_forward(w.ctypes.data, x.ctypes.data, len(x), y.ctypes.data))
+    return y
+
+
+def mlp_loss_grad(w, x, y):
+    """(mean squared standardised error, gradient over the MLP_TRAINABLE weights), on the GPU."""
+    w = np.ascontiguousarray(w, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    g = np.empty(MLP_TRAINABLE, np.float32)
+    loss = ctypes.c_double()
+    _check(lib().dfd_mlp_loss_grad(w.ctypes.data, x.ctypes.data, y.ctypes.data, len(x), ctypes.byref(loss),
+                                   g.ctypes.data))
+    return loss.value, g
+
+
+def mlp_train(w, x, y, epochs, batch=4096, lr=3e-3, seed=0):
+    """Minibatch Adam on the GPU; returns (trained weights, loss per epoch)."""
+    w = np.array(w, np.float32, copy=True)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    hist = np.zeros(epochs, np.float32)
+    _check(lib().dfd_mlp_train(x.ctypes.data, y.ctypes.data, len(x), int(epochs), int(batch), float(lr), int(seed),
+                               w.ctypes.data, hist.ctypes.data))
+    return w, hist
+
+
+def train_guess_net(samples, epochs=8, batch=4096, lr=3e-3, seed=0):
+    """Fit the learned Newton guess to recorded samples (n, 5) from newton_samples()."""
+    x, y = samples[:, :4], samples[:, 4]
+    xm, xs = x.mean(0), x.std(0) + 1e-6
+    w0 = mlp_init(seed, xm, xs, float(y.mean()), float(y.std() + 1e-6))
+    return mlp_train(w0, x, y, epochs, batch, lr, seed)
+
+
 # capacity of the static gather buffer of dfd_get_slice_noalloc (DFD_SLICE_SCRATCH_FLOATS)
 SLICE_SCRATCH_FLOATS = 1 << 22
 
@@ -87,6 +146,11 @@ def lib():
             "dfd_set_guess_net": [V, V, I], "dfd_fetch_outputs": [V, V],
             "dfd_run_timed": [V, I, I, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)],
             "dfd_interior_stats": [V, P(ctypes.c_float), P(ctypes.c_longlong)],
+            "dfd_newton_record": [V, I, I], "dfd_fault_node_ms": [V, P(ctypes.c_float)], "dfd_newton_samples": [V, V, I, P(ctypes.c_int)],
+            "dfd_mlp_init": [V, ctypes.c_uint, V, V, ctypes.c_float, ctypes.c_float],
+            "dfd_mlp_forward": [V, V, I, V],
+            "dfd_mlp_loss_grad": [V, V, V, I, P(ctypes.c_double), V],
+            "dfd_mlp_train": [V, V, I, I, I, ctypes.c_float, ctypes.c_uint, V, V],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)
@@ -248,8 +312,29 @@ class Simulation:
         return ms.value, nodes.value
 
     def set_guess_net(self, w):
+        """Load MLP weights (MLP_PARAMS floats) and use the learned Newton guess; None: plain guess."""
+        if w is None:
+            self._check(lib().dfd_set_guess_net(self.h, None, 0))
+            return
         a = np.ascontiguousarray(w, np.float32).ravel()
         self._check(lib().dfd_set_guess_net(self.h, a.ctypes.data, a.size))
+
+    def newton_record(self, capacity, every=1):
+        """Record (psi/a, log10 Vhat, log10 coef, a, x* residual) of one in `every` converged
+        plain Newton solves, up to capacity samples (0 stops recording)."""
+        self._check(lib().dfd_newton_record(self.h, int(capacity), int(every)))
+
+    def fault_node_ms(self):
+        """Fault node kernel device time of the last run_timed (ms, all stages)."""
+        ms = ctypes.c_float()
+        self._check(lib().dfd_fault_node_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def newton_samples(self, max_samples):
+        out = np.empty((max(int(max_samples), 1), 5), np.float32)
+        n = ctypes.c_int()
+        self._check(lib().dfd_newton_samples(self.h, out.ctypes.data, int(max_samples), ctypes.byref(n)))
+        return out[:n.value].copy()
 
     def output_open(self, outdir):
         self._check(lib().dfd_output_open(self.h, outdir.encode()))

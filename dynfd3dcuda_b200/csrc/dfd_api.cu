@@ -1,6 +1,7 @@
 // C ABI of the B200 dynamic-rupture time step: context (device memory owner), setup,
 // stage sequencing with a side stream for the fault band, CUDA-graph replay of whole
 // steps, state access and NetCDF output.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -77,12 +78,17 @@ struct dfd_ctx {
   int* it_dev = nullptr;
   int* flag_dev = nullptr;
   float* guess_net = nullptr;
+  float* rec = nullptr;             // Newton sample recording buffer (rec_cap x 5)
+  unsigned* rec_n = nullptr;
+  int rec_cap = 0;
+  int rec_every = 1;
   TileCtx tile;                    // tiled interior kernel (TMA maps)
   int* tile_err = nullptr;
   bool use_tile = true;
   long long interior_nodes = 0;   // nodes the interior kernel updates per stage
   long long n_band_columns = 0;   // non-united (j, k) fault columns
   float interior_ms = 0;          // interior kernel time of the last dfd_run_timed
+  float node_ms = 0;              // fault node kernel time of the last dfd_run_timed
   // host-side inputs
   std::vector<float> fxyz, planes, layers;
   std::vector<double> xl, fx, fy, fz;
@@ -235,7 +241,8 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->newton, 2);
   if (!rc) rc = dalloc(ctx, &ctx->it_dev, 1);
   if (!rc) rc = dalloc(ctx, &ctx->flag_dev, 1);
-  if (!rc) rc = dalloc(ctx, &ctx->guess_net, 1232);
+  if (!rc) rc = dalloc(ctx, &ctx->guess_net, DFD_MLP_PARAMS);
+  if (!rc) rc = dalloc(ctx, &ctx->rec_n, 1);
   if (!rc) rc = dalloc(ctx, &ctx->tile_err, 1);
   if (rc) { dfd_destroy(ctx); return rc; }
   // volume kernels: DFD_TILE=0 plain interior kernel + general shell kernel;
@@ -259,6 +266,7 @@ int dfd_destroy(dfd_ctx* ctx) {
   if (ctx->s1) cudaStreamSynchronize(ctx->s1);
   if (ctx->s2) cudaStreamSynchronize(ctx->s2);
   for (void* v : ctx->allocs) cudaFree(v);
+  if (ctx->rec) cudaFree(ctx->rec);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->ev_join2) cudaEventDestroy(ctx->ev_join2);
@@ -443,7 +451,8 @@ static const int kFlags[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1
 
 // enqueue one stage on the context streams (no synchronisation)
 static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr,
-                         cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr) {
+                         cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr, cudaEvent_t* nb = nullptr,
+                         cudaEvent_t* ne = nullptr) {
   const dfd_params& p = ctx->p;
   const Dims& d = ctx->d;
   int sg = (irk % 2) ? -1 : 1;
@@ -481,6 +490,7 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
     fa.united = ctx->ipl + I_UNITED * nf; fa.faultgrid = ctx->ipl + I_FAULTGRID * nf;
     fa.rupy = ctx->ipl + I_RUPY * nf; fa.rupz = ctx->ipl + I_RUPZ * nf;
     fa.newton = ctx->newton; fa.it_dev = ctx->it_dev; fa.guess_net = ctx->guess_net;
+    fa.rec = ctx->rec; fa.rec_n = ctx->rec_n; fa.rec_cap = ctx->rec_cap; fa.rec_every = ctx->rec_every;
     fa.rDH = (float)(1.0 / p.DH); fa.DH = (float)p.DH; fa.DT = DT; fa.rka = rka; fa.rkb = rkb;
     fa.mu_d = (float)p.mu_d; fa.viscosity = (float)p.viscosity;
     fa.dDT = (double)DT; fa.smooth_load_T = (double)(float)p.smooth_load_T;
@@ -489,7 +499,9 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
     fa.irk = irk; fa.FX = FX; fa.FY = FY; fa.FZ = FZ;
     fa.freenode = p.free_surface; fa.friction_type = p.Friction_type; fa.inport_stress = p.INPORT_STRESS_TYPE;
     fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess;
+    if (nb) cudaEventRecord(*nb, ctx->s0);
     launch_fault_node(fa, ctx->s0);
+    if (ne) cudaEventRecord(*ne, ctx->s0);
   }
   // fork: fault band on s1, volume shell on s2, volume interior on s0
   cudaEventRecord(ctx->ev_fork, ctx->s0);
@@ -736,23 +748,25 @@ int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* vol
   if (!ctx->ready || ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "not ready for a step");
   cudaSetDevice(ctx->device);
   int nev = 8 * nsteps + 2;
-  std::vector<cudaEvent_t> ev(nev), kev(8 * nsteps);
+  std::vector<cudaEvent_t> ev(nev), kev(8 * nsteps), fev(8 * nsteps);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   for (auto& e : kev) CK(cudaEventCreate(&e));
+  for (auto& e : fev) CK(cudaEventCreate(&e));
   CK(cudaEventRecord(ev[0], ctx->s0));
   int k = 1;
   for (int s = 0; s < nsteps; s++) {
     int it = it0 + s;
     dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it);
     for (int irk = 0; irk < 4; irk++) {
-      int r = enqueue_stage(ctx, ((it % 8) + 8) % 8, irk, &ev[k], &ev[k + 1], &kev[k - 1], &kev[k]);
+      int r = enqueue_stage(ctx, ((it % 8) + 8) % 8, irk, &ev[k], &ev[k + 1], &kev[k - 1], &kev[k],
+                            ctx->p.rupture ? &fev[k - 1] : nullptr, ctx->p.rupture ? &fev[k] : nullptr);
       if (r) return r;
       k += 2;
     }
   }
   CK(cudaEventRecord(ev[nev - 1], ctx->s0));
   CK(cudaEventSynchronize(ev[nev - 1]));
-  float tot = 0, vol = 0, inner = 0;
+  float tot = 0, vol = 0, inner = 0, node = 0;
   CK(cudaEventElapsedTime(&tot, ev[0], ev[nev - 1]));
   for (int i = 1; i + 1 < nev - 1; i += 2) {
     float m = 0;
@@ -760,10 +774,16 @@ int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* vol
     vol += m;
     CK(cudaEventElapsedTime(&m, kev[i - 1], kev[i]));
     inner += m;
+    if (ctx->p.rupture) {
+      CK(cudaEventElapsedTime(&m, fev[i - 1], fev[i]));
+      node += m;
+    }
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (auto& e : kev) cudaEventDestroy(e);
+  for (auto& e : fev) cudaEventDestroy(e);
   ctx->interior_ms = inner;
+  ctx->node_ms = node;
   if (total_ms) *total_ms = tot;
   if (volume_ms) *volume_ms = vol;
   if (fault_ms) *fault_ms = tot - vol;
@@ -777,9 +797,56 @@ int dfd_interior_stats(dfd_ctx* ctx, float* ms, long long* nodes) {
   return DFD_OK;
 }
 
+int dfd_fault_node_ms(dfd_ctx* ctx, float* ms) {
+  if (!ctx || !ms) return DFD_ERR_PARAM;
+  *ms = ctx->node_ms;
+  return DFD_OK;
+}
+
 int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {
-  if (!ctx || !w || n != 1225) return DFD_ERR_PARAM;
-  CK(cudaMemcpy(ctx->guess_net, w, sizeof(float) * n, cudaMemcpyHostToDevice));
+  if (!ctx || (w && n != DFD_MLP_PARAMS) || (!w && n != 0)) return DFD_ERR_PARAM;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  if (w) CK(cudaMemcpy(ctx->guess_net, w, sizeof(float) * n, cudaMemcpyHostToDevice));
+  ctx->p.rs_guess = w ? 1 : 0;
+  // the switch is baked into the step graphs: rebuild them
+  for (auto& g : ctx->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return DFD_OK;
+}
+
+int dfd_newton_record(dfd_ctx* ctx, int capacity, int every) {
+  if (!ctx || capacity < 0 || every < 1) return DFD_ERR_PARAM;
+  ctx->rec_every = every;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  if (ctx->rec) {
+    cudaFree(ctx->rec);
+    ctx->rec = nullptr;
+    ctx->rec_cap = 0;
+  }
+  if (capacity > 0) {
+    CK(cudaMalloc(&ctx->rec, sizeof(float) * 5 * (size_t)capacity));
+    ctx->rec_cap = capacity;
+  }
+  CK(cudaMemset(ctx->rec_n, 0, sizeof(unsigned)));
+  // the recording buffer is baked into the step graphs: rebuild them
+  for (auto& g : ctx->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return DFD_OK;
+}
+
+int dfd_newton_samples(dfd_ctx* ctx, float* host, int max, int* n) {
+  if (!ctx || !n || max < 0 || (max > 0 && !host)) return DFD_ERR_PARAM;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  unsigned got = 0;
+  CK(cudaMemcpy(&got, ctx->rec_n, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  int m = (int)std::min<unsigned>(got, (unsigned)ctx->rec_cap);
+  m = std::min(m, max);
+  if (m > 0) CK(cudaMemcpy(host, ctx->rec, sizeof(float) * 5 * (size_t)m, cudaMemcpyDeviceToHost));
+  *n = m;
+  CK(cudaMemset(ctx->rec_n, 0, sizeof(unsigned)));
   return DFD_OK;
 }
 

@@ -11,6 +11,7 @@
 //   update of those band nodes and of the split nodes (rk4.cu:573-789), the RK-weighted
 //   on-fault outputs (rk4.cu:466-571), the end-of-stage transfer and the sponge.
 #include "dfd_internal.cuh"
+#include "../../include/dfd_b200.h"
 
 namespace dfd {
 
@@ -114,37 +115,51 @@ __device__ __forceinline__ double gt_func(double t, double T) {  // device.cu:13
   return 1.0;
 }
 
-// Learned initial guess: MLP 4 -> 32 -> 32 -> 1 (tanh), inputs normalised by the
-// stored mean/scale.  Weight layout: W1[32][4] b1[32] W2[32][32] b2[32] W3[32] b3 mu[4] sd[4].
-__device__ float mlp_guess(const float* __restrict__ w, const float* xin) {
-  const float* W1 = w;
-  const float* b1 = W1 + 128;
-  const float* W2 = b1 + 32;
-  const float* b2 = W2 + 1024;
-  const float* W3 = b2 + 32;
-  const float* b3 = W3 + 32;
+// Learned initial guess: MLP 4 -> 32 -> 32 -> 1 (tanh) on the standardised inputs; the
+// de-standardised output is the residual x* - asinh(Vhat e^{psi/a} / (2 V0)).  Weight
+// layout (dfd_mlp.cu): W1[32][4] b1[32] W2[32][32] b2[32] W3[32] b3 mu[4] sd[4] ymu ysd.
+// The hidden activations use the hardware tanh approximation (absolute error ~5e-4): the
+// output is scaled by the residual's small standard deviation, and the Newton iteration
+// that follows removes what is left.
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ float mlp_residual(const float* w, const float* xin) {
+  const float4* W1 = reinterpret_cast<const float4*>(w);  // rows of 4
+  const float* b1 = w + 128;
+  const float4* W2 = reinterpret_cast<const float4*>(w + 160);
+  const float* b2 = w + 1184;
+  const float* W3 = w + 1216;
+  const float* b3 = w + 1248;
   const float* mu = b3 + 1;
   const float* sd = mu + 4;
+  const float* ys = sd + 4;
   float x[4];
 #pragma unroll
-  for (int c = 0; c < 4; c++) x[c] = (xin[c] - __ldg(mu + c)) / __ldg(sd + c);
+  for (int c = 0; c < 4; c++) x[c] = (xin[c] - mu[c]) / sd[c];
   float h1[32];
 #pragma unroll
   for (int r = 0; r < 32; r++) {
-    float s = __ldg(b1 + r);
-#pragma unroll
-    for (int c = 0; c < 4; c++) s = fmaf(__ldg(W1 + r * 4 + c), x[c], s);
-    h1[r] = tanhf(s);
+    const float4 wr = W1[r];
+    float s = b1[r];
+    s = fmaf(wr.x, x[0], s); s = fmaf(wr.y, x[1], s); s = fmaf(wr.z, x[2], s); s = fmaf(wr.w, x[3], s);
+    h1[r] = tanh_fast(s);
   }
-  float out = __ldg(b3);
+  float out = *b3;
 #pragma unroll 4
   for (int r = 0; r < 32; r++) {
-    float s = __ldg(b2 + r);
+    float s = b2[r];
 #pragma unroll
-    for (int c = 0; c < 32; c++) s = fmaf(__ldg(W2 + r * 32 + c), h1[c], s);
-    out = fmaf(__ldg(W3 + r), tanhf(s), out);
+    for (int c = 0; c < 8; c++) {
+      const float4 wv = W2[r * 8 + c];
+      s = fmaf(wv.x, h1[4 * c], s); s = fmaf(wv.y, h1[4 * c + 1], s);
+      s = fmaf(wv.z, h1[4 * c + 2], s); s = fmaf(wv.w, h1[4 * c + 3], s);
+    }
+    out = fmaf(W3[r], tanh_fast(s), out);
   }
-  return out;
+  return out * ys[1] + ys[0];
 }
 
 // Bounded Newton on f(x) = 2 V0 e^{-psi/a} sinh x + coef x - Vhat (trial_ratestate.cu:20-57);
@@ -173,6 +188,15 @@ __device__ double newton_rs(double x, double psi, double ra, double Vhat, double
 template <int FY, int FZ>
 __global__ void __launch_bounds__(128) fault_node_kernel(FaultArgs a) {
   const Dims& d = a.d;
+  // learned-guess weights staged in shared memory (every thread reads the same weight at
+  // the same time: a broadcast)
+  __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
+  const bool learned = a.friction_type != 0 && a.rs_guess && a.guess_net;
+  if (learned) {
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
+    for (int p = tid; p < DFD_MLP_PARAMS; p += nt) snet[p] = __ldg(a.guess_net + p);
+    __syncthreads();
+  }
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   int k = blockIdx.y * blockDim.y + threadIdx.y;
   if (j >= d.nj || k >= d.nk) return;
@@ -377,16 +401,38 @@ __global__ void __launch_bounds__(128) fault_node_kernel(FaultArgs a) {
     int its = 0, its2 = 0;
     bool ok = false;
     double xn;
+    const float fin[4] = {(float)(st / ra), (float)log10(fmax(Vtn, 1e-30)), (float)log10(fmax(coef, 1e-30)),
+                          (float)ra};
     if (a.rs_guess && a.guess_net) {
-      float fin[4] = {(float)(st / ra), (float)log10(fmax(Vtn, 1e-30)), (float)log10(fmax(coef, 1e-30)), (float)ra};
-      double xg = (double)mlp_guess(a.guess_net, fin);
+      // learned guess: the root without radiation damping corrected by the network, then
+      // the same Newton iteration (capped); the plain solve from the reference's guess
+      // takes over whenever it does not converge
+      double xa = asinh(Vtn * exp(st / ra) / (2.0 * 1e-6));
+      double xg = xa + (double)mlp_residual(snet, fin);
       xn = newton_rs(xg, st, ra, Vtn, coef, 12, &its, &ok);
-      if (!ok || !isfinite(xn)) xn = newton_rs(x0, st, ra, Vtn, coef, 100, &its2, &ok);  // fallback: plain Newton
+      if (!ok || !isfinite(xn)) xn = newton_rs(x0, st, ra, Vtn, coef, 100, &its2, &ok);
     } else {
       xn = newton_rs(x0, st, ra, Vtn, coef, 100, &its, &ok);
+      if (a.rec && ok && ((unsigned)q2 * 7919u + (unsigned)it * 4u + (unsigned)a.irk) % (unsigned)a.rec_every == 0) {
+        // training sample: inputs and the residual target of the converged solve
+        unsigned slot = atomicAdd(a.rec_n, 1u);
+        if (slot < (unsigned)a.rec_cap) {
+          float* o = a.rec + 5ull * slot;
+          o[0] = fin[0]; o[1] = fin[1]; o[2] = fin[2]; o[3] = fin[3];
+          o[4] = (float)(xn - asinh(Vtn * exp(st / ra) / (2.0 * 1e-6)));
+        }
+      }
     }
-    atomicAdd(a.newton, (unsigned long long)(its + its2));
-    if (!ok) atomicAdd(a.newton + 1, 1ull);
+    {
+      // Newton statistics, one atomic per warp
+      const unsigned m = __activemask();
+      const unsigned sum_it = __reduce_add_sync(m, (unsigned)(its + its2));
+      const unsigned n_bad = __reduce_add_sync(m, ok ? 0u : 1u);
+      if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == __ffs(m) - 1) {
+        atomicAdd(a.newton, (unsigned long long)sum_it);
+        if (n_bad) atomicAdd(a.newton + 1, (unsigned long long)n_bad);
+      }
+    }
     double V = 2.0 * 1e-6 * exp(-st / ra) * sinh(xn);
     double T = ra * xn * fabs(tn);
     a.friction[q2] = (float)(ra * xn);

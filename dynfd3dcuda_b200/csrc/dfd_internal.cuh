@@ -132,6 +132,10 @@ struct FaultArgs {
   unsigned long long* newton;      // [0] iterations, [1] capped solves
   const int* it_dev;               // current step index (device copy, advanced inside graphs)
   const float* guess_net;          // learned-guess MLP weights or null
+  float* rec;                      // Newton sample recording buffer (cap x 5) or null
+  unsigned* rec_n;                 // samples recorded
+  int rec_cap;
+  int rec_every;                   // record one solve in rec_every (by node and stage)
   // scalars
   float rDH, DH, DT, rka, rkb, mu_d, viscosity;
   double dDT, smooth_load_T, f0, V0, fw, Vini;

@@ -130,6 +130,9 @@ int dfd_run_timed(dfd_ctx *ctx, int it0, int nsteps, float *total_ms, float *vol
  * kernel updates per stage (the interior box minus the fault band); a measurement aid
  * with no counterpart in the reference */
 int dfd_interior_stats(dfd_ctx *ctx, float *ms, long long *nodes);
+/* device time of the fault node kernel (trial traction and friction solve) during the last
+ * dfd_run_timed, summed over all stages; a measurement aid */
+int dfd_fault_node_ms(dfd_ctx *ctx, float *ms);
 /* The same slice as dfd_get_slice, gathered into a static device array instead of a
  * temporary allocation; this entry has no counterpart in the reference.  It is for callers
  * that must not allocate or free device memory while they run (fixed memory budget, or no
@@ -151,10 +154,33 @@ int dfd_output_open(dfd_ctx *ctx, const char *outdir);
 int dfd_output_write(dfd_ctx *ctx, int it_skip);
 int dfd_output_close(dfd_ctx *ctx);
 
-/* ---- learned initial guess of the rate-and-state Newton solve ---- */
-/* MLP 4 -> 32 -> 32 -> 1 weights, packed W1(32x4) b1(32) W2(32x32) b2(32) W3(32) b3(1)
- * plus 8 normalisation constants (mean, scale of the 4 inputs) = 1225 floats */
+/* ---- learned initial guess of the rate-and-state Newton solve (replaces the guess of
+ *      trial_ratestate.cu:695; the Newton iteration of :20-57 stays as the check and the
+ *      fallback).  No counterpart in the reference beyond that guess. ---- */
+/* MLP 4 -> 32 -> 32 -> 1 (tanh).  Inputs (psi/a, log10 Vhat, log10 coef, a) of the solve
+ * f(x) = 2 V0 e^{-psi/a} sinh x + coef x - Vhat; output the residual
+ * x* - asinh(Vhat e^{psi/a} / (2 V0)).  Parameter vector, DFD_MLP_PARAMS floats:
+ * W1(32x4) b1(32) W2(32x32) b2(32) W3(32) b3 | input mean(4) scale(4) output mean scale;
+ * the first DFD_MLP_TRAINABLE are trained. */
+#define DFD_MLP_PARAMS 1259
+#define DFD_MLP_TRAINABLE 1249
+/* load the weights and switch the learned guess on (weights NULL, n 0: switch it off) */
 int dfd_set_guess_net(dfd_ctx *ctx, const float *weights, int n);
+/* record (psi/a, log10 Vhat, log10 coef, a, x* residual) of one in `every` converged plain
+ * Newton solves (chosen by node, step and stage) into a device buffer of `capacity`
+ * samples (0 frees it); solves beyond the capacity are dropped */
+int dfd_newton_record(dfd_ctx *ctx, int capacity, int every);
+/* copy up to max recorded samples (5 floats each) to host, set *n, and empty the buffer */
+int dfd_newton_samples(dfd_ctx *ctx, float *host, int max, int *n);
+/* stand-alone training and inference on the current device, host arrays in and out:
+ * initialise (Xavier weights from seed, standardisation constants), batch forward
+ * (x: n x 4, y: n residuals), loss (mean squared standardised error) and its gradient
+ * (DFD_MLP_TRAINABLE floats), and minibatch Adam training for `epochs` epochs */
+int dfd_mlp_init(float *w, unsigned seed, const float *x_mean, const float *x_scale, float y_mean, float y_scale);
+int dfd_mlp_forward(const float *w, const float *x, int n, float *y);
+int dfd_mlp_loss_grad(const float *w, const float *x, const float *y, int n, double *loss, float *grad);
+int dfd_mlp_train(const float *x, const float *y, int n, int epochs, int batch, float lr, unsigned seed, float *w,
+                  float *loss_per_epoch);
 
 const char *dfd_error_string(int status);
 const char *dfd_last_error(const dfd_ctx *ctx);

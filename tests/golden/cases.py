@@ -55,6 +55,26 @@ def curved_geometry(NY, NZ, DH, dip_deg=60.0, hill_amp=500.0, hill_width=5e3, nh
     return np.stack([x, y + 0 * k, z + 0 * j]).astype(np.float32)
 
 
+def rough_geometry(NY, NZ, DH, ratio=1e-3, lmin=1e3, hurst=1.0, seed=0):
+    """Vertical fault with seeded self-similar roughness x(y, z): a Gaussian random field
+    with isotropic power spectrum P(k) ~ k^-(2 hurst + 2) (hurst = 1: self-similar), cut
+    at the minimum wavelength lmin by a 4-pole low-pass, scaled so that its rms height is
+    ratio x the strike length (the amplitude-to-wavelength ratio of a self-similar surface,
+    after jobs/tpv3_free_dh100m/func_selfsimilar2d.m)."""
+    fx = flat_geometry(NY, NZ, DH).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    ky = np.fft.fftfreq(NY, d=DH)[None, :]
+    kz = np.fft.fftfreq(NZ, d=DH)[:, None]
+    k = np.sqrt(ky ** 2 + kz ** 2)
+    amp = np.zeros_like(k)
+    nz = k > 0
+    amp[nz] = k[nz] ** (-(hurst + 1.0)) / np.sqrt(1.0 + (k[nz] * lmin) ** 8)
+    h = np.real(np.fft.ifft2(np.fft.fft2(rng.standard_normal((NZ, NY))) * amp))
+    h *= ratio * NY * DH / h.std()
+    fx[0] = h
+    return fx.astype(np.float32)
+
+
 def surface_normal(fxyz, DH):
     """Unit normal of the fault surface x(y,z) from central differences (the base
     vector the reference's job scripts project the stress tensor on)."""
@@ -213,7 +233,29 @@ def get_case(name):
         st = sw_stress(fx, fg, tn=-120e6, ts=-40e6)
         st = rs_fields(st, fx, seed=7, L=0.02, patch=(0.0, -500.0, 600.0), patch_dtau=45e6)
         return p, fx, st, None, None, dict(steps=40, every=20, volume=False)
+    if name == "rs_rough":
+        return rs_rough_case(76, 24, 40, seed=31, L=0.02, steps=60)
     raise KeyError(name)
+
+
+def rs_rough_case(NY, NX, NZ, seed=0, DH=100.0, steps=40, L=0.4):
+    """Rate-and-state slip law on a seeded self-similar rough fault (the learned-guess
+    configuration): a log-uniform in [0.01, 0.02] per node, b = 0.014, L = 0.4 m,
+    V0 = 1e-6 m/s, f0 = 0.6, fw = 0.2, Vw = 0.1 m/s, Vini = 1e-16 m/s; normal stress
+    120 MPa, shear 40 MPa, a 45 MPa nucleation patch of 3 km radius at 7.5 km depth (600 m
+    at 500 m depth on small grids) loaded over smooth_load_T.  The small test grid uses a
+    shorter L so that it slips within its few steps."""
+    fg = [1, NY, 1, NZ]
+    p = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.008, TMAX=steps * 0.008 + 0.004, PML_N=min(12, NX // 4),
+             PML_velocity=6000.0, INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=2, Fault_grid=fg,
+             RS_V0=1e-6, RS_f0=0.6, RS_fw=0.2, RS_Vini=1e-16, RS_L=0.4, smooth_load_T=0.5, NormalRefine=0)
+    fx = rough_geometry(NY, NZ, DH, seed=seed)
+    n = surface_normal(fx, DH)
+    st = sw_stress(fx, fg, tn=-120e6, ts=-40e6)
+    # the patch lies inside the non-united area (30-node borders below and along strike)
+    depth, radius = (7.5e3, 3.0e3) if NZ * DH >= 1.2e4 else (500.0, 600.0)
+    st = rs_fields(st, fx, seed=seed + 1, L=L, normal=n, patch=(0.0, -depth, radius), patch_dtau=45e6)
+    return p, fx, st, None, None, dict(steps=steps, every=steps // 2, volume=False)
 
 
 CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat"]
