@@ -22,6 +22,7 @@ void launch_fault_coef(const Dims& d, const float* M, float* tab, float* tabf, f
 void launch_wave_free(const Dims& d, const float* M, const float* Bx, const float* By, const float* Bz, float* mx,
                       float* my, cudaStream_t s);
 void launch_metric(const GridArgs& g, float* M, cudaStream_t s);
+void launch_plane_metric(const GridArgs& g, float* pl, float* rxa, cudaStream_t s);
 void launch_cfl(const GridArgs& g, const float* M, float* hmin, float* vpmax, cudaStream_t s);
 
 __global__ void set_it_kernel(int* it, int v) { *it = v; }
@@ -66,6 +67,8 @@ struct dfd_ctx {
   std::vector<void*> allocs;
   float* W[4] = {};
   float* M = nullptr;
+  float* mplane = nullptr;          // separable metric / media planes (12, nz, py)
+  float* rxa = nullptr;             // 1/(d x / d xi) per padded x index
   float *rB[3] = {}, *B[3] = {}, *Dp[3] = {}, *Ap[3] = {};
   float* aux[6][3] = {};
   float *mVx2Vz = nullptr, *mVy2Vz = nullptr;
@@ -84,6 +87,7 @@ struct dfd_ctx {
   int rec_every = 1;
   TileCtx tile;                    // tiled interior kernel (TMA maps)
   int* tile_err = nullptr;
+  int* tile_sched = nullptr;         // tiled kernel's unit counters
   bool use_tile = true;
   long long interior_nodes = 0;   // nodes the interior kernel updates per stage
   long long n_band_columns = 0;   // non-united (j, k) fault columns
@@ -200,6 +204,8 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   int rc = 0;
   for (int b = 0; b < 4 && !rc; b++) rc = dalloc(ctx, &ctx->W[b], 9 * d.nxyz);
   if (!rc) rc = dalloc(ctx, &ctx->M, 13 * d.nxyz);
+  if (!rc) rc = dalloc(ctx, &ctx->mplane, 12LL * d.py * d.nz);
+  if (!rc) rc = dalloc(ctx, &ctx->rxa, d.nx);
   int len[3] = {d.ni, d.nj, d.nk};
   for (int a = 0; a < 3 && !rc; a++) {
     rc = dalloc(ctx, &ctx->rB[a], len[a]);
@@ -244,14 +250,16 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->guess_net, DFD_MLP_PARAMS);
   if (!rc) rc = dalloc(ctx, &ctx->rec_n, 1);
   if (!rc) rc = dalloc(ctx, &ctx->tile_err, 1);
+  if (!rc) rc = dalloc(ctx, &ctx->tile_sched, 2);
   if (rc) { dfd_destroy(ctx); return rc; }
   // volume kernels: DFD_TILE=0 plain interior kernel + general shell kernel;
-  // 1 (default) TMA-tiled interior box + general shell kernel; 2 TMA tiles also over the
-  // PML slabs
+  // 1 (default) TMA-tiled interior box + general shell kernel; 2 TMA tiles over every
+  // node below the free-surface rows; 3 TMA tiles over the interior box widened over the
+  // two x slabs of the PML
   const char* tv = getenv("DFD_TILE");
-  int mode = tv && tv[0] >= '0' && tv[0] <= '2' ? tv[0] - '0' : 1;
-  ctx->use_tile = mode > 0 && tile_setup(&ctx->tile, d, ctx->W, ctx->M, ctx->tile_err, device);
-  ctx->tile.pml = mode == 2;
+  int mode = tv && tv[0] >= '0' && tv[0] <= '3' ? tv[0] - '0' : 1;
+  ctx->use_tile = mode > 0 && tile_setup(&ctx->tile, d, ctx->W, ctx->mplane, ctx->tile_err, ctx->tile_sched, device);
+  ctx->tile.pml = mode == 2 ? 1 : mode == 3 ? 3 : 0;
   *out = ctx;
   return DFD_OK;
 }
@@ -347,6 +355,7 @@ int dfd_precompute(dfd_ctx* ctx) {
   g.mu2 = p.bi_rho2 * p.bi_vs2 * p.bi_vs2;
   g.rho2 = p.bi_rho2;
   launch_metric(g, ctx->M, s);
+  launch_plane_metric(g, ctx->mplane, ctx->rxa, s);
   CK(cudaGetLastError());
   // CFL check (main.cu:323-345)
   size_t ncol = (size_t)d.nj * d.nk;
@@ -525,6 +534,8 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   va.mVx2Vz = ctx->mVx2Vz; va.mVy2Vz = ctx->mVy2Vz;
   va.dampx = ctx->damp[0]; va.dampy = ctx->damp[1]; va.dampz = ctx->damp[2];
   va.united = p.rupture ? ctx->ipl + I_UNITED * nf : nullptr;
+  va.rxa = ctx->rxa;
+  va.nxhalf = p.NX / 2;
   va.rDH = (float)(1.0 / p.DH); va.rka = rka; va.rkb = rkb;
   va.irk = irk; va.freenode = p.free_surface;
   long long nodes =

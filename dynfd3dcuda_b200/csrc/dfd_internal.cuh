@@ -90,6 +90,8 @@ struct VolArgs {
   const float* __restrict__ dampy;
   const float* __restrict__ dampz;
   const int* __restrict__ united;    // (NZ, NY) or null when the fault is off
+  const float* __restrict__ rxa;     // 1/(d x / d xi) per padded x index (separable metric)
+  int nxhalf;                        // bimaterial split: padded x index < nxhalf is side 1
   float rDH, rka, rkb;
   int irk, freenode;
 };
@@ -161,21 +163,22 @@ struct TileMaps {
   CUtensorMap win;  // stencil input, halo box
   CUtensorMap w0;   // step-start state, pointwise box
   CUtensorMap t;    // RK accumulator, pointwise box
-  CUtensorMap m9;   // metric, fields 0..8
-  CUtensorMap m3;   // lam mu rho, fields 10..12
+  CUtensorMap plane;  // separable metric / media planes (12, nz, py)
 };
 // Per-context state of the tiled interior kernel: maps of the four volume buffers and of
 // the metric (fixed addresses, encoded once), the error flag, the SM count.
 struct TileCtx {
   CUtensorMap halo[4];
   CUtensorMap centre[4];
-  CUtensorMap m9, m3;
+  CUtensorMap plane;
   int* err = nullptr;
+  int* sched = nullptr;  // unit counter and finished-CTA counter (zero between launches)
   int nsm = 0;
-  int pml = 0;  // 1: the tiles also cover the PML slabs
+  int pml = 0;  // 1: the tiles cover every PML slab; 3: the two x slabs only
   bool ok = false;
 };
-bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* M, int* err, int device);
+bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, int* err, int* sched,
+                int device);
 bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi,
                  cudaStream_t s);
 

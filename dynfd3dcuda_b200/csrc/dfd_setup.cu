@@ -119,6 +119,67 @@ __global__ void cfl_kernel(GridArgs g, const float* M, float* hmin, float* vpmax
   vpmax[f] = (float)vm;
 }
 
+// Separable factors of the same discrete metric for the tiled interior kernel.  With
+// v1 = (a, 0, 0) (a = d xline / d xi), v2 = (p, q, r) and v3 = (s, t, w) the derivatives
+// along eta and zeta of the fault surface (fx, fy, fz), the inverse metric of
+// metric_kernel is
+//   xi = (1, (r s - p w) / D, (p t - q s) / D) / a,  et = (0, w, -t) / D,
+//   zt = (0, -r, q) / D,  D = q w - r t,
+// so it splits into six (j, k) planes U V ety etz zty ztz and the 1-D line 1/a(i); the
+// media are (j, k) planes for the two sides of the bimaterial split (equal otherwise).
+// Planes are stored (12, nz, py) with the volume row offset, so that the tiled kernel's
+// TMA boxes use the volume coordinates.
+__global__ void plane_metric_kernel(GridArgs g, float* pl, float* rxa) {
+  const Dims& d = g.d;
+  int j = blockIdx.x * blockDim.x + threadIdx.x + 3;
+  int k = blockIdx.y * blockDim.y + threadIdx.y + 3;
+  if (blockIdx.x == 0 && blockIdx.y == 0) {
+    for (int i = 3 + threadIdx.x + threadIdx.y * blockDim.x; i < d.nx - 3; i += blockDim.x * blockDim.y)
+      rxa[i] = (float)(1.0 / (0.5 * g.rDH * (g.xl[i + 1] - g.xl[i - 1])));
+  }
+  if (j >= d.ny - 3 || k >= d.nz - 3) return;
+  auto at = [&](int jj, int kk, int c) {
+    long long f = jj + (long long)kk * d.ny;
+    return c == 0 ? g.fx[f] : c == 1 ? g.fy[f] : g.fz[f];
+  };
+  double v2[3], v3[3];
+  for (int c = 0; c < 3; c++) {
+    v2[c] = 0.5 * g.rDH * (at(j + 1, k, c) - at(j - 1, k, c));
+    v3[c] = 0.5 * g.rDH * (at(j, k + 1, c) - at(j, k - 1, c));
+  }
+  double pp = v2[0], q = v2[1], r = v2[2], sv = v3[0], t = v3[1], w = v3[2];
+  double D = q * w - r * t;
+  const long long np = (long long)d.py * d.nz, o = (j + d.oy) + (long long)k * d.py;
+  pl[0 * np + o] = (float)((r * sv - pp * w) / D);
+  pl[1 * np + o] = (float)((pp * t - q * sv) / D);
+  pl[2 * np + o] = (float)(w / D);
+  pl[3 * np + o] = (float)(-t / D);
+  pl[4 * np + o] = (float)(-r / D);
+  pl[5 * np + o] = (float)(q / D);
+  double m[2][3];
+  if (g.nlayer > 0) {
+    double depth = -at(j, k, 2);
+    int l0 = g.nlayer - 1;
+    for (int l = g.nlayer - 1; l >= 0; l--)
+      if (depth > (double)g.layers[4 * l]) { l0 = l; break; }
+    double rh = g.layers[4 * l0 + 1], vp = g.layers[4 * l0 + 2], vs = g.layers[4 * l0 + 3];
+    m[0][0] = m[1][0] = rh * (vp * vp - 2 * vs * vs);
+    m[0][1] = m[1][1] = rh * vs * vs;
+    m[0][2] = m[1][2] = rh;
+  } else {
+    m[0][0] = g.lam1; m[0][1] = g.mu1; m[0][2] = g.rho1;
+    m[1][0] = g.lam2; m[1][1] = g.mu2; m[1][2] = g.rho2;
+  }
+  for (int sd = 0; sd < 2; sd++)
+    for (int c = 0; c < 3; c++) pl[(6 + 3 * sd + c) * np + o] = (float)m[sd][c];
+}
+
+void launch_plane_metric(const GridArgs& g, float* pl, float* rxa, cudaStream_t s) {
+  dim3 b(32, 4);
+  dim3 gr((g.d.ny - 6 + 31) / 32, (g.d.nz - 6 + 3) / 4);
+  plane_metric_kernel<<<gr, b, 0, s>>>(g, pl, rxa);
+}
+
 void launch_metric(const GridArgs& g, float* M, cudaStream_t s) {
   dim3 b(32, 4, 2);
   dim3 gr((g.d.ny - 6 + 31) / 32, (g.d.nz - 6 + 3) / 4, (g.d.nx - 6 + 1) / 2);

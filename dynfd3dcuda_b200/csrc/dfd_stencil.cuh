@@ -21,11 +21,31 @@ __device__ __forceinline__ void axis_terms(const float* d, float e0, float e1, f
   D[8] = (d[1] * e2 + d[2] * e1) * mu;
 }
 
-// PML auxiliary update of one face for this node: accumulates -aux/beta into p[] and
-// advances aux in place with the RK4 registers (pmlx.cu:165-208, rk4.cu:208-255).
-__device__ __forceinline__ void pml_face(const VolArgs& a, int face, long long qa, long long st, float rb, float b,
-                                         float dd, float al, const float* Dv, const float* dzv, float ez0,
-                                         float ez1, float ez2, float lam, float mu, float* p) {
+// ADE state of one PML face for this node, loaded ahead of its use: current value, and the
+// RK registers the stage needs (accumulator for stages 1..3, step start for stages 1, 2).
+struct PmlState {
+  float w[9], t[9], w0[9];
+};
+__device__ __forceinline__ void pml_load(const VolArgs& a, int face, long long qa, long long st, PmlState& ps) {
+  const float* aux = a.aux[face];
+  const float* aux0 = a.aux0[face];
+  const float* auxT = a.auxT[face];
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    const long long x = f * st + qa;
+    ps.w[f] = aux[x];
+    if (a.irk >= 1) ps.t[f] = auxT[x];
+    if (a.irk == 1 || a.irk == 2) ps.w0[f] = aux0[x];
+  }
+}
+
+// PML auxiliary update of one face for this node from its loaded state: accumulates
+// -aux/beta into p[] and advances aux in place with the RK4 registers (pmlx.cu:165-208,
+// rk4.cu:208-255).
+__device__ __forceinline__ void pml_update(const VolArgs& a, int face, long long qa, long long st, float rb, float b,
+                                           float dd, float al, const float* Dv, const float* dzv, float ez0,
+                                           float ez1, float ez2, float lam, float mu, const PmlState& ps,
+                                           float* p) {
   float* aux = a.aux[face];
   float* aux0 = a.aux0[face];
   float* auxT = a.auxT[face];
@@ -40,33 +60,34 @@ __device__ __forceinline__ void pml_face(const VolArgs& a, int face, long long q
     add[4] = c * mu * (ez2 * dzv[0] + ez0 * dzv[2]);
     add[5] = c * mu * (ez2 * dzv[1] + ez1 * dzv[2]);
   }
-  // all loads first: the compiler cannot prove the three buffers distinct, and a load
-  // issued after a store would wait for a full memory round trip per field
-  float w[9], t[9], w0[9];
 #pragma unroll
   for (int f = 0; f < 9; f++) {
     const long long x = f * st + qa;
-    w[f] = aux[x];
-    if (a.irk >= 1) t[f] = auxT[x];
-    if (a.irk == 1 || a.irk == 2) w0[f] = aux0[x];
-  }
-#pragma unroll
-  for (int f = 0; f < 9; f++) {
-    const long long x = f * st + qa;
-    p[f] += -w[f] * rb;
-    float h = ad * w[f] + dd * Dv[f];
+    p[f] += -ps.w[f] * rb;
+    float h = ad * ps.w[f] + dd * Dv[f];
     if (dzv && f >= 3) h += add[f - 3];
     if (a.irk == 0) {
-      aux0[x] = w[f];
-      auxT[x] = fmaf(a.rkb, h, w[f]);
-      aux[x] = fmaf(a.rka, h, w[f]);
+      aux0[x] = ps.w[f];
+      auxT[x] = fmaf(a.rkb, h, ps.w[f]);
+      aux[x] = fmaf(a.rka, h, ps.w[f]);
     } else if (a.irk < 3) {
-      auxT[x] = fmaf(a.rkb, h, t[f]);
-      aux[x] = fmaf(a.rka, h, w0[f]);
+      auxT[x] = fmaf(a.rkb, h, ps.t[f]);
+      aux[x] = fmaf(a.rka, h, ps.w0[f]);
     } else {
-      aux[x] = fmaf(a.rkb, h, t[f]);
+      aux[x] = fmaf(a.rkb, h, ps.t[f]);
     }
   }
+}
+
+// Both steps at once: every load of the face precedes every store (the compiler cannot
+// prove the three buffers distinct, and a load issued after a store would wait for a full
+// memory round trip per field).
+__device__ __forceinline__ void pml_face(const VolArgs& a, int face, long long qa, long long st, float rb, float b,
+                                         float dd, float al, const float* Dv, const float* dzv, float ez0,
+                                         float ez1, float ez2, float lam, float mu, float* p) {
+  PmlState ps;
+  pml_load(a, face, qa, st, ps);
+  pml_update(a, face, qa, st, rb, b, dd, al, Dv, dzv, ez0, ez1, ez2, lam, mu, ps, p);
 }
 
 // RK4 register update of the nine fields of node q with right-hand side h (+ p), then the

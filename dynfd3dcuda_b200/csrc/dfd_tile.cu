@@ -15,9 +15,9 @@
 // state, read and written in global memory); the others the lean interior path.  Outputs
 // (Wout, T) are written straight from registers.
 //
-// The kernel is persistent: one CTA per SM walks its units (tile column x chunk) and the
-// copy stream runs across unit boundaries, so the next unit's planes arrive while the
-// current one finishes.
+// The kernel is persistent: one CTA per SM takes units (tile column x chunk) from a global
+// counter, and its copy stream runs across unit boundaries, so the next unit's planes
+// arrive while the current one finishes.
 //
 // The right-hand side follows the reference's wave.cu:8-204, pmlx.cu / pmly.cu / pmlz.cu
 // and rk4.cu:20-33, as the general kernel in dfd_volume.cu does.
@@ -37,12 +37,14 @@ constexpr int HH = TK + 4;           // halo box height (z): 1 + 3 rows, side se
 constexpr int HBOX = HW * HH;        // floats per field of a halo box
 constexpr int HSLOT = 9 * HBOX;      // floats per stencil plane slot
 constexpr int PB = TJ * TK;          // floats per field of a pointwise box
-constexpr int PSLOT = 30 * PB;       // metric 9 + lam mu rho + W0 9 + T 9
-constexpr int NS = 7, NP = 3;        // ring depths (stencil planes, pointwise planes)
-constexpr size_t SMEM_BYTES = (size_t)(NS * HSLOT + NP * PSLOT) * 4 + 2 * (NS + NP) * 8;
+constexpr int PSLOT = 18 * PB;       // RK registers W0 9 + T 9
+constexpr int QSLOT = 12 * PB;       // metric / media planes of a unit: U V ety etz zty ztz, 2 x (lam mu rho)
+constexpr int NS = 8, NP = 3, NQ = 2;  // ring depths (stencil planes, RK registers, unit planes)
+constexpr size_t SMEM_BYTES = (size_t)(NS * HSLOT + NP * PSLOT + NQ * QSLOT) * 4 + 2 * (NS + NP + NQ) * 8 + NQ * 4;
 constexpr long long WAIT_LIMIT = 1LL << 22;  // polls of one mbarrier before giving up
 static_assert(SMEM_BYTES <= 232448, "tile ring exceeds the shared memory of one CTA");
-static_assert((HSLOT * 4) % 128 == 0 && (PSLOT * 4) % 128 == 0 && (PB * 4) % 128 == 0, "slot alignment");
+static_assert((HSLOT * 4) % 128 == 0 && (PSLOT * 4) % 128 == 0 && (QSLOT * 4) % 128 == 0 && (PB * 4) % 128 == 0,
+              "slot alignment");
 }  // namespace
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -80,6 +82,14 @@ __device__ __forceinline__ void tma_load4(float* dst, const CUtensorMap* map, in
       : "memory");
 }
 
+__device__ __forceinline__ void tma_load3(float* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(b))
+      : "memory");
+}
+
 // one-sided 5-point operators on values (v0..v4 = the five stencil points in order)
 template <int F>
 __device__ __forceinline__ float d5v(float v0, float v1, float v2, float v3, float v4) {
@@ -114,16 +124,28 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
 
+// Metric and media of a node of the tiled box: x row (xi), y row (eta), z row (zeta) and
+// the elastic constants (the separable factors of dfd_setup.cu's plane_metric_kernel; the
+// x components of eta and zeta are exactly zero there and in the stored metric).
+struct NodeMetric {
+  float ex0, ex1, ex2, ey1, ey2, ez1, ez2, lam, mu, rrho;
+};
+
 // Right-hand side of a node inside at least one PML slab: every axis with its 1/beta and
 // the ADE auxiliary update of the faces the node lies in (reference wave.cu:8-204 with
 // pmlx.cu / pmly.cu / pmlz.cu).  xv[m] are the five x-stencil planes, cur the plane x.
 template <int FX, int FY, int FZ>
 __device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* const* xv, const float* cur,
-                                               const float* P, int i, int j, int k, float* hv) {
+                                               const NodeMetric& g, int i, int j, int k, float* hv) {
   const Dims& d = a.d;
   const float r = a.rDH;
-  const float lam = P[9 * PB], mu = P[10 * PB], rrho = 1.0f / P[11 * PB];
   const float rb1 = __ldg(a.rBx + i), rb2 = __ldg(a.rBy + j), rb3 = __ldg(a.rBz + k);
+  // the x-face ADE state first, so that its latency overlaps the stencil evaluation
+  const bool px1 = a.aux[0] && i < d.N, px2 = a.aux[1] && i >= d.ni - d.N;
+  const long long stx = (long long)d.N * d.nj * d.nk;
+  const long long qax = j + (long long)k * d.nj + (long long)(px1 ? i : i - (d.ni - d.N)) * d.nj * d.nk;
+  PmlState psx;
+  if (px1 || px2) pml_load(a, px1 ? 0 : 1, qax, stx, psx);
   float p[9], D[9], dv[9];
 #pragma unroll
   for (int f = 0; f < 9; f++) p[f] = 0.0f;
@@ -133,21 +155,16 @@ __device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* co
     const int o = f * HBOX;
     dv[f] = d5v<FX>(xv[0][o], xv[1][o], xv[2][o], xv[3][o], xv[4][o]) * r;
   }
-  axis_terms(dv, P[0], P[PB], P[2 * PB], lam, mu, rrho, D);
+  axis_terms(dv, g.ex0, g.ex1, g.ex2, g.lam, g.mu, g.rrho, D);
 #pragma unroll
   for (int f = 0; f < 9; f++) hv[f] = D[f] * rb1;
-  const bool px1 = a.aux[0] && i < d.N, px2 = a.aux[1] && i >= d.ni - d.N;
-  if (px1 || px2) {
-    long long st = (long long)d.N * d.nj * d.nk;
-    int ia = px1 ? i : i - (d.ni - d.N);
-    long long qa = j + (long long)k * d.nj + (long long)ia * d.nj * d.nk;
-    pml_face(a, px1 ? 0 : 1, qa, st, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D, nullptr, 0.f,
-             0.f, 0.f, lam, mu, p);
-  }
+  if (px1 || px2)
+    pml_update(a, px1 ? 0 : 1, qax, stx, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D, nullptr, 0.f,
+               0.f, 0.f, g.lam, g.mu, psx, p);
   // y
 #pragma unroll
   for (int f = 0; f < 9; f++) dv[f] = d5s<FY, 1>(cur + f * HBOX) * r;
-  axis_terms(dv, P[3 * PB], P[4 * PB], P[5 * PB], lam, mu, rrho, D);
+  axis_terms(dv, 0.0f, g.ey1, g.ey2, g.lam, g.mu, g.rrho, D);
 #pragma unroll
   for (int f = 0; f < 9; f++) hv[f] += D[f] * rb2;
   const bool py1 = a.aux[2] && j < d.N, py2 = a.aux[3] && j >= d.nj - d.N;
@@ -156,12 +173,12 @@ __device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* co
     int ja = py1 ? j : j - (d.nj - d.N);
     long long qa = ja + (long long)k * d.N + (long long)i * d.N * d.nk;
     pml_face(a, py1 ? 2 : 3, qa, st, rb2, __ldg(a.By + j), __ldg(a.Dpy + j), __ldg(a.Apy + j), D, nullptr, 0.f,
-             0.f, 0.f, lam, mu, p);
+             0.f, 0.f, g.lam, g.mu, p);
   }
   // z
 #pragma unroll
   for (int f = 0; f < 9; f++) dv[f] = d5s<FZ, HW>(cur + f * HBOX) * r;
-  axis_terms(dv, P[6 * PB], P[7 * PB], P[8 * PB], lam, mu, rrho, D);
+  axis_terms(dv, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D);
 #pragma unroll
   for (int f = 0; f < 9; f++) hv[f] += D[f] * rb3;
   const bool pz1 = a.aux[4] && k < d.N, pz2 = a.aux[5] && k >= d.nk - d.N;
@@ -170,7 +187,7 @@ __device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* co
     int ka = pz1 ? k : k - (d.nk - d.N);
     long long qa = j + (long long)ka * d.nj + (long long)i * d.nj * d.N;
     pml_face(a, pz1 ? 4 : 5, qa, st, rb3, __ldg(a.Bz + k), __ldg(a.Dpz + k), __ldg(a.Apz + k), D, nullptr, 0.f,
-             0.f, 0.f, lam, mu, p);
+             0.f, 0.f, g.lam, g.mu, p);
   }
 #pragma unroll
   for (int f = 0; f < 9; f++) hv[f] += p[f];
@@ -178,29 +195,38 @@ __device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* co
 
 // Warp NCW issues the copies; warps 0..NCW-1 compute one node each per plane.  Each ring
 // slot has a "full" barrier (completed by the copy's transaction bytes) and an "empty"
-// barrier (one arrival per computing warp once it has finished reading the slot).  At
+// barrier (one arrival per computing warp once it has finished reading the slot).  Three
+// rings: stencil planes (NS), RK registers of the step (NP; none at stage 0, whose
+// step-start values are the stencil input), metric/media planes of the unit (NQ).  At
 // most 160 registers, so that a block of the fault band kernel fits beside the CTA.
 template <int FX, int FY, int FZ>
 __global__ void __maxnreg__(160)
-    volume_tile_kernel(const __grid_constant__ TileMaps mp, const VolArgs a, const TileSched sc, int* err) {
+    volume_tile_kernel(const __grid_constant__ TileMaps mp, const VolArgs a, const TileSched sc, int* err,
+                       int* sched) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   float* win = reinterpret_cast<float*>(smraw);
   float* pw = win + NS * HSLOT;
-  uint64_t* full_w = reinterpret_cast<uint64_t*>(pw + NP * PSLOT);
+  float* qs = pw + NP * PSLOT;
+  uint64_t* full_w = reinterpret_cast<uint64_t*>(qs + NQ * QSLOT);
   uint64_t* empty_w = full_w + NS;
   uint64_t* full_p = empty_w + NS;
   uint64_t* empty_p = full_p + NP;
+  uint64_t* full_q = empty_p + NP;
+  uint64_t* empty_q = full_q + NQ;
+  int* qunit = reinterpret_cast<int*>(empty_q + NQ);  // unit of each plane slot (-1: no more)
   const Dims& d = a.d;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int XLO = FX == 1 ? -1 : -3;  // first stencil plane relative to x
   constexpr int RZ = FZ == 1 ? 1 : 3;     // row of the tile's first z node inside the halo box
   const int irk = a.irk;
+  const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1, usep = needW0 || needT;
   const int ntile = sc.ntj * sc.ntk;
   const int G = gridDim.x;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; s++) { mbar_init(full_w + s, 1); mbar_init(empty_w + s, NCW); }
     for (int s = 0; s < NP; s++) { mbar_init(full_p + s, 1); mbar_init(empty_p + s, NCW); }
+    for (int s = 0; s < NQ; s++) { mbar_init(full_q + s, 1); mbar_init(empty_q + s, NCW); }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fence_async_shared();
   }
@@ -209,17 +235,31 @@ __global__ void __maxnreg__(160)
   if (warp == NCW) {
     // ---------------- copy-issuing warp (one lane)
     if (lane != 0) return;
-    const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1;
-    const unsigned ptx = (12 + (needW0 ? 9 : 0) + (needT ? 9 : 0)) * PB * 4;
-    Ring wr, pr;
-    int wcount = 0, pcount = 0;
+    const unsigned ptx = ((needW0 ? 9 : 0) + (needT ? 9 : 0)) * PB * 4;
+    Ring wr, pr, qr;
+    int wcount = 0, pcount = 0, qcount = 0;
     bool ok = true;
-    for (int u = blockIdx.x; u < sc.nunits && ok; u += G) {
+    // units are taken from a global counter, so that CTAs that start late (their SM busy
+    // with a concurrent kernel) simply take fewer
+    while (ok) {
+      const int u = atomicAdd(sched, 1);
+      if (qcount >= NQ && !(ok = mbar_wait(empty_q + qr.slot, qr.phase ^ 1))) break;
+      if (u >= sc.nunits) {
+        qunit[qr.slot] = -1;  // tell the computing warps that there is no further unit
+        mbar_arrive(full_q + qr.slot);
+        break;
+      }
       const int tc = u / ntile, ru = u % ntile;
       const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
       const int j0 = sc.lo_y + (ru % sc.ntj) * TJ, k0 = sc.lo_z + (ru / sc.ntj) * TK;
       const int cw0 = j0 + 3 + d.oy - 4, cw1 = k0 + 3 - RZ, cp0 = j0 + 3 + d.oy, cp1 = k0 + 3;
       const int nst = ie - ib;
+      // metric / media planes of the unit, with the unit's index
+      qunit[qr.slot] = u;
+      mbar_expect_tx(full_q + qr.slot, QSLOT * 4);
+      tma_load3(qs + qr.slot * QSLOT, &mp.plane, cp0, cp1, 0, full_q + qr.slot);
+      qr.next<NQ>();
+      qcount++;
       for (int m = 0; m < nst + 4 && ok; m++) {
         // stencil plane m of the unit (first needed by step m - 4)
         if (wcount >= NS && !(ok = mbar_wait(empty_w + wr.slot, wr.phase ^ 1))) break;
@@ -227,17 +267,15 @@ __global__ void __maxnreg__(160)
         tma_load4(win + wr.slot * HSLOT, &mp.win, cw0, cw1, ib + XLO + m + 3, 0, full_w + wr.slot);
         wr.next<NS>();
         wcount++;
-        if (m < 4) continue;
-        // pointwise streams of step m - 4
+        if (m < 4 || !usep) continue;
+        // RK registers of step m - 4
         if (pcount >= NP && !(ok = mbar_wait(empty_p + pr.slot, pr.phase ^ 1))) break;
         uint64_t* b = full_p + pr.slot;
         float* dst = pw + pr.slot * PSLOT;
         const int cp2 = ib + (m - 4) + 3;
         mbar_expect_tx(b, ptx);
-        tma_load4(dst, &mp.m9, cp0, cp1, cp2, 0, b);
-        tma_load4(dst + 9 * PB, &mp.m3, cp0, cp1, cp2, 10, b);
-        if (needW0) tma_load4(dst + 12 * PB, &mp.w0, cp0, cp1, cp2, 0, b);
-        if (needT) tma_load4(dst + 21 * PB, &mp.t, cp0, cp1, cp2, 0, b);
+        if (needW0) tma_load4(dst, &mp.w0, cp0, cp1, cp2, 0, b);
+        if (needT) tma_load4(dst + 9 * PB, &mp.t, cp0, cp1, cp2, 0, b);
         pr.next<NP>();
         pcount++;
       }
@@ -247,6 +285,13 @@ __global__ void __maxnreg__(160)
       atomicExch(err, 1);
       for (int c = max(0, wcount - NS); c < wcount; c++) mbar_wait(full_w + c % NS, (c / NS) & 1);
       for (int c = max(0, pcount - NP); c < pcount; c++) mbar_wait(full_p + c % NP, (c / NP) & 1);
+      for (int c = max(0, qcount - NQ); c < qcount; c++) mbar_wait(full_q + c % NQ, (c / NQ) & 1);
+    }
+    // the last CTA to stop taking units resets the counter for the next launch
+    __threadfence();
+    if (atomicAdd(sched + 1, 1) == G - 1) {
+      atomicExch(sched, 0);
+      atomicExch(sched + 1, 0);
     }
     return;
   }
@@ -256,9 +301,15 @@ __global__ void __maxnreg__(160)
   const float r = a.rDH;
   const int hc = (warp + RZ) * HW + lane + 4;  // node inside a halo field box
   const int pc = warp * TJ + lane;             // node inside a pointwise field box
-  Ring wr, pr;  // next stencil plane to wait for; pointwise slot of the step
-  int sb = 0;   // slot of the step's first stencil plane
-  for (int u = blockIdx.x; u < sc.nunits; u += G) {
+  Ring wr, pr, qr;  // next stencil plane to wait for; RK-register slot of the step; unit planes
+  int sb = 0;       // slot of the step's first stencil plane
+  for (;;) {
+    if (!__all_sync(0xffffffffu, mbar_wait(full_q + qr.slot, qr.phase))) {
+      if (lane == 0) atomicExch(err, 1);
+      return;
+    }
+    const int u = qunit[qr.slot];
+    if (u < 0) break;
     const int tc = u / ntile, ru = u % ntile;
     const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
     const int j = sc.lo_y + (ru % sc.ntj) * TJ + lane, k = sc.lo_z + (ru / sc.ntj) * TK + warp;
@@ -270,13 +321,15 @@ __global__ void __maxnreg__(160)
     if (active && a.dampx) dyz = fminf(__ldg(a.dampy + j + 3), __ldg(a.dampz + k + 3));
     const long long qyz = idx3(d, 0, j + 3, k + 3);
     const int nst = ie - ib;
+    const float* Q = qs + qr.slot * QSLOT + pc;
+    const float mU = Q[0], mV = Q[PB], ety = Q[2 * PB], etz = Q[3 * PB], zty = Q[4 * PB], ztz = Q[5 * PB];
     for (int s = 0; s < nst; s++) {
       bool ok = true;
       for (int c = s == 0 ? 5 : 1; c > 0; c--) {
         ok = ok && mbar_wait(full_w + wr.slot, wr.phase);
         wr.next<NS>();
       }
-      ok = ok && mbar_wait(full_p + pr.slot, pr.phase);
+      if (usep) ok = ok && mbar_wait(full_p + pr.slot, pr.phase);
       if (!__all_sync(0xffffffffu, ok)) {
         if (lane == 0) atomicExch(err, 1);
         return;
@@ -294,44 +347,66 @@ __global__ void __maxnreg__(160)
         const float* xs3 = win + s3 * HSLOT + hc;
         const float* xs4 = win + s4 * HSLOT + hc;
         const float* cur = FX == 1 ? xs1 : xs3;  // plane x itself
+        // metric (xi row from the 1-D factor) and media of the side of the bimaterial split
+        NodeMetric g;
+        const float rA = __ldg(a.rxa + i + 3);
+        g.ex0 = rA; g.ex1 = mU * rA; g.ex2 = mV * rA;
+        g.ey1 = ety; g.ey2 = etz; g.ez1 = zty; g.ez2 = ztz;
+        const int side = i + 3 < a.nxhalf ? 6 : 9;
+        g.lam = Q[side * PB]; g.mu = Q[(side + 1) * PB]; g.rrho = 1.0f / Q[(side + 2) * PB];
         const bool pml = pml_yz || (a.aux[0] && i < d.N) || (a.aux[1] && i >= d.ni - d.N);
         float hv[9];
         if (pml) {
           const float* xv[5] = {xs0, xs1, xs2, xs3, xs4};
-          tile_pml_point<FX, FY, FZ>(a, xv, cur, P, i, j, k, hv);
+          tile_pml_point<FX, FY, FZ>(a, xv, cur, g, i, j, k, hv);
         } else {
-          const float lam = P[9 * PB], mu = P[10 * PB];
-          const float rrho = 1.0f / P[11 * PB];
+          const float lam = g.lam, mu = g.mu, rrho = g.rrho;
           const float l2m = lam + 2.0f * mu;
           float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f, h8 = 0.f;
-#define DFD_TAXIS(DER, MO)                                                                          \
+          // the x row has three components; the y and z rows have no x component, so the
+          // terms with it (exact zeros) and the derivative of Txx along y and z drop out
+          {
+            const float e0 = g.ex0, e1 = g.ex1, e2 = g.ex2;
+            float dv;
+#define DFD_DERX(f) d5v<FX>(xs0[(f) * HBOX], xs1[(f) * HBOX], xs2[(f) * HBOX], xs3[(f) * HBOX], xs4[(f) * HBOX])
+            dv = DFD_DERX(0) * r;
+            h3 += dv * e0 * l2m; h4 += dv * e0 * lam; h5 += dv * e0 * lam; h6 += dv * e1 * mu; h7 += dv * e2 * mu;
+            dv = DFD_DERX(1) * r;
+            h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h6 += dv * e0 * mu; h8 += dv * e2 * mu;
+            dv = DFD_DERX(2) * r;
+            h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h7 += dv * e0 * mu; h8 += dv * e1 * mu;
+            const float er0 = e0 * rrho, er1 = e1 * rrho, er2 = e2 * rrho;
+            dv = DFD_DERX(3) * r; h0 += dv * er0;
+            dv = DFD_DERX(4) * r; h1 += dv * er1;
+            dv = DFD_DERX(5) * r; h2 += dv * er2;
+            dv = DFD_DERX(6) * r; h0 += dv * er1; h1 += dv * er0;
+            dv = DFD_DERX(7) * r; h0 += dv * er2; h2 += dv * er0;
+            dv = DFD_DERX(8) * r; h1 += dv * er2; h2 += dv * er1;
+#undef DFD_DERX
+          }
+#define DFD_TAXIS0(DER, E1, E2)                                                                     \
   {                                                                                                 \
-    const float e0 = P[(MO) * PB], e1 = P[((MO) + 1) * PB], e2 = P[((MO) + 2) * PB];                 \
+    const float e1 = (E1), e2 = (E2);                                                               \
     float dv;                                                                                       \
-    dv = DER(0) * r;                                                                                \
-    h3 += dv * e0 * l2m; h4 += dv * e0 * lam; h5 += dv * e0 * lam; h6 += dv * e1 * mu; h7 += dv * e2 * mu; \
+    dv = DER(0) * r; h6 += dv * e1 * mu; h7 += dv * e2 * mu;                                        \
     dv = DER(1) * r;                                                                                \
-    h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h6 += dv * e0 * mu; h8 += dv * e2 * mu; \
+    h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h8 += dv * e2 * mu;              \
     dv = DER(2) * r;                                                                                \
-    h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h7 += dv * e0 * mu; h8 += dv * e1 * mu; \
-    const float er0 = e0 * rrho, er1 = e1 * rrho, er2 = e2 * rrho;                                  \
-    dv = DER(3) * r; h0 += dv * er0;                                                                \
+    h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h8 += dv * e1 * mu;              \
+    const float er1 = e1 * rrho, er2 = e2 * rrho;                                                   \
     dv = DER(4) * r; h1 += dv * er1;                                                                \
     dv = DER(5) * r; h2 += dv * er2;                                                                \
-    dv = DER(6) * r; h0 += dv * er1; h1 += dv * er0;                                                \
-    dv = DER(7) * r; h0 += dv * er2; h2 += dv * er0;                                                \
+    dv = DER(6) * r; h0 += dv * er1;                                                                \
+    dv = DER(7) * r; h0 += dv * er2;                                                                \
     dv = DER(8) * r; h1 += dv * er2; h2 += dv * er1;                                                \
   }
-#define DFD_DERX(f) d5v<FX>(xs0[(f) * HBOX], xs1[(f) * HBOX], xs2[(f) * HBOX], xs3[(f) * HBOX], xs4[(f) * HBOX])
 #define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HBOX)
 #define DFD_DERZ(f) d5s<FZ, HW>(cur + (f) * HBOX)
-          DFD_TAXIS(DFD_DERX, 0)
-          DFD_TAXIS(DFD_DERY, 3)
-          DFD_TAXIS(DFD_DERZ, 6)
-#undef DFD_DERX
+          DFD_TAXIS0(DFD_DERY, g.ey1, g.ey2)
+          DFD_TAXIS0(DFD_DERZ, g.ez1, g.ez2)
 #undef DFD_DERY
 #undef DFD_DERZ
-#undef DFD_TAXIS
+#undef DFD_TAXIS0
           hv[0] = h0; hv[1] = h1; hv[2] = h2; hv[3] = h3; hv[4] = h4;
           hv[5] = h5; hv[6] = h6; hv[7] = h7; hv[8] = h8;
         }
@@ -347,10 +422,10 @@ __global__ void __maxnreg__(160)
             a.T[x] = fmaf(a.rkb, hv[f], w0);
             w = fmaf(a.rka, hv[f], w0);
           } else if (irk < 3) {
-            a.T[x] = fmaf(a.rkb, hv[f], P[(21 + f) * PB]);
-            w = fmaf(a.rka, hv[f], P[(12 + f) * PB]);
+            a.T[x] = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
+            w = fmaf(a.rka, hv[f], P[f * PB]);
           } else {
-            w = fmaf(a.rkb, hv[f], P[(21 + f) * PB]);
+            w = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
           }
           a.Wout[x] = w * damp;
         }
@@ -362,13 +437,15 @@ __global__ void __maxnreg__(160)
           mbar_arrive(empty_w + sb);
         } else {
           for (int m = 0, sl = sb; m < 5; m++, sl = sl + 1 == NS ? 0 : sl + 1) mbar_arrive(empty_w + sl);
+          mbar_arrive(empty_q + qr.slot);
         }
-        mbar_arrive(empty_p + pr.slot);
+        if (usep) mbar_arrive(empty_p + pr.slot);
       }
-      pr.next<NP>();
+      if (usep) pr.next<NP>();
       sb += s + 1 < nst ? 1 : 5;
       if (sb >= NS) sb -= NS;
     }
+    qr.next<NQ>();
   }
 }
 
@@ -406,9 +483,25 @@ static bool set_smem() {
                               (int)SMEM_BYTES) == cudaSuccess;
 }
 
-bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* M, int* err, int device) {
+// 3-D map over the 12 metric / media planes (py, nz, 12) with box (32, 8, 12)
+static bool make_plane_map(CUtensorMap* m, const Dims& d, const float* base) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)d.py, (cuuint64_t)d.nz, 12};
+  cuuint64_t strides[2] = {(cuuint64_t)d.py * 4, (cuuint64_t)d.py * d.nz * 4};
+  cuuint32_t box[3] = {(cuuint32_t)TJ, (cuuint32_t)TK, 12};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, int* err, int* sched,
+                int device) {
   tc->ok = false;
   tc->err = err;
+  tc->sched = sched;
   if (cudaDeviceGetAttribute(&tc->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return false;
   // the tile's halo box must start on a 16-byte boundary: (first interior row node) % 4 == 0
   bool ok = true;
@@ -416,8 +509,7 @@ bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* M, i
     ok = make_map(&tc->halo[b], d, W[b], 9, HW, HH, 9);
     ok = ok && make_map(&tc->centre[b], d, W[b], 9, TJ, TK, 9);
   }
-  ok = ok && make_map(&tc->m9, d, M, 13, TJ, TK, 9);
-  ok = ok && make_map(&tc->m3, d, M, 13, TJ, TK, 3);
+  ok = ok && make_plane_map(&tc->plane, d, planes);
   ok = ok && set_smem<-1, -1, -1>() && set_smem<-1, -1, 1>() && set_smem<-1, 1, -1>() && set_smem<-1, 1, 1>();
   ok = ok && set_smem<1, -1, -1>() && set_smem<1, -1, 1>() && set_smem<1, 1, -1>() && set_smem<1, 1, 1>();
   tc->ok = ok;
@@ -452,11 +544,10 @@ static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3
   mp.win = tc.halo[bin];
   mp.w0 = tc.centre[0];
   mp.t = tc.centre[3];
-  mp.m9 = tc.m9;
-  mp.m3 = tc.m3;
+  mp.plane = tc.plane;
   int grid = 0;
   TileSched sc = plan(a.d, lo, hi, tc.nsm, &grid);
-  volume_tile_kernel<FX, FY, FZ><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err);
+  volume_tile_kernel<FX, FY, FZ><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err, tc.sched);
 }
 
 // true when the tiled kernel took the interior box

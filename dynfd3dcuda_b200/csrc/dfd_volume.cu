@@ -185,8 +185,9 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 
 
 // Shell kernel: the general update on up to six boxes (PML slabs, free-surface rows) that
-// surround the interior box; one 1-D grid of 256-thread blocks is split over the boxes.
-// A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z, 2 x) per block; a
+// surround the interior box; one 1-D grid of 128-thread blocks is split over the boxes
+// (small blocks fit beside a CTA of the tiled interior kernel, so the two kernels share
+// the SMs).  A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z) per block; a
 // thinner box (the y slabs of the PML, the free-surface rows) is flattened over (y, z)
 // with y fastest, so that no thread idles and the y-face PML state (y fastest over N
 // nodes, then z) is read contiguously.
@@ -197,16 +198,18 @@ struct Boxes {
   int start[7];            // first block of each box
 };
 
+constexpr int SHELL_THREADS = 128;
+
 template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(256, 2) volume_shell_kernel(VolArgs a, Boxes bx) {
+__global__ void __launch_bounds__(SHELL_THREADS, 4) volume_shell_kernel(VolArgs a, Boxes bx) {
   int b = 0;
   while (b + 1 < bx.n && (int)blockIdx.x >= bx.start[b + 1]) b++;
   int loc = blockIdx.x - bx.start[b];
   int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
   int i, j, k;
   if (bx.thin[b]) {
-    int gyz = (nj * nk + 255) / 256;
-    int t = (loc % gyz) * 256 + threadIdx.x;
+    int gyz = (nj * nk + SHELL_THREADS - 1) / SHELL_THREADS;
+    int t = (loc % gyz) * SHELL_THREADS + threadIdx.x;
     i = loc / gyz;
     j = t % nj;
     k = t / nj;
@@ -215,8 +218,8 @@ __global__ void __launch_bounds__(256, 2) volume_shell_kernel(VolArgs a, Boxes b
     int gj = (nj + 31) / 32, gk = (nk + 3) / 4;
     int bj = loc % gj, bk = (loc / gj) % gk, bi = loc / (gj * gk);
     j = bj * 32 + (threadIdx.x & 31);
-    k = bk * 4 + ((threadIdx.x >> 5) & 3);
-    i = bi * 2 + (threadIdx.x >> 7);
+    k = bk * 4 + (threadIdx.x >> 5);
+    i = bi;
     if (i >= ni || j >= nj || k >= nk) return;
   }
   volume_point_general<FX, FY, FZ>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
@@ -300,7 +303,7 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
   const int ktop = a.freenode ? d.nk - 3 : d.nk;
   long long nodes = 0;  // nodes of the box the interior (or tiled) kernel covers
   if (kb) cudaEventRecord(*kb, s);
-  if (tc && tc->ok && tc->pml &&
+  if (tc && tc->ok && tc->pml == 1 &&
       launch_tile(tc, a, FX, FY, FZ, bin, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop), s)) {
     // TMA-tiled kernel over every node below the free-surface rows; the general kernel
     // takes the free-surface rows
@@ -313,9 +316,16 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     // PML path).
     int3 tlo = lo;
     tlo.y -= (lo.y + 3 + d.oy) % 4;
+    int3 thi = hi;
+    if (tc && tc->pml == 3) {
+      // the tiles also cover the two x slabs of the PML
+      tlo.x = 0;
+      thi.x = d.ni;
+    }
     const bool some = hi.x > lo.x && hi.y > lo.y && hi.z > lo.z;
-    if (some && tlo.y >= 0 && launch_tile(tc, a, FX, FY, FZ, bin, tlo, hi, s)) {
+    if (some && tlo.y >= 0 && launch_tile(tc, a, FX, FY, FZ, bin, tlo, thi, s)) {
       lo = tlo;
+      hi = thi;
     } else if (some) {
       const int chunk = 8;
       dim3 block(32, 8, 1);
@@ -335,11 +345,11 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     bx.start[b] = tot;
     int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
     bx.thin[b] = nj < 32 || nk < 4;
-    tot += bx.thin[b] ? ((nj * nk + 255) / 256) * ni : ((nj + 31) / 32) * ((nk + 3) / 4) * ((ni + 1) / 2);
+    tot += bx.thin[b] ? ((nj * nk + SHELL_THREADS - 1) / SHELL_THREADS) * ni : ((nj + 31) / 32) * ((nk + 3) / 4) * ni;
   }
   bx.start[bx.n] = tot;
   if (ke) cudaEventRecord(*ke, s);
-  if (tot > 0) volume_shell_kernel<FX, FY, FZ><<<tot, 256, 0, s_shell>>>(a, bx);
+  if (tot > 0) volume_shell_kernel<FX, FY, FZ><<<tot, SHELL_THREADS, 0, s_shell>>>(a, bx);
   return nodes;
 }
 

@@ -114,7 +114,7 @@ def test_run_many_steps_equals_single_steps():
     assert np.array_equal(a.fault("State"), b.fault("State"))
 
 
-@pytest.mark.parametrize("mode", ["1", "2"])
+@pytest.mark.parametrize("mode", ["1", "2", "3"])
 @pytest.mark.parametrize("name", ["vol_curved", "sw_curved"])
 def test_tiled_interior_matches_plain_kernel(monkeypatch, name, mode):
     """The TMA-tiled kernel over the interior box (DFD_TILE=1, default) or over the PML
