@@ -179,7 +179,8 @@ struct TileCtx {
 };
 bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, int* err, int* sched,
                 int device);
-bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi,
+// pmlp: the box contains PML nodes (the kernel variant with the PML path)
+bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi, bool pmlp,
                  cudaStream_t s);
 
 __host__ __device__ inline long long idx3(const Dims& d, int i, int j, int k) {

@@ -108,8 +108,8 @@ struct TileSched {
   int ntj, ntk, ci, nunits;               // tiles in y and z, planes per chunk, units
 };
 
-constexpr int NCW = NTHR / 32;   // computing warps, one node per thread
-constexpr int NTOT = NTHR + 32;  // plus one copy-issuing warp
+constexpr int NCW = 2 * NTHR / 32;  // computing warps: two per 32-node row of the tile
+constexpr int NTOT = NCW * 32 + 32;  // plus one copy-issuing warp
 
 // slot / phase-parity cursor over a ring of N mbarrier-guarded slots
 struct Ring {
@@ -122,6 +122,30 @@ struct Ring {
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+// RK4 register update of fields F0..F1-1 of node q with right-hand side hv, then the
+// sponge factor (rk4.cu:20-33, cerjan.cu:166-200): step-start values from the stencil
+// input at stage 0, the RK registers from the pointwise slot P at stages 1..3.
+template <int F0, int F1>
+__device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, long long q, const float* cur,
+                                              const float* P, const float* hv, float damp) {
+#pragma unroll
+  for (int f = F0; f < F1; f++) {
+    const long long x = f * n + q;
+    float w;
+    if (a.irk == 0) {
+      const float w0 = cur[f * HBOX];
+      a.T[x] = fmaf(a.rkb, hv[f], w0);
+      w = fmaf(a.rka, hv[f], w0);
+    } else if (a.irk < 3) {
+      a.T[x] = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
+      w = fmaf(a.rka, hv[f], P[f * PB]);
+    } else {
+      w = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
+    }
+    a.Wout[x] = w * damp;
+  }
 }
 
 // Metric and media of a node of the tiled box: x row (xi), y row (eta), z row (zeta) and
@@ -198,9 +222,10 @@ __device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* co
 // barrier (one arrival per computing warp once it has finished reading the slot).  Three
 // rings: stencil planes (NS), RK registers of the step (NP; none at stage 0, whose
 // step-start values are the stencil input), metric/media planes of the unit (NQ).  At
-// most 160 registers, so that a block of the fault band kernel fits beside the CTA.
-template <int FX, int FY, int FZ>
-__global__ void __maxnreg__(160)
+// most 96 registers: the 17 warps are spread over the SM's four 16 K-register partitions,
+// five warps on one of them.
+template <int FX, int FY, int FZ, bool PMLP>
+__global__ void __maxnreg__(96)
     volume_tile_kernel(const __grid_constant__ TileMaps mp, const VolArgs a, const TileSched sc, int* err,
                        int* sched) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -296,11 +321,15 @@ __global__ void __maxnreg__(160)
     return;
   }
 
-  // ---------------- computing warps: thread (lane, warp) owns node (y = lane, z = warp)
+  // ---------------- computing warps: warps w and w + NCW/2 share the row of nodes
+  // (y = lane, z = w): the first computes the momentum equation (velocity fields), the
+  // second the constitutive law (stress fields)
+  const int role = warp >= NCW / 2 ? 1 : 0;
+  const int ty = warp - role * (NCW / 2);
   const long long n = d.nxyz;
   const float r = a.rDH;
-  const int hc = (warp + RZ) * HW + lane + 4;  // node inside a halo field box
-  const int pc = warp * TJ + lane;             // node inside a pointwise field box
+  const int hc = (ty + RZ) * HW + lane + 4;  // node inside a halo field box
+  const int pc = ty * TJ + lane;             // node inside a pointwise field box
   Ring wr, pr, qr;  // next stencil plane to wait for; RK-register slot of the step; unit planes
   int sb = 0;       // slot of the step's first stencil plane
   for (;;) {
@@ -312,7 +341,7 @@ __global__ void __maxnreg__(160)
     if (u < 0) break;
     const int tc = u / ntile, ru = u % ntile;
     const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
-    const int j = sc.lo_y + (ru % sc.ntj) * TJ + lane, k = sc.lo_z + (ru / sc.ntj) * TK + warp;
+    const int j = sc.lo_y + (ru % sc.ntj) * TJ + lane, k = sc.lo_z + (ru / sc.ntj) * TK + ty;
     const bool active = j < sc.hi_y && k < sc.hi_z;
     const bool band = active && a.united && !a.united[j + k * d.nj];
     const bool pml_yz = (a.aux[2] && j < d.N) || (a.aux[3] && j >= d.nj - d.N) || (a.aux[4] && k < d.N) ||
@@ -354,37 +383,67 @@ __global__ void __maxnreg__(160)
         g.ey1 = ety; g.ey2 = etz; g.ez1 = zty; g.ez2 = ztz;
         const int side = i + 3 < a.nxhalf ? 6 : 9;
         g.lam = Q[side * PB]; g.mu = Q[(side + 1) * PB]; g.rrho = 1.0f / Q[(side + 2) * PB];
-        const bool pml = pml_yz || (a.aux[0] && i < d.N) || (a.aux[1] && i >= d.ni - d.N);
+        const bool pml = PMLP && (pml_yz || (a.aux[0] && i < d.N) || (a.aux[1] && i >= d.ni - d.N));
+        const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
+        const long long q = qyz + (long long)(i + 3) * d.sx;
         float hv[9];
         if (pml) {
-          const float* xv[5] = {xs0, xs1, xs2, xs3, xs4};
-          tile_pml_point<FX, FY, FZ>(a, xv, cur, g, i, j, k, hv);
+          // a node in a PML slab is taken whole by the velocity warp of the pair
+          if (PMLP && role == 0) {
+            const float* xv[5] = {xs0, xs1, xs2, xs3, xs4};
+            tile_pml_point<FX, FY, FZ>(a, xv, cur, g, i, j, k, hv);
+            rk_tile_store<0, 9>(a, n, q, cur, P, hv, damp);
+          }
         } else {
           const float lam = g.lam, mu = g.mu, rrho = g.rrho;
           const float l2m = lam + 2.0f * mu;
-          float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f, h8 = 0.f;
+#define DFD_DERX(f) d5v<FX>(xs0[(f) * HBOX], xs1[(f) * HBOX], xs2[(f) * HBOX], xs3[(f) * HBOX], xs4[(f) * HBOX])
+#define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HBOX)
+#define DFD_DERZ(f) d5s<FZ, HW>(cur + (f) * HBOX)
           // the x row has three components; the y and z rows have no x component, so the
           // terms with it (exact zeros) and the derivative of Txx along y and z drop out
-          {
-            const float e0 = g.ex0, e1 = g.ex1, e2 = g.ex2;
-            float dv;
-#define DFD_DERX(f) d5v<FX>(xs0[(f) * HBOX], xs1[(f) * HBOX], xs2[(f) * HBOX], xs3[(f) * HBOX], xs4[(f) * HBOX])
-            dv = DFD_DERX(0) * r;
-            h3 += dv * e0 * l2m; h4 += dv * e0 * lam; h5 += dv * e0 * lam; h6 += dv * e1 * mu; h7 += dv * e2 * mu;
-            dv = DFD_DERX(1) * r;
-            h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h6 += dv * e0 * mu; h8 += dv * e2 * mu;
-            dv = DFD_DERX(2) * r;
-            h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h7 += dv * e0 * mu; h8 += dv * e1 * mu;
-            const float er0 = e0 * rrho, er1 = e1 * rrho, er2 = e2 * rrho;
-            dv = DFD_DERX(3) * r; h0 += dv * er0;
-            dv = DFD_DERX(4) * r; h1 += dv * er1;
-            dv = DFD_DERX(5) * r; h2 += dv * er2;
-            dv = DFD_DERX(6) * r; h0 += dv * er1; h1 += dv * er0;
-            dv = DFD_DERX(7) * r; h0 += dv * er2; h2 += dv * er0;
-            dv = DFD_DERX(8) * r; h1 += dv * er2; h2 += dv * er1;
-#undef DFD_DERX
-          }
-#define DFD_TAXIS0(DER, E1, E2)                                                                     \
+          if (role == 0) {
+            // momentum: velocity rates from the six stress derivatives per axis
+            float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+            {
+              const float er0 = g.ex0 * rrho, er1 = g.ex1 * rrho, er2 = g.ex2 * rrho;
+              float dv;
+              dv = DFD_DERX(3) * r; h0 += dv * er0;
+              dv = DFD_DERX(4) * r; h1 += dv * er1;
+              dv = DFD_DERX(5) * r; h2 += dv * er2;
+              dv = DFD_DERX(6) * r; h0 += dv * er1; h1 += dv * er0;
+              dv = DFD_DERX(7) * r; h0 += dv * er2; h2 += dv * er0;
+              dv = DFD_DERX(8) * r; h1 += dv * er2; h2 += dv * er1;
+            }
+#define DFD_VAXIS0(DER, E1, E2)                                                                     \
+  {                                                                                                 \
+    const float er1 = (E1) * rrho, er2 = (E2) * rrho;                                               \
+    float dv;                                                                                       \
+    dv = DER(4) * r; h1 += dv * er1;                                                                \
+    dv = DER(5) * r; h2 += dv * er2;                                                                \
+    dv = DER(6) * r; h0 += dv * er1;                                                                \
+    dv = DER(7) * r; h0 += dv * er2;                                                                \
+    dv = DER(8) * r; h1 += dv * er2; h2 += dv * er1;                                                \
+  }
+            DFD_VAXIS0(DFD_DERY, g.ey1, g.ey2)
+            DFD_VAXIS0(DFD_DERZ, g.ez1, g.ez2)
+#undef DFD_VAXIS0
+            hv[0] = h0; hv[1] = h1; hv[2] = h2;
+            rk_tile_store<0, 3>(a, n, q, cur, P, hv, damp);
+          } else {
+            // constitutive law: stress rates from the three velocity derivatives per axis
+            float h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f, h8 = 0.f;
+            {
+              const float e0 = g.ex0, e1 = g.ex1, e2 = g.ex2;
+              float dv;
+              dv = DFD_DERX(0) * r;
+              h3 += dv * e0 * l2m; h4 += dv * e0 * lam; h5 += dv * e0 * lam; h6 += dv * e1 * mu; h7 += dv * e2 * mu;
+              dv = DFD_DERX(1) * r;
+              h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h6 += dv * e0 * mu; h8 += dv * e2 * mu;
+              dv = DFD_DERX(2) * r;
+              h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h7 += dv * e0 * mu; h8 += dv * e1 * mu;
+            }
+#define DFD_SAXIS0(DER, E1, E2)                                                                     \
   {                                                                                                 \
     const float e1 = (E1), e2 = (E2);                                                               \
     float dv;                                                                                       \
@@ -393,41 +452,16 @@ __global__ void __maxnreg__(160)
     h3 += dv * e1 * lam; h4 += dv * e1 * l2m; h5 += dv * e1 * lam; h8 += dv * e2 * mu;              \
     dv = DER(2) * r;                                                                                \
     h3 += dv * e2 * lam; h4 += dv * e2 * lam; h5 += dv * e2 * l2m; h8 += dv * e1 * mu;              \
-    const float er1 = e1 * rrho, er2 = e2 * rrho;                                                   \
-    dv = DER(4) * r; h1 += dv * er1;                                                                \
-    dv = DER(5) * r; h2 += dv * er2;                                                                \
-    dv = DER(6) * r; h0 += dv * er1;                                                                \
-    dv = DER(7) * r; h0 += dv * er2;                                                                \
-    dv = DER(8) * r; h1 += dv * er2; h2 += dv * er1;                                                \
   }
-#define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HBOX)
-#define DFD_DERZ(f) d5s<FZ, HW>(cur + (f) * HBOX)
-          DFD_TAXIS0(DFD_DERY, g.ey1, g.ey2)
-          DFD_TAXIS0(DFD_DERZ, g.ez1, g.ez2)
+            DFD_SAXIS0(DFD_DERY, g.ey1, g.ey2)
+            DFD_SAXIS0(DFD_DERZ, g.ez1, g.ez2)
+#undef DFD_SAXIS0
+            hv[3] = h3; hv[4] = h4; hv[5] = h5; hv[6] = h6; hv[7] = h7; hv[8] = h8;
+            rk_tile_store<3, 9>(a, n, q, cur, P, hv, damp);
+          }
+#undef DFD_DERX
 #undef DFD_DERY
 #undef DFD_DERZ
-#undef DFD_TAXIS0
-          hv[0] = h0; hv[1] = h1; hv[2] = h2; hv[3] = h3; hv[4] = h4;
-          hv[5] = h5; hv[6] = h6; hv[7] = h7; hv[8] = h8;
-        }
-        // RK4 registers and Cerjan sponge (rk4.cu:20-33, cerjan.cu:166-200)
-        const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
-        const long long q = qyz + (long long)(i + 3) * d.sx;
-#pragma unroll
-        for (int f = 0; f < 9; f++) {
-          const long long x = f * n + q;
-          float w;
-          if (irk == 0) {
-            const float w0 = cur[f * HBOX];
-            a.T[x] = fmaf(a.rkb, hv[f], w0);
-            w = fmaf(a.rka, hv[f], w0);
-          } else if (irk < 3) {
-            a.T[x] = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
-            w = fmaf(a.rka, hv[f], P[f * PB]);
-          } else {
-            w = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
-          }
-          a.Wout[x] = w * damp;
         }
       }
       // release the slots this warp has finished with
@@ -479,7 +513,9 @@ static bool make_map(CUtensorMap* m, const Dims& d, const float* base, int nf, i
 
 template <int FX, int FY, int FZ>
 static bool set_smem() {
-  return cudaFuncSetAttribute(volume_tile_kernel<FX, FY, FZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(volume_tile_kernel<FX, FY, FZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)SMEM_BYTES) == cudaSuccess &&
+         cudaFuncSetAttribute(volume_tile_kernel<FX, FY, FZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)SMEM_BYTES) == cudaSuccess;
 }
 
@@ -539,7 +575,7 @@ static TileSched plan(const Dims& d, int3 lo, int3 hi, int nsm, int* grid) {
 }
 
 template <int FX, int FY, int FZ>
-static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
+static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, bool pmlp, cudaStream_t s) {
   TileMaps mp;
   mp.win = tc.halo[bin];
   mp.w0 = tc.centre[0];
@@ -547,24 +583,27 @@ static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3
   mp.plane = tc.plane;
   int grid = 0;
   TileSched sc = plan(a.d, lo, hi, tc.nsm, &grid);
-  volume_tile_kernel<FX, FY, FZ><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err, tc.sched);
+  if (pmlp)
+    volume_tile_kernel<FX, FY, FZ, true><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err, tc.sched);
+  else
+    volume_tile_kernel<FX, FY, FZ, false><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err, tc.sched);
 }
 
 // true when the tiled kernel took the interior box
-bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi,
+bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi, bool pmlp,
                  cudaStream_t s) {
   if (!tc || !tc->ok) return false;
   if ((lo.y + 3 + a.d.oy) % 4 != 0 || lo.z < 0 || hi.x <= lo.x || hi.y <= lo.y || hi.z <= lo.z) return false;
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: launch_t<-1, -1, -1>(*tc, a, bin, lo, hi, s); break;
-    case 1: launch_t<-1, -1, 1>(*tc, a, bin, lo, hi, s); break;
-    case 2: launch_t<-1, 1, -1>(*tc, a, bin, lo, hi, s); break;
-    case 3: launch_t<-1, 1, 1>(*tc, a, bin, lo, hi, s); break;
-    case 4: launch_t<1, -1, -1>(*tc, a, bin, lo, hi, s); break;
-    case 5: launch_t<1, -1, 1>(*tc, a, bin, lo, hi, s); break;
-    case 6: launch_t<1, 1, -1>(*tc, a, bin, lo, hi, s); break;
-    default: launch_t<1, 1, 1>(*tc, a, bin, lo, hi, s); break;
+    case 0: launch_t<-1, -1, -1>(*tc, a, bin, lo, hi, pmlp, s); break;
+    case 1: launch_t<-1, -1, 1>(*tc, a, bin, lo, hi, pmlp, s); break;
+    case 2: launch_t<-1, 1, -1>(*tc, a, bin, lo, hi, pmlp, s); break;
+    case 3: launch_t<-1, 1, 1>(*tc, a, bin, lo, hi, pmlp, s); break;
+    case 4: launch_t<1, -1, -1>(*tc, a, bin, lo, hi, pmlp, s); break;
+    case 5: launch_t<1, -1, 1>(*tc, a, bin, lo, hi, pmlp, s); break;
+    case 6: launch_t<1, 1, -1>(*tc, a, bin, lo, hi, pmlp, s); break;
+    default: launch_t<1, 1, 1>(*tc, a, bin, lo, hi, pmlp, s); break;
   }
   return true;
 }

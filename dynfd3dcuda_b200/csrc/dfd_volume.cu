@@ -184,7 +184,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 }
 
 
-// Shell kernel: the general update on up to six boxes (PML slabs, free-surface rows) that
+// Shell kernel: the general update on up to eight boxes (PML slabs, free-surface rows) that
 // surround the interior box; one 1-D grid of 128-thread blocks is split over the boxes
 // (small blocks fit beside a CTA of the tiled interior kernel, so the two kernels share
 // the SMs).  A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z) per block; a
@@ -193,9 +193,9 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 // nodes, then z) is read contiguously.
 struct Boxes {
   int n;
-  int lo[6][3], hi[6][3];  // (i, j, k) interior-index bounds, half open
-  int thin[6];             // flattened (y, z) mapping
-  int start[7];            // first block of each box
+  int lo[8][3], hi[8][3];  // (i, j, k) interior-index bounds, half open
+  int thin[8];             // flattened (y, z) mapping
+  int start[9];            // first block of each box
 };
 
 constexpr int SHELL_THREADS = 128;
@@ -304,7 +304,7 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
   long long nodes = 0;  // nodes of the box the interior (or tiled) kernel covers
   if (kb) cudaEventRecord(*kb, s);
   if (tc && tc->ok && tc->pml == 1 &&
-      launch_tile(tc, a, FX, FY, FZ, bin, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop), s)) {
+      launch_tile(tc, a, FX, FY, FZ, bin, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop), true, s)) {
     // TMA-tiled kernel over every node below the free-surface rows; the general kernel
     // takes the free-surface rows
     nodes = (long long)d.ni * d.nj * ktop;
@@ -312,27 +312,30 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
   } else {
     // interior box by the TMA-tiled kernel (or the plain interior kernel), the shell
     // around it by the general kernel.  The tiles start on a 16-byte boundary in y: the
-    // box is widened down to it (the few PML columns this adds take the tile kernel's
-    // PML path).
-    int3 tlo = lo;
-    tlo.y -= (lo.y + 3 + d.oy) % 4;
-    int3 thi = hi;
-    if (tc && tc->pml == 3) {
+    // tiled box starts at the next boundary, and the general kernel takes the (at most
+    // three) interior columns before it.
+    int3 tlo = lo, thi = hi;
+    const int ygap = (4 - (lo.y + 3 + d.oy) % 4) % 4;
+    tlo.y += ygap;
+    const bool xslabs = tc && tc->pml == 3;
+    if (xslabs) {
       // the tiles also cover the two x slabs of the PML
       tlo.x = 0;
       thi.x = d.ni;
     }
     const bool some = hi.x > lo.x && hi.y > lo.y && hi.z > lo.z;
-    if (some && tlo.y >= 0 && launch_tile(tc, a, FX, FY, FZ, bin, tlo, thi, s)) {
-      lo = tlo;
-      hi = thi;
+    if (some && thi.y > tlo.y && launch_tile(tc, a, FX, FY, FZ, bin, tlo, thi, xslabs, s)) {
+      add(tlo.x, thi.x, lo.y, tlo.y, lo.z, hi.z);
+      lo.x = tlo.x;
+      hi.x = thi.x;
+      nodes = (long long)(thi.x - tlo.x) * (thi.y - tlo.y) * (thi.z - tlo.z);
     } else if (some) {
       const int chunk = 8;
       dim3 block(32, 8, 1);
       dim3 grid((hi.y - lo.y + 31) / 32, (hi.z - lo.z + 7) / 8, (hi.x - lo.x + chunk - 1) / chunk);
       volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, lo, hi, chunk);
+      nodes = (long long)(hi.x - lo.x) * (hi.y - lo.y) * (hi.z - lo.z);
     }
-    if (some) nodes = (long long)(hi.x - lo.x) * (hi.y - lo.y) * (hi.z - lo.z);
     add(0, lo.x, 0, d.nj, 0, d.nk);
     add(hi.x, d.ni, 0, d.nj, 0, d.nk);
     add(lo.x, hi.x, 0, lo.y, 0, d.nk);
