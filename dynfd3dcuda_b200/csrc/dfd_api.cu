@@ -103,7 +103,7 @@ struct dfd_ctx {
   cudaGraphExec_t graph[8] = {};
   // output
   NcWriter ncf, ncw[3];
-  int vf[16] = {}, vw[3][3] = {};
+  int vf[24] = {}, vw[3][3] = {};
   bool out_open = false;
 };
 

@@ -51,8 +51,8 @@ extern void init_fault_coef(realptr_t M, Fault);
 extern void init_wave_free(realptr_t M, PML, Wave);
 extern void nc_read_init_stress(Fault F);
 #ifdef useCerjan
-extern void init_cerjan_host(realptr_t damp);
-extern void apply_cerjan(Wave, realptr_t);
+extern void init_cerjan_host(float *damp);
+extern void apply_cerjan(Wave, float *);
 #endif
 
 static const int kFlags[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1},
@@ -164,7 +164,9 @@ int main(int argc, char **argv) {
 
   char *gp[2] = {argv[0], argv[1]};
   get_params(2, gp);
-  // single-rank topology (main.cu:155-193)
+  // single-rank topology (main.cu:151-193): every neighbour is MPI_PROC_NULL, which the
+  // boundary treatments test (the Cerjan sponge damps only faces without a neighbour)
+  for (int d = 0; d < 2; d++) neigxid[d] = neigyid[d] = neigzid[d] = MPI_PROC_NULL;
   masternode = 1;
 #ifdef FreeSurface
   freenode = 1;
@@ -205,11 +207,12 @@ int main(int argc, char **argv) {
   cpy_host2device_pml(P, hP);
 #endif
 #ifdef useCerjan
-  real_t *damp_h = (real_t *)calloc(nxyz, sizeof(real_t));
-  real_t *damp;
-  cudaMalloc((void **)&damp, sizeof(real_t) * nxyz);
+  // the sponge table is float in every build (cerjan.cu:14-31, main.cu)
+  float *damp_h = (float *)calloc(nxyz, sizeof(float));
+  float *damp;
+  cudaMalloc((void **)&damp, sizeof(float) * nxyz);
   init_cerjan_host(damp_h);
-  cudaMemcpy(damp, damp_h, sizeof(real_t) * nxyz, cudaMemcpyHostToDevice);
+  cudaMemcpy(damp, damp_h, sizeof(float) * nxyz, cudaMemcpyHostToDevice);
 #endif
   real_t *hC = (real_t *)calloc(nxyz * CSIZE, sizeof(real_t));
   real_t *hM = (real_t *)calloc(nxyz * MSIZE, sizeof(real_t));

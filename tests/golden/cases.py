@@ -213,6 +213,16 @@ def get_case(name):
         fx = flat_geometry(NY, NZ, DH)
         st = sw_stress(fx, fg, patch=(0.0, -500.0, 450.0), patch_ts=-95e6, Dc=0.05, mu_d=0.525)
         return p, fx, st, None, None, dict(steps=60, every=20, volume=False)
+    if name == "sw_cerjan":
+        # slip weakening with the Cerjan sponge on top of the PML (reference -DuseCerjan)
+        NX, NY, NZ, DH = 24, 76, 40, 100.0
+        fg = [21, 56, 21, 40]
+        p = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.008, TMAX=0.4, PML_N=6, PML_velocity=6000.0,
+                 INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=0, Fault_grid=fg,
+                 mu_s=0.677, mu_d=0.525, Dc=0.4, C0=0.0, useCerjan=1, DAMP_N=8)
+        fx = flat_geometry(NY, NZ, DH)
+        st = sw_stress(fx, fg, patch=(0.0, -500.0, 450.0), patch_ts=-95e6, Dc=0.05, mu_d=0.525)
+        return p, fx, st, None, None, dict(steps=60, every=20, volume=False)
     if name == "sw_curved":
         NX, NY, NZ, DH = 24, 76, 40, 100.0
         fg = [21, 56, 21, 40]
@@ -258,7 +268,7 @@ def rs_rough_case(NY, NX, NZ, seed=0, DH=100.0, steps=40, L=0.4):
     return p, fx, st, None, None, dict(steps=steps, every=steps // 2, volume=False)
 
 
-CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat"]
+CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan"]
 
 
 def write_inputs(name, outdir):

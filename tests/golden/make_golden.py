@@ -57,7 +57,8 @@ def run_case(name, variant, outdir):
     with tempfile.TemporaryDirectory() as td:
         job, meta = cases.write_inputs(name, td)
         nr = "" if int(p.get("NormalRefine", 1)) else "_nr"
-        exe = os.path.join(ROOT, "oracle", "_ref", f"refharness_{variant}{nr}")
+        cj = "_cj" if int(p.get("useCerjan", 0)) else ""
+        exe = os.path.join(ROOT, "oracle", "_ref", f"refharness_{variant}{nr}{cj}")
         cmd = [exe, os.path.join(td, "params.json"), td, str(meta["steps"]), str(meta["every"])]
         if meta["volume"]:
             cmd.append("--volume")

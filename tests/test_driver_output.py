@@ -1,0 +1,66 @@
+"""The drop-in driver executable and the NetCDF outputs, on the GPU.
+
+The driver (dynfd3dcuda_b200/dfd_b200) reads the same params.json and NetCDF inputs as
+the reference's executable and writes fault_mpi000000.nc and wave_{yz,xz,xy}_mpi000000.nc
+with the reference's variable names, one record per EXPORT_TIME_SKIP steps, written before
+the step (main.cu:425-437, io_fault.cu, io_wave_*.cu).  The records must equal the state
+that the Python mirror of the C ABI reads before the same steps.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "dynfd3dcuda_b200", "dfd_b200")
+
+
+def test_driver_writes_reference_outputs(tmp_path):
+    from scipy.io import netcdf_file
+
+    import dynfd3dcuda_b200 as dfd
+
+    job, meta = cases.write_inputs("sw_flat", str(tmp_path))
+    job.update(EXPORT_TIME_SKIP=5, EXPORT_WAVE_SLICE_X=job["NX"] // 2, EXPORT_WAVE_SLICE_Y=30,
+               EXPORT_WAVE_SLICE_Z=job["NZ"] - 1, TMAX=0.2 + 0.004)
+    with open(tmp_path / "params.json", "w") as f:
+        json.dump(job, f)
+    r = subprocess.run([EXE, str(tmp_path / "params.json")], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    NT = int(np.float32(job["TMAX"]) / np.float32(job["DT"]))
+    assert NT == 25
+
+    p, fx, st, _, _, _ = cases.get_case("sw_flat")
+    sim = dfd.Simulation(dict(job), fx, st, None)
+    recs = {k: [] for k in ("Vs1", "Vs2", "Tn", "Ts1", "Ts2", "slip", "State")}
+    slices = []
+    for it in range(NT):
+        if it % 5 == 0:
+            for k in recs:
+                recs[k].append(sim.fault(k))
+            slices.append([sim.slice(0, job["NX"] // 2), sim.slice(1, 30), sim.slice(2, job["NZ"] - 1)])
+        sim.step(it)
+    t0 = sim.fault("init_t0")
+    sim.close()
+
+    with netcdf_file(tmp_path / "fault_mpi000000.nc", "r", mmap=False) as f:
+        v = f.variables
+        assert v["Vs1"].shape == (NT // 5, job["NZ"], job["NY"])
+        for nc, k in (("Vs1", "Vs1"), ("Vs2", "Vs2"), ("tn", "Tn"), ("ts1", "Ts1"), ("ts2", "Ts2"), ("Us0", "slip"),
+                      ("State", "State")):
+            np.testing.assert_array_equal(np.asarray(v[nc][:]), np.stack(recs[k]), err_msg=nc)
+        assert np.asarray(v["y"][:]).shape == (job["NZ"], job["NY"])
+        # rupture times as of the last record (written before step 20)
+        assert np.asarray(v["init_t0"][:]).shape == t0.shape
+    for a, name in enumerate(("wave_yz", "wave_xz", "wave_xy")):
+        with netcdf_file(tmp_path / f"{name}_mpi000000.nc", "r", mmap=False) as f:
+            for c, comp in enumerate(("Vx", "Vy", "Vz")):
+                got = np.asarray(f.variables[comp][:])
+                want = np.stack([s[a][c] for s in slices])
+                np.testing.assert_array_equal(got, want, err_msg=f"{name}/{comp}")

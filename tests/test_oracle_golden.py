@@ -24,6 +24,7 @@ TOL = {
     ("sw_flat_nr", "dp"): 1e-6, ("sw_flat_nr", "sp"): 1e-5,
     ("sw_curved", "dp"): 3e-5, ("sw_curved", "sp"): 1e-4,
     ("rs_flat", "dp"): 3e-5, ("rs_flat", "sp"): 3e-4,
+    ("sw_cerjan", "dp"): 1e-6, ("sw_cerjan", "sp"): 1e-5,
 }
 
 
