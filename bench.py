@@ -308,13 +308,57 @@ def learned_rs(dfd, steps=600, every=7, epochs=4, device=0):
     return out
 
 
+def run_ensemble(args, dfd, local):
+    """Batched ensemble (64 scenarios, grids of 100-300 nodes per axis, slip weakening and
+    rate and state mixed): aggregate Gpt-steps/s of the whole batch, after the autotuner has
+    picked the unit length of the tiled kernel."""
+    import cases
+    import torch
+
+    n = 64
+    specs = [cases.ensemble_case(i) for i in range(n)]
+    nodes = sum(p["NX"] * p["NY"] * p["NZ"] for p, _, _ in specs)
+    need = sum((p["NX"] + 6) * (p["NY"] + 8) * (p["NZ"] + 6) * 4 * (36 + 13 + 8) for p, _, _ in specs)
+    free, _ = torch.cuda.mem_get_info(local)
+    if need > 0.92 * free:
+        raise SystemExit(f"ensemble needs about {need / 1e9:.0f} GB, {free / 1e9:.0f} GB free")
+    t0 = time.perf_counter()
+    sims = [dfd.Simulation(p, fx, st, None, device=local) for p, fx, st in specs]
+    ens = dfd.Ensemble(sims)
+    setup_s = time.perf_counter() - t0
+    times, best, it = ens.autotune(0, candidates=(0, 32, 64, 128), steps=2)
+    ens.run(it, args.warmup)
+    ens.synchronize()
+    it += args.warmup
+    clk = Clocks(local)
+    clk.start()
+    ms = ens.run_timed(it, args.steps)
+    clocks = clk.stop()
+    value = job_rate(nodes, args.steps, 1, ms / 1e3)
+    nf = sum(p["NY"] * p["NZ"] for p, _, _ in specs)
+    line = {"metric": "Gpt-steps/s", "value": value, "unit": "Gpt-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched ensemble: 64 scenarios, grids 100-300 nodes per axis, dh=100 m, "
+                                   "stress drop 2-8 MPa, Dc/L 0.2-0.8 m, slip weakening and rate and state mixed",
+                       "nodes": nodes, "fault_nodes": nf, "scenarios": n, "parallelism": "one batched launch "
+                       "per kernel and RK stage, CUDA graph per step",
+                       "l2": "inputs larger than L2; no flush"},
+            "autotune": {"unit_planes_ms": {str(k): v for k, v in times.items()}, "chosen": best},
+            "setup_s": setup_s, "gpu_launches": 17 * args.steps, "clocks": clocks}
+    ens.close()
+    for s in sims:
+        s.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="curved", choices=["curved", "flat", "profile", "large"])
+    ap.add_argument("--config", default="curved", choices=["curved", "flat", "profile", "large", "ensemble"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned Newton-guess comparison")
     args = ap.parse_args()
@@ -329,6 +373,10 @@ def main():
     import dynfd3dcuda_b200 as dfd
 
     torch.cuda.set_device(local)
+    if args.config == "ensemble":
+        if rank == 0:
+            run_ensemble(args, dfd, local)
+        return
     dist = None
     if world > 1:
         import datetime

@@ -28,6 +28,71 @@ STATUS = {0: "ok", 1: "bad or unsupported parameter", 2: "CUDA error", 3: "file 
           7: "Newton solve hit its iteration cap"}
 
 
+class Ensemble:
+    """Prepared Simulations on one device stepped together (dfd_ens_*): one batched launch
+    per kernel and RK stage over all scenarios, replayed from CUDA graphs.  The scenarios
+    keep their state; read it from the Simulation objects."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (ctypes.c_void_p * len(self.sims))(*[s.h.value if hasattr(s.h, "value") else s.h for s in self.sims])
+        h = ctypes.c_void_p()
+        r = lib().dfd_ens_create(arr, len(self.sims), ctypes.byref(h))
+        if r:
+            raise DfdError(r, "dfd_ens_create")
+        self.h = h
+
+    def _check(self, r):
+        if r:
+            lib().dfd_ens_last_error.restype = ctypes.c_char_p
+            lib().dfd_ens_last_error.argtypes = [ctypes.c_void_p]
+            raise DfdError(r, (lib().dfd_ens_last_error(self.h) or b"").decode())
+
+    def run(self, it0, nsteps):
+        self._check(lib().dfd_ens_run(self.h, it0, nsteps))
+
+    def synchronize(self):
+        self._check(lib().dfd_ens_synchronize(self.h))
+
+    def run_timed(self, it0, nsteps):
+        """Device time (ms) of nsteps steps."""
+        ms = ctypes.c_float()
+        self._check(lib().dfd_ens_run_timed(self.h, it0, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def set_chunk(self, chunk):
+        """x planes per unit of the tiled kernel (0: each scenario's own plan)."""
+        self._check(lib().dfd_ens_set_chunk(self.h, int(chunk)))
+
+    def nodes(self):
+        n = ctypes.c_longlong()
+        self._check(lib().dfd_ens_nodes(self.h, ctypes.byref(n)))
+        return n.value
+
+    def autotune(self, it0, candidates=(0, 16, 32, 64, 128), steps=4):
+        """Time a few steps with each unit length and keep the fastest; returns {chunk: ms}.
+        The steps are real steps: the scenarios advance by len(candidates) * steps."""
+        times = {}
+        it = it0
+        for c in candidates:
+            self.set_chunk(c)
+            self.run(it, 1)  # graphs of this layout
+            it += 1
+            times[c] = self.run_timed(it, steps)
+            it += steps
+        best = min(times, key=times.get)
+        self.set_chunk(best)
+        return times, best, it
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dfd_ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 # parameter vector of the learned Newton guess (DFD_MLP_PARAMS, DFD_MLP_TRAINABLE)
 MLP_PARAMS = 1259
 MLP_TRAINABLE = 1249
@@ -146,6 +211,9 @@ def lib():
             "dfd_set_guess_net": [V, V, I], "dfd_fetch_outputs": [V, V],
             "dfd_run_timed": [V, I, I, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)],
             "dfd_interior_stats": [V, P(ctypes.c_float), P(ctypes.c_longlong)],
+            "dfd_ens_create": [V, I, P(ctypes.c_void_p)], "dfd_ens_destroy": [V], "dfd_ens_run": [V, I, I],
+            "dfd_ens_synchronize": [V], "dfd_ens_run_timed": [V, I, I, P(ctypes.c_float)],
+            "dfd_ens_set_chunk": [V, I], "dfd_ens_nodes": [V, P(ctypes.c_longlong)],
             "dfd_newton_record": [V, I, I], "dfd_fault_node_ms": [V, P(ctypes.c_float)], "dfd_newton_samples": [V, V, I, P(ctypes.c_int)],
             "dfd_mlp_init": [V, ctypes.c_uint, V, V, ctypes.c_float, ctypes.c_float],
             "dfd_mlp_forward": [V, V, I, V],

@@ -459,9 +459,9 @@ static const int kFlags[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1
                                  {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
 
 // enqueue one stage on the context streams (no synchronisation)
-static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr,
-                         cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr, cudaEvent_t* nb = nullptr,
-                         cudaEvent_t* ne = nullptr) {
+// Arguments of the fault kernels for stage irk of a step with flag pattern `pattern`
+// (main.cu:448-470: FD_Flags reversed at every stage).
+static FaultArgs fault_args(dfd_ctx* ctx, int pattern, int irk) {
   const dfd_params& p = ctx->p;
   const Dims& d = ctx->d;
   int sg = (irk % 2) ? -1 : 1;
@@ -473,7 +473,7 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   float rka = a_ * DT, rkb = b_ * DT;
   size_t nf = (size_t)d.nj * d.nk;
   FaultArgs fa;
-  if (p.rupture) {
+  {
     memset(&fa, 0, sizeof fa);
     fa.d = d;
     fa.Win = ctx->W[bin[irk]]; fa.W0 = ctx->W[0]; fa.Wout = ctx->W[bout[irk]]; fa.T = ctx->W[3];
@@ -508,19 +508,22 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
     fa.irk = irk; fa.FX = FX; fa.FY = FY; fa.FZ = FZ;
     fa.freenode = p.free_surface; fa.friction_type = p.Friction_type; fa.inport_stress = p.INPORT_STRESS_TYPE;
     fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess;
-    if (nb) cudaEventRecord(*nb, ctx->s0);
-    launch_fault_node(fa, ctx->s0);
-    if (ne) cudaEventRecord(*ne, ctx->s0);
   }
-  // fork: fault band on s1, volume shell on s2, volume interior on s0
-  cudaEventRecord(ctx->ev_fork, ctx->s0);
-  if (vb) cudaEventRecord(*vb, ctx->s0);
-  if (p.rupture) {
-    cudaStreamWaitEvent(ctx->s1, ctx->ev_fork, 0);
-    launch_fault_band(fa, ctx->s1);
-    cudaEventRecord(ctx->ev_join, ctx->s1);
-  }
-  cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
+  (void)FX;
+  return fa;
+}
+
+// Arguments of the volume kernels for the same stage.
+static VolArgs vol_args(dfd_ctx* ctx, int pattern, int irk) {
+  const dfd_params& p = ctx->p;
+  const Dims& d = ctx->d;
+  (void)pattern;
+  static const int bin[4] = {0, 1, 2, 1}, bout[4] = {1, 2, 1, 0};
+  float a_ = irk == 0 ? 0.5f : irk == 1 ? 0.5f : irk == 2 ? 1.0f : 1e10f;
+  float b_ = (irk == 0 || irk == 3) ? (float)(1.0 / 6.0) : (float)(1.0 / 3.0);
+  float DT = (float)p.DT;
+  float rka = a_ * DT, rkb = b_ * DT;
+  size_t nf = (size_t)d.nj * d.nk;
   VolArgs va;
   memset(&va, 0, sizeof va);
   va.d = d;
@@ -538,6 +541,33 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   va.nxhalf = p.NX / 2;
   va.rDH = (float)(1.0 / p.DH); va.rka = rka; va.rkb = rkb;
   va.irk = irk; va.freenode = p.free_surface;
+  return va;
+}
+
+static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr,
+                         cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr, cudaEvent_t* nb = nullptr,
+                         cudaEvent_t* ne = nullptr) {
+  const dfd_params& p = ctx->p;
+  int sg = (irk % 2) ? -1 : 1;
+  int FX = kFlags[pattern][0] * sg, FY = kFlags[pattern][1] * sg, FZ = kFlags[pattern][2] * sg;
+  static const int bin[4] = {0, 1, 2, 1};
+  FaultArgs fa;
+  if (p.rupture) {
+    fa = fault_args(ctx, pattern, irk);
+    if (nb) cudaEventRecord(*nb, ctx->s0);
+    launch_fault_node(fa, ctx->s0);
+    if (ne) cudaEventRecord(*ne, ctx->s0);
+  }
+  // fork: fault band on s1, volume shell on s2, volume interior on s0
+  cudaEventRecord(ctx->ev_fork, ctx->s0);
+  if (vb) cudaEventRecord(*vb, ctx->s0);
+  if (p.rupture) {
+    cudaStreamWaitEvent(ctx->s1, ctx->ev_fork, 0);
+    launch_fault_band(fa, ctx->s1);
+    cudaEventRecord(ctx->ev_join, ctx->s1);
+  }
+  cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
+  VolArgs va = vol_args(ctx, pattern, irk);
   long long nodes =
       launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke);
   ctx->interior_nodes = nodes - (p.rupture ? 7LL * ctx->n_band_columns : 0);
@@ -1000,5 +1030,309 @@ int dfd_output_close(dfd_ctx* ctx) {
   ctx->out_open = false;
   return DFD_OK;
 }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ ensemble --
+// A batch of prepared scenarios (contexts on one device) stepped together: per RK stage
+// one batched launch each of the fault node, fault band and general (shell) kernels over
+// every scenario, and one persistent launch of the tiled interior kernel whose units span
+// all scenarios.  The per-stage argument tables live in device memory (one set per flag
+// pattern and stage); each step is replayed from a CUDA graph.  Scenario state stays in
+// the scenarios' own contexts, so results are read with the usual getters.
+struct EnsStage {
+  FaultArgs* fault = nullptr;  // rupture scenarios
+  int* fstart = nullptr;       // (nf + 1) block starts of the fault kernels
+  int fblocks = 0;
+  VolArgs* vol = nullptr;      // all scenarios
+  Boxes* boxes = nullptr;
+  int* sstart = nullptr;       // (n + 1) block starts of the shell kernel
+  int sblocks = 0;
+  TileScen* tile = nullptr;    // all scenarios
+  TileScen first;              // scenario 0, passed by value (stage-wide values)
+  int nunits = 0;
+  bool pmlp = false;
+  int FX = 1, FY = 1, FZ = 1;
+};
+
+struct dfd_ens {
+  std::vector<dfd_ctx*> sc;
+  std::vector<int> rup;        // indices of rupture scenarios
+  int device = 0;
+  int nsm = 148;
+  int chunk = 0;               // planes per unit of the tiled kernel (0: per-scenario plan)
+  cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
+  int* it_dev = nullptr;
+  int* sched = nullptr;
+  int* err = nullptr;
+  std::vector<void*> allocs;
+  EnsStage st[8][4];
+  bool built = false;
+  cudaGraphExec_t graph[8] = {};
+  std::string msg;
+  long long nodes = 0;
+};
+
+static int ens_fail(dfd_ens* e, int code, const std::string& m) {
+  if (e) e->msg = m;
+  return code;
+}
+#define ECK(call)                                                                          \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess) return ens_fail(e, DFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+template <typename T>
+static int ens_upload(dfd_ens* e, T** dst, const std::vector<T>& v) {
+  void* p = nullptr;
+  ECK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(v.size(), 1)));
+  e->allocs.push_back(p);
+  if (!v.empty()) ECK(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  *dst = (T*)p;
+  return DFD_OK;
+}
+
+// tables of every (pattern, stage): argument structs, block starts, tile units
+static int ens_build(dfd_ens* e) {
+  for (auto& row : e->st)
+    for (auto& t : row) t = EnsStage();
+  for (void* p : e->allocs) cudaFree(p);
+  e->allocs.clear();
+  static const int bin[4] = {0, 1, 2, 1};
+  const int n = (int)e->sc.size();
+  for (int pat = 0; pat < 8; pat++)
+    for (int irk = 0; irk < 4; irk++) {
+      EnsStage& S = e->st[pat][irk];
+      int sg = (irk % 2) ? -1 : 1;
+      S.FX = kFlags[pat][0] * sg; S.FY = kFlags[pat][1] * sg; S.FZ = kFlags[pat][2] * sg;
+      std::vector<FaultArgs> fa;
+      std::vector<int> fs(1, 0);
+      for (int r : e->rup) {
+        FaultArgs a = fault_args(e->sc[r], pat, irk);
+        a.it_dev = e->it_dev;  // one step counter for the whole ensemble
+        fa.push_back(a);
+        fs.push_back(fs.back() + ((a.d.nj + 31) / 32) * ((a.d.nk + 3) / 4));
+      }
+      S.fblocks = fs.back();
+      std::vector<VolArgs> va;
+      std::vector<Boxes> bx;
+      std::vector<int> ss(1, 0);
+      std::vector<TileScen> ts(n);
+      int units = 0;
+      for (int i = 0; i < n; i++) {
+        dfd_ctx* c = e->sc[i];
+        VolArgs a = vol_args(c, pat, irk);
+        VolPlan pl = plan_volume(a, c->use_tile ? &c->tile : nullptr);
+        if (!pl.tiled) return ens_fail(e, DFD_ERR_PARAM, "scenario " + std::to_string(i) + " cannot use the tiled kernel");
+        va.push_back(a);
+        bx.push_back(pl.bx);
+        ss.push_back(ss.back() + pl.shell_blocks);
+        int grid = 0;
+        TileSched sch = tile_plan(pl.lo, pl.hi, e->nsm, &grid);
+        if (e->chunk > 0) {
+          sch.ci = std::min(e->chunk, pl.hi.x - pl.lo.x);
+          sch.nunits = sch.ntj * sch.ntk * ((pl.hi.x - pl.lo.x + sch.ci - 1) / sch.ci);
+        }
+        TileScen& t = ts[i];
+        t.mp.win = c->tile.halo[bin[irk]];
+        t.mp.w0 = c->tile.centre[0];
+        t.mp.t = c->tile.centre[3];
+        t.mp.plane = c->tile.plane;
+        t.a = a;
+        t.sc = sch;
+        t.unit0 = units;
+        units += sch.nunits;
+        S.pmlp = S.pmlp || pl.pmlp;
+      }
+      S.nunits = units;
+      S.sblocks = ss.back();
+      S.first = ts[0];
+      int r = 0;
+      if (!e->rup.empty()) {
+        r = r ? r : ens_upload(e, &S.fault, fa);
+        r = r ? r : ens_upload(e, &S.fstart, fs);
+      }
+      r = r ? r : ens_upload(e, &S.vol, va);
+      r = r ? r : ens_upload(e, &S.boxes, bx);
+      r = r ? r : ens_upload(e, &S.sstart, ss);
+      r = r ? r : ens_upload(e, &S.tile, ts);
+      if (r) return r;
+    }
+  e->built = true;
+  return DFD_OK;
+}
+
+static int ens_enqueue(dfd_ens* e, int pat, int irk) {
+  const EnsStage& S = e->st[pat][irk];
+  const int nr = (int)e->rup.size(), n = (int)e->sc.size();
+  if (nr) launch_fault_node_batch(S.fault, S.fstart, nr, S.fblocks, S.FY, S.FZ, e->s0);
+  cudaEventRecord(e->ev_fork, e->s0);
+  if (nr) {
+    cudaStreamWaitEvent(e->s1, e->ev_fork, 0);
+    launch_fault_band_batch(S.fault, S.fstart, nr, S.fblocks, S.FX, S.FY, S.FZ, e->s1);
+    cudaEventRecord(e->ev_join, e->s1);
+  }
+  cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
+  launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, e->s2);
+  cudaEventRecord(e->ev_join2, e->s2);
+  launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, S.pmlp, e->err, e->sched, e->s0);
+  if (nr) cudaStreamWaitEvent(e->s0, e->ev_join, 0);
+  cudaStreamWaitEvent(e->s0, e->ev_join2, 0);
+  cudaError_t ce = cudaGetLastError();
+  return ce == cudaSuccess ? DFD_OK : ens_fail(e, DFD_ERR_CUDA, std::string("ensemble stage: ") + cudaGetErrorString(ce));
+}
+
+static void ens_drop_graphs(dfd_ens* e) {
+  for (auto& g : e->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+static int ens_graph(dfd_ens* e, int pat) {
+  cudaGraph_t g;
+  ECK(cudaStreamBeginCapture(e->s0, cudaStreamCaptureModeThreadLocal));
+  int r = 0;
+  for (int irk = 0; irk < 4 && !r; irk++) r = ens_enqueue(e, pat, irk);
+  dfd::inc_it_kernel<<<1, 1, 0, e->s0>>>(e->it_dev);
+  cudaError_t ce = cudaStreamEndCapture(e->s0, &g);
+  if (r) return r;
+  ECK(ce);
+  ECK(cudaGraphInstantiate(&e->graph[pat], g, 0));
+  cudaGraphDestroy(g);
+  return DFD_OK;
+}
+
+extern "C" {
+
+int dfd_ens_create(dfd_ctx* const* scenarios, int n, dfd_ens** out) {
+  if (!scenarios || n <= 0 || !out) return DFD_ERR_PARAM;
+  *out = nullptr;
+  dfd_ens* e = new dfd_ens();
+  e->device = scenarios[0]->device;
+  for (int i = 0; i < n; i++) {
+    dfd_ctx* c = scenarios[i];
+    if (!c || !c->ready || c->device != e->device || c->next_stage != 0 || !c->use_tile) {
+      delete e;
+      return DFD_ERR_PARAM;
+    }
+    e->sc.push_back(c);
+    if (c->p.rupture) e->rup.push_back(i);
+    e->nodes += (long long)c->p.NX * c->p.NY * c->p.NZ;
+  }
+  cudaSetDevice(e->device);
+  e->nsm = scenarios[0]->tile.nsm;
+  auto done = [&](int rc) {
+    if (rc) dfd_ens_destroy(e);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&e->s1, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&e->s2, cudaStreamNonBlocking) != cudaSuccess)
+    return done(DFD_ERR_CUDA);
+  cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&e->ev_join2, cudaEventDisableTiming);
+  void* p = nullptr;
+  if (cudaMalloc(&p, 4 * sizeof(int)) != cudaSuccess) return done(DFD_ERR_CUDA);
+  cudaMemset(p, 0, 4 * sizeof(int));
+  e->it_dev = (int*)p;
+  e->sched = e->it_dev + 1;  // unit counter, finished-CTA counter
+  e->err = e->it_dev + 3;
+  for (dfd_ctx* c : e->sc) cudaStreamSynchronize(c->s0);
+  int r = ens_build(e);
+  if (r) return done(r);
+  *out = e;
+  return DFD_OK;
+}
+
+int dfd_ens_destroy(dfd_ens* e) {
+  if (!e) return DFD_OK;
+  cudaSetDevice(e->device);
+  ens_drop_graphs(e);
+  if (e->s0) cudaStreamSynchronize(e->s0);
+  if (e->s1) cudaStreamSynchronize(e->s1);
+  if (e->s2) cudaStreamSynchronize(e->s2);
+  for (void* p : e->allocs) cudaFree(p);
+  if (e->it_dev) cudaFree(e->it_dev);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
+  if (e->ev_join2) cudaEventDestroy(e->ev_join2);
+  if (e->s0) cudaStreamDestroy(e->s0);
+  if (e->s1) cudaStreamDestroy(e->s1);
+  if (e->s2) cudaStreamDestroy(e->s2);
+  delete e;
+  return DFD_OK;
+}
+
+int dfd_ens_run(dfd_ens* e, int it0, int nsteps) {
+  if (!e) return DFD_ERR_PARAM;
+  cudaSetDevice(e->device);
+  dfd::set_it_kernel<<<1, 1, 0, e->s0>>>(e->it_dev, it0);
+  for (int s = 0; s < nsteps; s++) {
+    int pat = (((it0 + s) % 8) + 8) % 8;
+    if (!e->graph[pat]) {
+      int r = ens_graph(e, pat);
+      if (r) return r;
+    }
+    ECK(cudaGraphLaunch(e->graph[pat], e->s0));
+  }
+  return DFD_OK;
+}
+
+int dfd_ens_synchronize(dfd_ens* e) {
+  if (!e) return DFD_ERR_PARAM;
+  cudaSetDevice(e->device);
+  ECK(cudaStreamSynchronize(e->s0));
+  ECK(cudaStreamSynchronize(e->s1));
+  ECK(cudaStreamSynchronize(e->s2));
+  int f = 0;
+  ECK(cudaMemcpy(&f, e->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (f) return ens_fail(e, DFD_ERR_CUDA, "tiled interior kernel: a TMA copy did not complete");
+  return DFD_OK;
+}
+
+int dfd_ens_run_timed(dfd_ens* e, int it0, int nsteps, float* ms) {
+  if (!e || nsteps <= 0) return DFD_ERR_PARAM;
+  cudaSetDevice(e->device);
+  cudaEvent_t a, b;
+  ECK(cudaEventCreate(&a));
+  ECK(cudaEventCreate(&b));
+  for (int s = 0; s < nsteps; s++) {  // graphs first, outside the timed region
+    int pat = (((it0 + s) % 8) + 8) % 8;
+    if (!e->graph[pat]) {
+      int r = ens_graph(e, pat);
+      if (r) return r;
+    }
+  }
+  ECK(cudaEventRecord(a, e->s0));
+  int r = dfd_ens_run(e, it0, nsteps);
+  if (r) return r;
+  ECK(cudaEventRecord(b, e->s0));
+  ECK(cudaEventSynchronize(b));
+  float t = 0;
+  ECK(cudaEventElapsedTime(&t, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (ms) *ms = t;
+  return dfd_ens_synchronize(e);
+}
+
+int dfd_ens_set_chunk(dfd_ens* e, int chunk) {
+  if (!e || chunk < 0) return DFD_ERR_PARAM;
+  cudaSetDevice(e->device);
+  ECK(cudaStreamSynchronize(e->s0));
+  ens_drop_graphs(e);
+  e->chunk = chunk;
+  return ens_build(e);
+}
+
+int dfd_ens_nodes(const dfd_ens* e, long long* nodes) {
+  if (!e || !nodes) return DFD_ERR_PARAM;
+  *nodes = e->nodes;
+  return DFD_OK;
+}
+
+const char* dfd_ens_last_error(const dfd_ens* e) { return e ? e->msg.c_str() : ""; }
 
 }  // extern "C"

@@ -185,20 +185,21 @@ __device__ double newton_rs(double x, double psi, double ra, double Vhat, double
   return xn;
 }
 
+// Body of the fault node kernel for the block (bx, by) of a (32, 4) grid over (NY, NZ);
+// snet is the block's shared copy of the learned-guess weights.
 template <int FY, int FZ>
-__global__ void __launch_bounds__(128) fault_node_kernel(FaultArgs a) {
+__device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int by, float* snet) {
   const Dims& d = a.d;
   // learned-guess weights staged in shared memory (every thread reads the same weight at
   // the same time: a broadcast)
-  __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
   const bool learned = a.friction_type != 0 && a.rs_guess && a.guess_net;
   if (learned) {
     const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
     for (int p = tid; p < DFD_MLP_PARAMS; p += nt) snet[p] = __ldg(a.guess_net + p);
     __syncthreads();
   }
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int k = blockIdx.y * blockDim.y + threadIdx.y;
+  int j = bx * blockDim.x + threadIdx.x;
+  int k = by * blockDim.y + threadIdx.y;
   if (j >= d.nj || k >= d.nk) return;
   int q2 = j + k * d.nj;
   if (a.united[q2]) return;
@@ -502,10 +503,10 @@ __device__ __forceinline__ void rk_store(const FaultArgs& a, long long x, float 
 }
 
 template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(128) fault_band_kernel(FaultArgs a) {
+__device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int by) {
   const Dims& d = a.d;
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int k = blockIdx.y * blockDim.y + threadIdx.y;
+  int j = bx * blockDim.x + threadIdx.x;
+  int k = by * blockDim.y + threadIdx.y;
   if (j >= d.nj || k >= d.nk) return;
   int q2 = j + k * d.nj;
   if (a.united[q2]) {
@@ -771,6 +772,38 @@ __global__ void __launch_bounds__(128) fault_band_kernel(FaultArgs a) {
   fault_to_volume(a, a.FWout, a.Wout, j1, k1, damp0);
 }
 
+template <int FY, int FZ>
+__global__ void __launch_bounds__(128) fault_node_kernel(const __grid_constant__ FaultArgs a) {
+  __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
+  fault_node_body<FY, FZ>(a, blockIdx.x, blockIdx.y, snet);
+}
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(128) fault_band_kernel(const __grid_constant__ FaultArgs a) {
+  fault_band_body<FX, FY, FZ>(a, blockIdx.x, blockIdx.y);
+}
+
+// Batched launches over the scenarios of an ensemble: scenario s owns the blocks
+// [start[s], start[s+1]) of a 1-D grid, laid out as its own (32, 4)-block grid over (NY, NZ).
+template <int FY, int FZ>
+__global__ void __launch_bounds__(128) fault_node_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
+                                                        int n) {
+  __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
+  int loc;
+  const int sc = scenario_of(start, n, blockIdx.x, &loc);
+  const FaultArgs& a = tab[sc];
+  const int gx = (a.d.nj + 31) / 32;
+  fault_node_body<FY, FZ>(a, loc % gx, loc / gx, snet);
+}
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(128) fault_band_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
+                                                        int n) {
+  int loc;
+  const int sc = scenario_of(start, n, blockIdx.x, &loc);
+  const FaultArgs& a = tab[sc];
+  const int gx = (a.d.nj + 31) / 32;
+  fault_band_body<FX, FY, FZ>(a, loc % gx, loc / gx);
+}
+
 void launch_fault_node(const FaultArgs& a, cudaStream_t s) {
   dim3 block(32, 4, 1);
   dim3 grid((a.d.nj + 31) / 32, (a.d.nk + 3) / 4, 1);
@@ -796,6 +829,35 @@ void launch_fault_band(const FaultArgs& a, cudaStream_t s) {
     case 5: fault_band_kernel<1, -1, 1><<<grid, block, 0, s>>>(a); break;
     case 6: fault_band_kernel<1, 1, -1><<<grid, block, 0, s>>>(a); break;
     default: fault_band_kernel<1, 1, 1><<<grid, block, 0, s>>>(a); break;
+  }
+}
+
+// tab, start: device arrays of n scenarios (start has n + 1 entries, start[n] = blocks);
+// FX, FY, FZ are the ensemble's (every scenario is at the same step and stage)
+void launch_fault_node_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FY, int FZ,
+                             cudaStream_t s) {
+  dim3 block(32, 4, 1);
+  int code = (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: fault_node_batch<-1, -1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 1: fault_node_batch<-1, 1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 2: fault_node_batch<1, -1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    default: fault_node_batch<1, 1><<<blocks, block, 0, s>>>(tab, start, n); break;
+  }
+}
+void launch_fault_band_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FX, int FY, int FZ,
+                             cudaStream_t s) {
+  dim3 block(32, 4, 1);
+  int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: fault_band_batch<-1, -1, -1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 1: fault_band_batch<-1, -1, 1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 2: fault_band_batch<-1, 1, -1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 3: fault_band_batch<-1, 1, 1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 4: fault_band_batch<1, -1, -1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 5: fault_band_batch<1, -1, 1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    case 6: fault_band_batch<1, 1, -1><<<blocks, block, 0, s>>>(tab, start, n); break;
+    default: fault_band_batch<1, 1, 1><<<blocks, block, 0, s>>>(tab, start, n); break;
   }
 }
 

@@ -179,6 +179,58 @@ struct TileCtx {
 };
 bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, int* err, int* sched,
                 int device);
+// Units of the tiled kernel over a box: tile columns (32 y x 8 z) times chunks of x planes.
+struct TileSched {
+  int lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;  // tiled box, interior indices, half open
+  int ntj, ntk, ci, nunits;               // tiles in y and z, planes per chunk, units
+};
+// One scenario of a batched (ensemble) launch of the tiled kernel, in device memory.
+struct alignas(64) TileScen {
+  TileMaps mp;
+  VolArgs a;
+  TileSched sc;
+  int unit0;  // first global unit of the scenario
+};
+// Boxes of the general (shell) kernel: up to eight, each flattened or tiled.
+struct Boxes {
+  int n;
+  int lo[8][3], hi[8][3];  // (i, j, k) interior-index bounds, half open
+  int thin[8];             // flattened (y, z) mapping
+  int start[9];            // first block of each box
+};
+// Volume work of one stage of one scenario: the box of the tiled (or plain) interior
+// kernel and the general kernel's boxes.
+struct VolPlan {
+  bool tiled, pmlp, plain;
+  int3 lo, hi;        // interior-kernel box
+  Boxes bx;
+  int shell_blocks;
+  long long nodes;    // nodes of the interior-kernel box
+};
+VolPlan plan_volume(const VolArgs& a, const TileCtx* tc);
+bool tile_feasible(const TileCtx* tc, const VolArgs& a, int3 lo, int3 hi);
+TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid);
+// batched launches (dfd_volume.cu, dfd_tile.cu, dfd_fault.cu)
+void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,
+                       int FZ, bool pmlp, int* err, int* sched, cudaStream_t s);
+void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, int FX, int FY,
+                        int FZ, cudaStream_t s);
+void launch_fault_node_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FY, int FZ,
+                             cudaStream_t s);
+void launch_fault_band_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FX, int FY, int FZ,
+                             cudaStream_t s);
+
+// scenario owning block b of a batched launch: start[s] <= b < start[s + 1]
+__device__ __forceinline__ int scenario_of(const int* start, int n, int b, int* local) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    int m = (lo + hi) / 2;
+    if (start[m] <= b) lo = m; else hi = m;
+  }
+  *local = b - start[lo];
+  return lo;
+}
+
 // pmlp: the box contains PML nodes (the kernel variant with the PML path)
 bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi, bool pmlp,
                  cudaStream_t s);

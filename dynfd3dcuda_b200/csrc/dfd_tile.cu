@@ -103,10 +103,6 @@ __device__ __forceinline__ float d5s(const float* p) {
   else return d5v<-1>(p[-3 * S], p[-2 * S], p[-S], p[0], p[S]);
 }
 
-struct TileSched {
-  int lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;  // tiled box, interior indices, half open
-  int ntj, ntk, ci, nunits;               // tiles in y and z, planes per chunk, units
-};
 
 constexpr int NCW = 2 * NTHR / 32;  // computing warps: two per 32-node row of the tile
 constexpr int NTOT = NCW * 32 + 32;  // plus one copy-issuing warp
@@ -224,10 +220,23 @@ __device__ __forceinline__ void tile_pml_point(const VolArgs& a, const float* co
 // step-start values are the stencil input), metric/media planes of the unit (NQ).  At
 // most 96 registers: the 17 warps are spread over the SM's four 16 K-register partitions,
 // five warps on one of them.
-template <int FX, int FY, int FZ, bool PMLP>
+// first scenario of a batched launch whose units include the global unit u
+__device__ __forceinline__ int tile_scenario(const TileScen* tab, int n, int u) {
+  int lo = 0, hi = n;  // tab[lo].unit0 <= u < tab[hi].unit0
+  while (hi - lo > 1) {
+    int m = (lo + hi) / 2;
+    if (tab[m].unit0 <= u) lo = m; else hi = m;
+  }
+  return lo;
+}
+
+// BATCH: the units of the nscen scenarios of tab (an ensemble) in one launch; the
+// parameters mp0, a0, sc0 then describe scenario 0 and give the stage's common values.
+template <int FX, int FY, int FZ, bool PMLP, bool BATCH>
 __global__ void __maxnreg__(96)
-    volume_tile_kernel(const __grid_constant__ TileMaps mp, const VolArgs a, const TileSched sc, int* err,
-                       int* sched) {
+    volume_tile_kernel(const __grid_constant__ TileMaps mp0, const __grid_constant__ VolArgs a0,
+                       const __grid_constant__ TileSched sc0, const TileScen* __restrict__ tab, int nscen,
+                       int nunits, int* err, int* sched) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   float* win = reinterpret_cast<float*>(smraw);
   float* pw = win + NS * HSLOT;
@@ -239,13 +248,11 @@ __global__ void __maxnreg__(96)
   uint64_t* full_q = empty_p + NP;
   uint64_t* empty_q = full_q + NQ;
   int* qunit = reinterpret_cast<int*>(empty_q + NQ);  // unit of each plane slot (-1: no more)
-  const Dims& d = a.d;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int XLO = FX == 1 ? -1 : -3;  // first stencil plane relative to x
   constexpr int RZ = FZ == 1 ? 1 : 3;     // row of the tile's first z node inside the halo box
-  const int irk = a.irk;
+  const int irk = a0.irk;
   const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1, usep = needW0 || needT;
-  const int ntile = sc.ntj * sc.ntk;
   const int G = gridDim.x;
 
   if (threadIdx.x == 0) {
@@ -269,12 +276,19 @@ __global__ void __maxnreg__(96)
     while (ok) {
       const int u = atomicAdd(sched, 1);
       if (qcount >= NQ && !(ok = mbar_wait(empty_q + qr.slot, qr.phase ^ 1))) break;
-      if (u >= sc.nunits) {
+      if (u >= nunits) {
         qunit[qr.slot] = -1;  // tell the computing warps that there is no further unit
         mbar_arrive(full_q + qr.slot);
         break;
       }
-      const int tc = u / ntile, ru = u % ntile;
+      const int scn = BATCH ? tile_scenario(tab, nscen, u) : 0;
+      const TileMaps& mp = BATCH ? tab[scn].mp : mp0;
+      const VolArgs& a = BATCH ? tab[scn].a : a0;
+      const TileSched& sc = BATCH ? tab[scn].sc : sc0;
+      const Dims& d = a.d;
+      const int lu = BATCH ? u - tab[scn].unit0 : u;
+      const int ntile = sc.ntj * sc.ntk;
+      const int tc = lu / ntile, ru = lu % ntile;
       const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
       const int j0 = sc.lo_y + (ru % sc.ntj) * TJ, k0 = sc.lo_z + (ru / sc.ntj) * TK;
       const int cw0 = j0 + 3 + d.oy - 4, cw1 = k0 + 3 - RZ, cp0 = j0 + 3 + d.oy, cp1 = k0 + 3;
@@ -326,8 +340,6 @@ __global__ void __maxnreg__(96)
   // second the constitutive law (stress fields)
   const int role = warp >= NCW / 2 ? 1 : 0;
   const int ty = warp - role * (NCW / 2);
-  const long long n = d.nxyz;
-  const float r = a.rDH;
   const int hc = (ty + RZ) * HW + lane + 4;  // node inside a halo field box
   const int pc = ty * TJ + lane;             // node inside a pointwise field box
   Ring wr, pr, qr;  // next stencil plane to wait for; RK-register slot of the step; unit planes
@@ -339,7 +351,15 @@ __global__ void __maxnreg__(96)
     }
     const int u = qunit[qr.slot];
     if (u < 0) break;
-    const int tc = u / ntile, ru = u % ntile;
+    const int scn = BATCH ? tile_scenario(tab, nscen, u) : 0;
+    const VolArgs& a = BATCH ? tab[scn].a : a0;
+    const TileSched& sc = BATCH ? tab[scn].sc : sc0;
+    const Dims& d = a.d;
+    const long long n = d.nxyz;
+    const float r = a.rDH;
+    const int lu = BATCH ? u - tab[scn].unit0 : u;
+    const int ntile = sc.ntj * sc.ntk;
+    const int tc = lu / ntile, ru = lu % ntile;
     const int ib = sc.lo_x + tc * sc.ci, ie = min(ib + sc.ci, sc.hi_x);
     const int j = sc.lo_y + (ru % sc.ntj) * TJ + lane, k = sc.lo_z + (ru / sc.ntj) * TK + ty;
     const bool active = j < sc.hi_y && k < sc.hi_z;
@@ -513,10 +533,13 @@ static bool make_map(CUtensorMap* m, const Dims& d, const float* base, int nf, i
 
 template <int FX, int FY, int FZ>
 static bool set_smem() {
-  return cudaFuncSetAttribute(volume_tile_kernel<FX, FY, FZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)SMEM_BYTES) == cudaSuccess &&
-         cudaFuncSetAttribute(volume_tile_kernel<FX, FY, FZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)SMEM_BYTES) == cudaSuccess;
+  auto one = [](const void* f) {
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES) == cudaSuccess;
+  };
+  return one((const void*)volume_tile_kernel<FX, FY, FZ, false, false>) &&
+         one((const void*)volume_tile_kernel<FX, FY, FZ, true, false>) &&
+         one((const void*)volume_tile_kernel<FX, FY, FZ, false, true>) &&
+         one((const void*)volume_tile_kernel<FX, FY, FZ, true, true>);
 }
 
 // 3-D map over the 12 metric / media planes (py, nz, 12) with box (32, 8, 12)
@@ -555,7 +578,7 @@ bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* plan
 
 // Chunking of the x range: minimise the busiest CTA's plane loads, ceil(units / grid) x
 // (planes per chunk + 4 halo planes).
-static TileSched plan(const Dims& d, int3 lo, int3 hi, int nsm, int* grid) {
+TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid) {
   TileSched s;
   s.lo_x = lo.x; s.lo_y = lo.y; s.lo_z = lo.z; s.hi_x = hi.x; s.hi_y = hi.y; s.hi_z = hi.z;
   s.ntj = (hi.y - lo.y + TJ - 1) / TJ;
@@ -570,7 +593,6 @@ static TileSched plan(const Dims& d, int3 lo, int3 hi, int nsm, int* grid) {
     long long cost = (units + g - 1) / g * (ci + 4);
     if (best < 0 || cost < best) { best = cost; s.ci = ci; s.nunits = (int)units; *grid = (int)g; }
   }
-  (void)d;
   return s;
 }
 
@@ -582,18 +604,50 @@ static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3
   mp.t = tc.centre[3];
   mp.plane = tc.plane;
   int grid = 0;
-  TileSched sc = plan(a.d, lo, hi, tc.nsm, &grid);
+  TileSched sc = tile_plan(lo, hi, tc.nsm, &grid);
   if (pmlp)
-    volume_tile_kernel<FX, FY, FZ, true><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err, tc.sched);
+    volume_tile_kernel<FX, FY, FZ, true, false>
+        <<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, nullptr, 1, sc.nunits, tc.err, tc.sched);
   else
-    volume_tile_kernel<FX, FY, FZ, false><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, tc.err, tc.sched);
+    volume_tile_kernel<FX, FY, FZ, false, false>
+        <<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, nullptr, 1, sc.nunits, tc.err, tc.sched);
 }
 
 // true when the tiled kernel took the interior box
+bool tile_feasible(const TileCtx* tc, const VolArgs& a, int3 lo, int3 hi) {
+  if (!tc || !tc->ok) return false;
+  return (lo.y + 3 + a.d.oy) % 4 == 0 && lo.z >= 0 && hi.x > lo.x && hi.y > lo.y && hi.z > lo.z;
+}
+
+template <int FX, int FY, int FZ>
+static void launch_tb(const TileScen& f, const TileScen* tab, int n, int nunits, int grid, bool pmlp, int* err,
+                      int* sched, cudaStream_t s) {
+  if (pmlp)
+    volume_tile_kernel<FX, FY, FZ, true, true>
+        <<<grid, NTOT, SMEM_BYTES, s>>>(f.mp, f.a, f.sc, tab, n, nunits, err, sched);
+  else
+    volume_tile_kernel<FX, FY, FZ, false, true>
+        <<<grid, NTOT, SMEM_BYTES, s>>>(f.mp, f.a, f.sc, tab, n, nunits, err, sched);
+}
+// every scenario of an ensemble in one persistent launch (units numbered across them)
+void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,
+                       int FZ, bool pmlp, int* err, int* sched, cudaStream_t s) {
+  int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: launch_tb<-1, -1, -1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+    case 1: launch_tb<-1, -1, 1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+    case 2: launch_tb<-1, 1, -1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+    case 3: launch_tb<-1, 1, 1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+    case 4: launch_tb<1, -1, -1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+    case 5: launch_tb<1, -1, 1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+    case 6: launch_tb<1, 1, -1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+    default: launch_tb<1, 1, 1>(first, tab, n, nunits, grid, pmlp, err, sched, s); break;
+  }
+}
+
 bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi, bool pmlp,
                  cudaStream_t s) {
-  if (!tc || !tc->ok) return false;
-  if ((lo.y + 3 + a.d.oy) % 4 != 0 || lo.z < 0 || hi.x <= lo.x || hi.y <= lo.y || hi.z <= lo.z) return false;
+  if (!tile_feasible(tc, a, lo, hi)) return false;
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
     case 0: launch_t<-1, -1, -1>(*tc, a, bin, lo, hi, pmlp, s); break;

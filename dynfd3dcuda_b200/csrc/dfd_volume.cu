@@ -191,20 +191,14 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 // thinner box (the y slabs of the PML, the free-surface rows) is flattened over (y, z)
 // with y fastest, so that no thread idles and the y-face PML state (y fastest over N
 // nodes, then z) is read contiguously.
-struct Boxes {
-  int n;
-  int lo[8][3], hi[8][3];  // (i, j, k) interior-index bounds, half open
-  int thin[8];             // flattened (y, z) mapping
-  int start[9];            // first block of each box
-};
-
 constexpr int SHELL_THREADS = 128;
 
+// block blk of the shell grid of one scenario
 template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(SHELL_THREADS, 4) volume_shell_kernel(VolArgs a, Boxes bx) {
+__device__ __forceinline__ void volume_shell_body(const VolArgs& a, const Boxes& bx, int blk) {
   int b = 0;
-  while (b + 1 < bx.n && (int)blockIdx.x >= bx.start[b + 1]) b++;
-  int loc = blockIdx.x - bx.start[b];
+  while (b + 1 < bx.n && blk >= bx.start[b + 1]) b++;
+  int loc = blk - bx.start[b];
   int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
   int i, j, k;
   if (bx.thin[b]) {
@@ -223,6 +217,20 @@ __global__ void __launch_bounds__(SHELL_THREADS, 4) volume_shell_kernel(VolArgs 
     if (i >= ni || j >= nj || k >= nk) return;
   }
   volume_point_general<FX, FY, FZ>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
+}
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(SHELL_THREADS, 4)
+    volume_shell_kernel(const __grid_constant__ VolArgs a, const __grid_constant__ Boxes bx) {
+  volume_shell_body<FX, FY, FZ>(a, bx, blockIdx.x);
+}
+// all scenarios of an ensemble in one launch: scenario s owns blocks [start[s], start[s+1])
+template <int FX, int FY, int FZ>
+__global__ void __launch_bounds__(SHELL_THREADS, 4)
+    volume_shell_batch(const VolArgs* __restrict__ tab, const Boxes* __restrict__ boxes,
+                       const int* __restrict__ start, int n) {
+  int loc;
+  const int sc = scenario_of(start, n, blockIdx.x, &loc);
+  volume_shell_body<FX, FY, FZ>(tab[sc], boxes[sc], loc);
 }
 
 // Interior kernel: no PML (beta = 1, no auxiliary state), no free-surface rows.  Each
@@ -283,11 +291,14 @@ __global__ void __launch_bounds__(256, 3) volume_interior_kernel(VolArgs a, int3
   }
 }
 
-template <int FX, int FY, int FZ>
-static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin,
-                              cudaEvent_t* kb, cudaEvent_t* ke) {
+// Volume work of one stage: which box the tiled (or plain) interior kernel takes and the
+// boxes of the general kernel around it.
+VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
   const Dims& d = a.d;
-  Boxes bx;
+  VolPlan pl;
+  pl.tiled = pl.pmlp = pl.plain = false;
+  pl.nodes = 0;
+  Boxes& bx = pl.bx;
   bx.n = 0;
   auto add = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
     if (i1 <= i0 || j1 <= j0 || k1 <= k0) return;
@@ -301,13 +312,12 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
   int nz0 = a.aux[4] ? d.N : 0, nz1 = a.aux[5] ? d.N : (a.freenode ? 3 : 0);
   int3 lo = make_int3(nx0, ny0, nz0), hi = make_int3(d.ni - nx1, d.nj - ny1, d.nk - nz1);
   const int ktop = a.freenode ? d.nk - 3 : d.nk;
-  long long nodes = 0;  // nodes of the box the interior (or tiled) kernel covers
-  if (kb) cudaEventRecord(*kb, s);
-  if (tc && tc->ok && tc->pml == 1 &&
-      launch_tile(tc, a, FX, FY, FZ, bin, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop), true, s)) {
+  if (tc && tc->ok && tc->pml == 1 && tile_feasible(tc, a, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop))) {
     // TMA-tiled kernel over every node below the free-surface rows; the general kernel
     // takes the free-surface rows
-    nodes = (long long)d.ni * d.nj * ktop;
+    pl.tiled = pl.pmlp = true;
+    pl.lo = make_int3(0, 0, 0);
+    pl.hi = make_int3(d.ni, d.nj, ktop);
     add(0, d.ni, 0, d.nj, ktop, d.nk);
   } else {
     // interior box by the TMA-tiled kernel (or the plain interior kernel), the shell
@@ -315,8 +325,7 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     // tiled box starts at the next boundary, and the general kernel takes the (at most
     // three) interior columns before it.
     int3 tlo = lo, thi = hi;
-    const int ygap = (4 - (lo.y + 3 + d.oy) % 4) % 4;
-    tlo.y += ygap;
+    tlo.y += (4 - (lo.y + 3 + d.oy) % 4) % 4;
     const bool xslabs = tc && tc->pml == 3;
     if (xslabs) {
       // the tiles also cover the two x slabs of the PML
@@ -324,17 +333,18 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
       thi.x = d.ni;
     }
     const bool some = hi.x > lo.x && hi.y > lo.y && hi.z > lo.z;
-    if (some && thi.y > tlo.y && launch_tile(tc, a, FX, FY, FZ, bin, tlo, thi, xslabs, s)) {
+    if (some && thi.y > tlo.y && tile_feasible(tc, a, tlo, thi)) {
+      pl.tiled = true;
+      pl.pmlp = xslabs;
+      pl.lo = tlo;
+      pl.hi = thi;
       add(tlo.x, thi.x, lo.y, tlo.y, lo.z, hi.z);
       lo.x = tlo.x;
       hi.x = thi.x;
-      nodes = (long long)(thi.x - tlo.x) * (thi.y - tlo.y) * (thi.z - tlo.z);
     } else if (some) {
-      const int chunk = 8;
-      dim3 block(32, 8, 1);
-      dim3 grid((hi.y - lo.y + 31) / 32, (hi.z - lo.z + 7) / 8, (hi.x - lo.x + chunk - 1) / chunk);
-      volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, lo, hi, chunk);
-      nodes = (long long)(hi.x - lo.x) * (hi.y - lo.y) * (hi.z - lo.z);
+      pl.plain = true;
+      pl.lo = lo;
+      pl.hi = hi;
     }
     add(0, lo.x, 0, d.nj, 0, d.nk);
     add(hi.x, d.ni, 0, d.nj, 0, d.nk);
@@ -343,6 +353,7 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     add(lo.x, hi.x, lo.y, hi.y, 0, lo.z);
     add(lo.x, hi.x, lo.y, hi.y, hi.z, d.nk);
   }
+  if (pl.tiled || pl.plain) pl.nodes = (long long)(pl.hi.x - pl.lo.x) * (pl.hi.y - pl.lo.y) * (pl.hi.z - pl.lo.z);
   int tot = 0;
   for (int b = 0; b < bx.n; b++) {
     bx.start[b] = tot;
@@ -351,9 +362,47 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     tot += bx.thin[b] ? ((nj * nk + SHELL_THREADS - 1) / SHELL_THREADS) * ni : ((nj + 31) / 32) * ((nk + 3) / 4) * ni;
   }
   bx.start[bx.n] = tot;
+  pl.shell_blocks = tot;
+  return pl;
+}
+
+template <int FX, int FY, int FZ>
+static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin,
+                              cudaEvent_t* kb, cudaEvent_t* ke) {
+  const VolPlan pl = plan_volume(a, tc);
+  if (kb) cudaEventRecord(*kb, s);
+  if (pl.tiled) {
+    launch_tile(tc, a, FX, FY, FZ, bin, pl.lo, pl.hi, pl.pmlp, s);
+  } else if (pl.plain) {
+    const int chunk = 8;
+    dim3 block(32, 8, 1);
+    dim3 grid((pl.hi.y - pl.lo.y + 31) / 32, (pl.hi.z - pl.lo.z + 7) / 8, (pl.hi.x - pl.lo.x + chunk - 1) / chunk);
+    volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, pl.lo, pl.hi, chunk);
+  }
   if (ke) cudaEventRecord(*ke, s);
-  if (tot > 0) volume_shell_kernel<FX, FY, FZ><<<tot, SHELL_THREADS, 0, s_shell>>>(a, bx);
-  return nodes;
+  if (pl.shell_blocks > 0) volume_shell_kernel<FX, FY, FZ><<<pl.shell_blocks, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
+  return pl.nodes;
+}
+
+template <int FX, int FY, int FZ>
+static void shell_batch_t(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks,
+                          cudaStream_t s) {
+  volume_shell_batch<FX, FY, FZ><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n);
+}
+void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, int FX, int FY,
+                        int FZ, cudaStream_t s) {
+  if (blocks <= 0) return;
+  int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: shell_batch_t<-1, -1, -1>(tab, boxes, start, n, blocks, s); break;
+    case 1: shell_batch_t<-1, -1, 1>(tab, boxes, start, n, blocks, s); break;
+    case 2: shell_batch_t<-1, 1, -1>(tab, boxes, start, n, blocks, s); break;
+    case 3: shell_batch_t<-1, 1, 1>(tab, boxes, start, n, blocks, s); break;
+    case 4: shell_batch_t<1, -1, -1>(tab, boxes, start, n, blocks, s); break;
+    case 5: shell_batch_t<1, -1, 1>(tab, boxes, start, n, blocks, s); break;
+    case 6: shell_batch_t<1, 1, -1>(tab, boxes, start, n, blocks, s); break;
+    default: shell_batch_t<1, 1, 1>(tab, boxes, start, n, blocks, s); break;
+  }
 }
 
 // Launches the volume kernels of one stage; kb/ke (optional) are recorded on s right

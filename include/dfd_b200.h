@@ -182,6 +182,25 @@ int dfd_mlp_loss_grad(const float *w, const float *x, const float *y, int n, dou
 int dfd_mlp_train(const float *x, const float *y, int n, int epochs, int batch, float lr, unsigned seed, float *w,
                   float *loss_per_epoch);
 
+/* ---- ensemble: prepared scenarios stepped together (no counterpart in the reference,
+ *      which runs one job per process).  Every scenario is a context created, loaded and
+ *      set up as usual on the same device; the ensemble advances all of them from step
+ *      it0 with one batched launch per kernel and RK stage (fault node, fault band,
+ *      general kernel) and one persistent launch of the tiled interior kernel whose units
+ *      span every scenario, replayed from CUDA graphs.  Results stay in the scenarios'
+ *      contexts.  Destroy the ensemble before its contexts. ---- */
+typedef struct dfd_ens dfd_ens;
+int dfd_ens_create(dfd_ctx *const *scenarios, int n, dfd_ens **out);
+int dfd_ens_destroy(dfd_ens *e);
+int dfd_ens_run(dfd_ens *e, int it0, int nsteps);
+int dfd_ens_synchronize(dfd_ens *e);
+/* nsteps steps timed with CUDA events on the ensemble's stream (graphs built beforehand) */
+int dfd_ens_run_timed(dfd_ens *e, int it0, int nsteps, float *ms);
+/* x planes per unit of the tiled kernel (0: each scenario's own plan); for autotuning */
+int dfd_ens_set_chunk(dfd_ens *e, int chunk);
+int dfd_ens_nodes(const dfd_ens *e, long long *nodes);
+const char *dfd_ens_last_error(const dfd_ens *e);
+
 const char *dfd_error_string(int status);
 const char *dfd_last_error(const dfd_ctx *ctx);
 

@@ -268,6 +268,32 @@ def rs_rough_case(NY, NX, NZ, seed=0, DH=100.0, steps=40, L=0.4):
     return p, fx, st, None, None, dict(steps=steps, every=steps // 2, volume=False)
 
 
+def ensemble_case(i, seed=2025, size=(100, 300), DH=100.0, DT=0.008, steps=1000):
+    """Scenario i of the batched-ensemble configuration: grid size per axis drawn from
+    size, stress drop uniform in 2-8 MPa and Dc (slip weakening) or L (rate and state)
+    uniform in 0.2-0.8 m from the seed; even scenarios slip weakening, odd ones rate and
+    state (slip law); planar fault, homogeneous medium, PML 12, free surface."""
+    rng = np.random.default_rng([seed, i])
+    NX, NY, NZ = (int(v) for v in rng.integers(size[0], size[1] + 1, 3))
+    drop = rng.uniform(2e6, 8e6)
+    dc = rng.uniform(0.2, 0.8)
+    fg = [31, NY - 30, 31, NZ]
+    depth = min(7.5e3, 0.4 * (NZ - 31) * DH)
+    radius = min(1.5e3, 0.15 * (NY - 60) * DH)
+    p = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=DT, TMAX=steps * DT + DT / 2, PML_N=12, PML_velocity=6000.0,
+             INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Fault_grid=fg, NormalRefine=0)
+    fx = flat_geometry(NY, NZ, DH)
+    if i % 2 == 0:
+        p.update(Friction_type=0, mu_s=0.677, mu_d=0.525, Dc=dc, C0=0.0)
+        tau = 0.525 * 120e6 + drop
+        st = sw_stress(fx, fg, tn=-120e6, ts=-tau, patch=(0.0, -depth, radius), patch_ts=-82.5e6, Dc=dc, mu_d=0.525)
+    else:
+        p.update(Friction_type=2, RS_V0=1e-6, RS_f0=0.6, RS_fw=0.2, RS_Vini=1e-16, RS_L=dc, smooth_load_T=0.5)
+        st = sw_stress(fx, fg, tn=-120e6, ts=-(35e6 + drop))
+        st = rs_fields(st, fx, seed=seed + i, L=dc, patch=(0.0, -depth, radius), patch_dtau=45e6)
+    return p, fx, st
+
+
 CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan"]
 
 
