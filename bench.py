@@ -315,7 +315,7 @@ def run_ensemble(args, dfd, local):
     import cases
     import torch
 
-    n = 64
+    n = args.scenarios
     specs = [cases.ensemble_case(i) for i in range(n)]
     nodes = sum(p["NX"] * p["NY"] * p["NZ"] for p, _, _ in specs)
     need = sum((p["NX"] + 6) * (p["NY"] + 8) * (p["NZ"] + 6) * 4 * (36 + 13 + 8) for p, _, _ in specs)
@@ -339,7 +339,7 @@ def run_ensemble(args, dfd, local):
     line = {"metric": "Gpt-steps/s", "value": value, "unit": "Gpt-steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batched ensemble: 64 scenarios, grids 100-300 nodes per axis, dh=100 m, "
+            "config": {"workload": f"batched ensemble: {n} scenarios, grids 100-300 nodes per axis, dh=100 m, "
                                    "stress drop 2-8 MPa, Dc/L 0.2-0.8 m, slip weakening and rate and state mixed",
                        "nodes": nodes, "fault_nodes": nf, "scenarios": n, "parallelism": "one batched launch "
                        "per kernel and RK stage, CUDA graph per step",
@@ -360,6 +360,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="curved", choices=["curved", "flat", "profile", "large", "ensemble"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--scenarios", type=int, default=64, help="scenarios of the ensemble configuration")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned Newton-guess comparison")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

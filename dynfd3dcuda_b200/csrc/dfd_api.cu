@@ -14,7 +14,7 @@
 
 namespace dfd {
 long long launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
-                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke);
+                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out);
 void launch_fault_node(const FaultArgs& a, cudaStream_t s);
 void launch_fault_band(const FaultArgs& a, cudaStream_t s);
 void launch_fault_coef(const Dims& d, const float* M, float* tab, float* tabf, float* vecn, float* vecs1,
@@ -89,8 +89,12 @@ struct dfd_ctx {
   int* tile_err = nullptr;
   int* tile_sched = nullptr;         // tiled kernel's unit counters
   bool use_tile = true;
+  // volume shell and fault band on s0 after the interior kernel (default), or on two
+  // further streams beside it (DFD_STREAMS=3)
+  bool serial = true;
   long long interior_nodes = 0;   // nodes the interior kernel updates per stage
   long long n_band_columns = 0;   // non-united (j, k) fault columns
+  std::vector<int> united_h;      // (NZ, NY) host copy of the united plane
   float interior_ms = 0;          // interior kernel time of the last dfd_run_timed
   float node_ms = 0;              // fault node kernel time of the last dfd_run_timed
   // host-side inputs
@@ -194,6 +198,10 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   d.sx = (long long)d.py * d.nz;
   d.nxyz = d.sx * d.nx;
   d.nyz = (long long)d.ny * d.nz;
+  // y-face PML state rows: the N nodes with the columns before them up to a 16-byte
+  // boundary; the y2 face starts at the boundary at or before its first node
+  d.wy = (d.N + 4 + 3) / 4 * 4;
+  d.yb3 = (d.nj - d.N + 3 + d.oy) / 4 * 4;
   auto done = [&](int rc) { if (rc) { dfd_destroy(ctx); return rc; } return 0; };
   if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s0, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
   if (done(cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->s1, cudaStreamNonBlocking), "stream"))) return DFD_ERR_CUDA;
@@ -214,11 +222,15 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
     if (!rc) rc = dalloc(ctx, &ctx->Ap[a], len[a]);
   }
   if (!rc && q.use_pml) {
-    long long sz[6] = {(long long)d.N * d.nj * d.nk, (long long)d.N * d.nj * d.nk, (long long)d.N * d.nk * d.ni,
-                       (long long)d.N * d.nk * d.ni, (long long)d.N * d.ni * d.nj, (long long)d.N * d.ni * d.nj};
+    // one block of 27 fields per face: value, RK accumulator, step-start copy
     for (int f = 0; f < 6 && !rc; f++) {
       if (f == 5 && q.free_surface) continue;
-      for (int r3 = 0; r3 < 3 && !rc; r3++) rc = dalloc(ctx, &ctx->aux[f][r3], 9 * sz[f]);
+      const long long fs = pml_fstride(d, f);
+      rc = dalloc(ctx, &ctx->aux[f][0], 27 * fs);
+      if (!rc) {
+        ctx->aux[f][2] = ctx->aux[f][0] + 9 * fs;   // accumulator
+        ctx->aux[f][1] = ctx->aux[f][0] + 18 * fs;  // step start
+      }
     }
   }
   if (!rc) rc = dalloc(ctx, &ctx->mVx2Vz, 9LL * d.nx * d.ny);
@@ -252,14 +264,17 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->tile_err, 1);
   if (!rc) rc = dalloc(ctx, &ctx->tile_sched, 2);
   if (rc) { dfd_destroy(ctx); return rc; }
-  // volume kernels: DFD_TILE=0 plain interior kernel + general shell kernel;
-  // 1 (default) TMA-tiled interior box + general shell kernel; 2 TMA tiles over every
-  // node below the free-surface rows; 3 TMA tiles over the interior box widened over the
-  // two x slabs of the PML
+  // volume kernels: DFD_TILE=0 plain interior kernel + general kernel on the PML slabs
+  // and free-surface rows; otherwise (default) the TMA-staged interior and PML kernels
+  // + the general kernel on the free-surface rows
   const char* tv = getenv("DFD_TILE");
-  int mode = tv && tv[0] >= '0' && tv[0] <= '3' ? tv[0] - '0' : 1;
-  ctx->use_tile = mode > 0 && tile_setup(&ctx->tile, d, ctx->W, ctx->mplane, ctx->tile_err, ctx->tile_sched, device);
-  ctx->tile.pml = mode == 2 ? 1 : mode == 3 ? 3 : 0;
+  const int mode = tv && tv[0] == '0' ? 0 : 1;
+  float* auxb[6];
+  for (int f = 0; f < 6; f++) auxb[f] = ctx->aux[f][0];
+  ctx->use_tile =
+      mode > 0 && tile_setup(&ctx->tile, d, ctx->W, ctx->mplane, auxb, ctx->tile_err, ctx->tile_sched, device);
+  const char* sv = getenv("DFD_STREAMS");
+  ctx->serial = !(sv && sv[0] == '3');
   *out = ctx;
   return DFD_OK;
 }
@@ -426,6 +441,7 @@ int dfd_precompute(dfd_ctx* ctx) {
         {I_UNITED, &h.united}, {I_FAULTGRID, &h.faultgrid}, {I_RUPY, &h.rupy}, {I_RUPZ, &h.rupz}};
     ctx->n_band_columns = 0;
     for (int v : h.united) ctx->n_band_columns += v == 0;
+    ctx->united_h = h.united;
     for (auto& u : iup)
       CK(cudaMemcpyAsync(ctx->ipl + u.plane * nf, u.v->data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s));
     for (int b = 0; b < 2; b++) CK(cudaMemsetAsync(ctx->FW[b], 0, sizeof(float) * 18 * d.nyz, s));
@@ -436,13 +452,8 @@ int dfd_precompute(dfd_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->hT1, 0, sizeof(float) * 3 * d.nyz, s));
   }
   for (int b = 0; b < 4; b++) CK(cudaMemsetAsync(ctx->W[b], 0, sizeof(float) * 9 * d.nxyz, s));
-  {
-    long long sz[6] = {(long long)d.N * d.nj * d.nk, (long long)d.N * d.nj * d.nk, (long long)d.N * d.nk * d.ni,
-                       (long long)d.N * d.nk * d.ni, (long long)d.N * d.ni * d.nj, (long long)d.N * d.ni * d.nj};
-    for (int f = 0; f < 6; f++)
-      for (int r3 = 0; r3 < 3; r3++)
-        if (ctx->aux[f][r3]) CK(cudaMemsetAsync(ctx->aux[f][r3], 0, sizeof(float) * 9 * sz[f], s));
-  }
+  for (int f = 0; f < 6; f++)
+    if (ctx->aux[f][0]) CK(cudaMemsetAsync(ctx->aux[f][0], 0, sizeof(float) * 27 * pml_fstride(d, f), s));
   CK(cudaMemsetAsync(ctx->newton, 0, 2 * sizeof(unsigned long long), s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
@@ -544,6 +555,21 @@ static VolArgs vol_args(dfd_ctx* ctx, int pattern, int irk) {
   return va;
 }
 
+// nodes the interior kernel updates in a stage: its box less the fault-band nodes in it
+static long long interior_nodes(const dfd_ctx* ctx, const VolPlan& pl) {
+  if (!(pl.tiled || pl.plain)) return 0;
+  long long n = pl.nodes;
+  const Dims& d = ctx->d;
+  if (ctx->p.rupture && !ctx->united_h.empty() && pl.lo.x + 3 <= d.i0 + 3 && pl.hi.x + 3 > d.i0 - 3) {
+    long long cols = 0;
+    for (int k = pl.lo.z; k < pl.hi.z; k++)
+      for (int j = pl.lo.y; j < pl.hi.y; j++) cols += ctx->united_h[(size_t)k * d.nj + j] == 0;
+    const int x0 = std::max(pl.lo.x + 3, d.i0 - 3), x1 = std::min(pl.hi.x + 3, d.i0 + 4);
+    n -= cols * std::max(0, x1 - x0);
+  }
+  return n;
+}
+
 static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr,
                          cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr, cudaEvent_t* nb = nullptr,
                          cudaEvent_t* ne = nullptr) {
@@ -558,9 +584,20 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
     launch_fault_node(fa, ctx->s0);
     if (ne) cudaEventRecord(*ne, ctx->s0);
   }
+  if (vb) cudaEventRecord(*vb, ctx->s0);
+  if (ctx->serial) {
+    // one stream: interior kernel, shell kernel, fault band
+    VolArgs va = vol_args(ctx, pattern, irk);
+    VolPlan pl;
+    launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s0, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke,
+                        &pl);
+    ctx->interior_nodes = interior_nodes(ctx, pl);
+    if (p.rupture) launch_fault_band(fa, ctx->s0);
+    if (ve) cudaEventRecord(*ve, ctx->s0);
+    return cuda_check(ctx, cudaGetLastError(), "stage launch");
+  }
   // fork: fault band on s1, volume shell on s2, volume interior on s0
   cudaEventRecord(ctx->ev_fork, ctx->s0);
-  if (vb) cudaEventRecord(*vb, ctx->s0);
   if (p.rupture) {
     cudaStreamWaitEvent(ctx->s1, ctx->ev_fork, 0);
     launch_fault_band(fa, ctx->s1);
@@ -568,9 +605,9 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   }
   cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
   VolArgs va = vol_args(ctx, pattern, irk);
-  long long nodes =
-      launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke);
-  ctx->interior_nodes = nodes - (p.rupture ? 7LL * ctx->n_band_columns : 0);
+  VolPlan pl;
+  launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke, &pl);
+  ctx->interior_nodes = interior_nodes(ctx, pl);
   cudaEventRecord(ctx->ev_join2, ctx->s2);
   if (p.rupture) cudaStreamWaitEvent(ctx->s0, ctx->ev_join, 0);
   cudaStreamWaitEvent(ctx->s0, ctx->ev_join2, 0);
@@ -1046,12 +1083,16 @@ struct EnsStage {
   int fblocks = 0;
   VolArgs* vol = nullptr;      // all scenarios
   Boxes* boxes = nullptr;
-  int* sstart = nullptr;       // (n + 1) block starts of the shell kernel
+  int* sstart = nullptr;       // (n + 1) block starts of the shell kernel, boxes below the top rows
   int sblocks = 0;
-  TileScen* tile = nullptr;    // all scenarios
+  int* tstart = nullptr;       // (n + 1) block starts of the shell kernel, free-surface rows
+  int tblocks = 0;
+  TileScen* tile = nullptr;    // all scenarios, interior kernel
   TileScen first;              // scenario 0, passed by value (stage-wide values)
   int nunits = 0;
-  bool pmlp = false;
+  TileScen* ptile = nullptr;   // all scenarios, PML kernel
+  TileScen pfirst;
+  int punits = 0;
   int FX = 1, FY = 1, FZ = 1;
 };
 
@@ -1118,36 +1159,51 @@ static int ens_build(dfd_ens* e) {
       S.fblocks = fs.back();
       std::vector<VolArgs> va;
       std::vector<Boxes> bx;
-      std::vector<int> ss(1, 0);
-      std::vector<TileScen> ts(n);
-      int units = 0;
+      std::vector<int> ss(1, 0), tt(1, 0);
+      std::vector<TileScen> ts(n), ps(n);
+      int units = 0, punits = 0;
       for (int i = 0; i < n; i++) {
         dfd_ctx* c = e->sc[i];
         VolArgs a = vol_args(c, pat, irk);
         VolPlan pl = plan_volume(a, c->use_tile ? &c->tile : nullptr);
-        if (!pl.tiled) return ens_fail(e, DFD_ERR_PARAM, "scenario " + std::to_string(i) + " cannot use the tiled kernel");
+        if (pl.plain || pl.ps.nunits < 0)
+          return ens_fail(e, DFD_ERR_PARAM, "scenario " + std::to_string(i) + " cannot use the tiled kernels");
         va.push_back(a);
         bx.push_back(pl.bx);
-        ss.push_back(ss.back() + pl.shell_blocks);
-        int grid = 0;
-        TileSched sch = tile_plan(pl.lo, pl.hi, e->nsm, &grid);
-        if (e->chunk > 0) {
-          sch.ci = std::min(e->chunk, pl.hi.x - pl.lo.x);
-          sch.nunits = sch.ntj * sch.ntk * ((pl.hi.x - pl.lo.x + sch.ci - 1) / sch.ci);
+        ss.push_back(ss.back() + pl.bx.start[pl.bx.ntop]);
+        tt.push_back(tt.back() + pl.bx.start[pl.bx.n] - pl.bx.start[pl.bx.ntop]);
+        TileSched sch;
+        memset(&sch, 0, sizeof sch);
+        if (pl.tiled) {
+          int grid = 0;
+          sch = tile_plan(pl.lo, pl.hi, e->nsm, &grid);
+          if (e->chunk > 0) {
+            sch.ci = std::min(e->chunk, pl.hi.x - pl.lo.x);
+            sch.nunits = sch.ntj * sch.ntk * ((pl.hi.x - pl.lo.x + sch.ci - 1) / sch.ci);
+          }
         }
         TileScen& t = ts[i];
         t.mp.win = c->tile.halo[bin[irk]];
         t.mp.w0 = c->tile.centre[0];
         t.mp.t = c->tile.centre[3];
         t.mp.plane = c->tile.plane;
-        t.a = a;
-        t.sc = sch;
-        t.unit0 = units;
+        for (int f = 0; f < 6; f++) t.mp.aux[f] = c->tile.aux[f];
+        t.u.a = a;
+        t.u.sc = sch;
+        t.u.unit0 = units;
         units += sch.nunits;
-        S.pmlp = S.pmlp || pl.pmlp;
+        TileScen& tp = ps[i];
+        tp.mp = t.mp;
+        tp.u.a = a;
+        tp.u.sc = pl.ps;
+        tp.u.unit0 = punits;
+        punits += pl.ps.nunits;
       }
       S.nunits = units;
+      S.punits = punits;
+      S.pfirst = ps[0];
       S.sblocks = ss.back();
+      S.tblocks = tt.back();
       S.first = ts[0];
       int r = 0;
       if (!e->rup.empty()) {
@@ -1157,7 +1213,9 @@ static int ens_build(dfd_ens* e) {
       r = r ? r : ens_upload(e, &S.vol, va);
       r = r ? r : ens_upload(e, &S.boxes, bx);
       r = r ? r : ens_upload(e, &S.sstart, ss);
+      r = r ? r : ens_upload(e, &S.tstart, tt);
       r = r ? r : ens_upload(e, &S.tile, ts);
+      r = r ? r : ens_upload(e, &S.ptile, ps);
       if (r) return r;
     }
   e->built = true;
@@ -1168,6 +1226,15 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
   const EnsStage& S = e->st[pat][irk];
   const int nr = (int)e->rup.size(), n = (int)e->sc.size();
   if (nr) launch_fault_node_batch(S.fault, S.fstart, nr, S.fblocks, S.FY, S.FZ, e->s0);
+  if (e->sc[0]->serial) {
+    launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
+    launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
+    launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, e->s0);
+    launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s0);
+    if (nr) launch_fault_band_batch(S.fault, S.fstart, nr, S.fblocks, S.FX, S.FY, S.FZ, e->s0);
+    cudaError_t ce = cudaGetLastError();
+    return ce == cudaSuccess ? DFD_OK : ens_fail(e, DFD_ERR_CUDA, std::string("ensemble stage: ") + cudaGetErrorString(ce));
+  }
   cudaEventRecord(e->ev_fork, e->s0);
   if (nr) {
     cudaStreamWaitEvent(e->s1, e->ev_fork, 0);
@@ -1175,9 +1242,11 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
     cudaEventRecord(e->ev_join, e->s1);
   }
   cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
-  launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, e->s2);
+  launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, e->s2);
+  launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s2);
   cudaEventRecord(e->ev_join2, e->s2);
-  launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, S.pmlp, e->err, e->sched, e->s0);
+  launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
+  launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
   if (nr) cudaStreamWaitEvent(e->s0, e->ev_join, 0);
   cudaStreamWaitEvent(e->s0, e->ev_join2, 0);
   cudaError_t ce = cudaGetLastError();

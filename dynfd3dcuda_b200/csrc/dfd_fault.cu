@@ -788,18 +788,26 @@ template <int FY, int FZ>
 __global__ void __launch_bounds__(128) fault_node_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
                                                         int n) {
   __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
+  __shared__ __align__(16) unsigned char raw[sizeof(FaultArgs)];
+  FaultArgs* sa = reinterpret_cast<FaultArgs*>(raw);
   int loc;
   const int sc = scenario_of(start, n, blockIdx.x, &loc);
-  const FaultArgs& a = tab[sc];
+  stage_args(sa, tab + sc);
+  __syncthreads();
+  const FaultArgs& a = *sa;
   const int gx = (a.d.nj + 31) / 32;
   fault_node_body<FY, FZ>(a, loc % gx, loc / gx, snet);
 }
 template <int FX, int FY, int FZ>
 __global__ void __launch_bounds__(128) fault_band_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
                                                         int n) {
+  __shared__ __align__(16) unsigned char raw[sizeof(FaultArgs)];
+  FaultArgs* sa = reinterpret_cast<FaultArgs*>(raw);
   int loc;
   const int sc = scenario_of(start, n, blockIdx.x, &loc);
-  const FaultArgs& a = tab[sc];
+  stage_args(sa, tab + sc);
+  __syncthreads();
+  const FaultArgs& a = *sa;
   const int gx = (a.d.nj + 31) / 32;
   fault_band_body<FX, FY, FZ>(a, loc % gx, loc / gx);
 }

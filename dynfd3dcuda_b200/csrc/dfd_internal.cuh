@@ -59,7 +59,34 @@ struct Dims {
   long long sx;         // volume x stride, py * nz
   long long nxyz;       // volume field size, sx * nx
   long long nyz;        // fault-plane size, ny * nz
+  int wy;               // row width of the y-face PML state (N + 4 rounded up to 4)
+  int yb3;              // first stored column of the y2-face PML state (a multiple of 4)
 };
+
+// ADE state of PML face f (x1 x2 y1 y2 z1 z2): one block of 27 fields per face, the
+// current value (fields 0..8), the RK accumulator (9..17) and the step-start copy
+// (18..26), each field pml_fstride apart.  The layouts keep the volume's row frame, so
+// that a 32 x 8 tile of nodes is one TMA box at a 16-byte aligned column:
+//   x faces: N planes of (nz rows, py columns), column j + 3 + oy, row k + 3;
+//   y faces: ni planes of (nz rows, wy columns), column j + 3 + oy - (0 | yb3), row k + 3;
+//   z faces: ni planes of (N rows, py columns), column j + 3 + oy, row k - (0 | nk - N).
+__host__ __device__ inline long long pml_fstride(const Dims& d, int f) {
+  if (f < 2) return (long long)d.N * d.sx;
+  if (f < 4) return (long long)d.ni * d.wy * d.nz;
+  return (long long)d.ni * d.py * d.N;
+}
+__host__ __device__ inline long long pml_index(const Dims& d, int f, int i, int j, int k) {
+  if (f < 2) {
+    int ia = f == 0 ? i : i - (d.ni - d.N);
+    return (long long)(j + 3 + d.oy) + (long long)(k + 3) * d.py + (long long)ia * d.sx;
+  }
+  if (f < 4) {
+    int c = j + 3 + d.oy - (f == 2 ? 0 : d.yb3);
+    return (long long)c + (long long)(k + 3) * d.wy + (long long)i * d.wy * d.nz;
+  }
+  int kz = f == 4 ? k : k - (d.nk - d.N);
+  return (long long)(j + 3 + d.oy) + (long long)kz * d.py + (long long)i * d.py * d.N;
+}
 
 // Arguments of the fused volume stage kernel.
 struct VolArgs {
@@ -158,51 +185,71 @@ struct GridArgs {
   double lam1, mu1, rho1, lam2, mu2, rho2;
 };
 
-// TMA tensor maps handed to the tiled interior kernel (dfd_tile.cu)
+// Tile of the TMA-staged kernels: 32 nodes along y (one warp) by 8 along z.
+constexpr int TILE_J = 32, TILE_K = 8;
+
+// TMA tensor maps handed to the tiled kernels (dfd_tile.cu, dfd_pml.cu)
 struct TileMaps {
   CUtensorMap win;  // stencil input, halo box
   CUtensorMap w0;   // step-start state, pointwise box
   CUtensorMap t;    // RK accumulator, pointwise box
   CUtensorMap plane;  // separable metric / media planes (12, nz, py)
+  CUtensorMap aux[6];  // PML state of each face (27 fields), pointwise box of 9 fields
 };
-// Per-context state of the tiled interior kernel: maps of the four volume buffers and of
-// the metric (fixed addresses, encoded once), the error flag, the SM count.
+// Per-context state of the tiled kernels: maps of the four volume buffers, of the metric
+// and of the PML state (fixed addresses, encoded once), the error flag, the SM count.
 struct TileCtx {
   CUtensorMap halo[4];
   CUtensorMap centre[4];
   CUtensorMap plane;
+  CUtensorMap aux[6];
   int* err = nullptr;
   int* sched = nullptr;  // unit counter and finished-CTA counter (zero between launches)
   int nsm = 0;
-  int pml = 0;  // 1: the tiles cover every PML slab; 3: the two x slabs only
   bool ok = false;
 };
-bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, int* err, int* sched,
-                int device);
-// Units of the tiled kernel over a box: tile columns (32 y x 8 z) times chunks of x planes.
+bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, float* const aux[6], int* err,
+                int* sched, int device);
+// Units of a tiled kernel: tile columns (32 y x 8 z) times chunks of x planes.
+//   interior kernel: the tiles of the box lo..hi;
+//   PML kernel: over the nodes below the free-surface rows (k < ktop) outside the
+//   interior kernel's tile rectangle [tja, tjb) x [tka, tkb) (tile indices of the frame
+//   starting at j = 0, k = 0): every tile of the x slabs [0, nx1) and [ni - nx2, ni), then
+//   in chunks of ci planes over [nx1, ni - nx2) the nedge tiles outside the rectangle.
 struct TileSched {
   int lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;  // tiled box, interior indices, half open
   int ntj, ntk, ci, nunits;               // tiles in y and z, planes per chunk, units
+  int tja, tjb, tka, tkb;                 // PML kernel: the interior kernel's tile rectangle
+  int nx1, nx2, ktop, nedge;              // PML kernel: x slab widths, top row bound, edge tiles
 };
-// One scenario of a batched (ensemble) launch of the tiled kernel, in device memory.
-struct alignas(64) TileScen {
-  TileMaps mp;
+// Values of one scenario of a batched (ensemble) launch of the tiled kernel that the
+// computing warps read; a CTA copies them into shared memory with each unit's planes.
+struct alignas(16) TileUnit {
   VolArgs a;
   TileSched sc;
   int unit0;  // first global unit of the scenario
 };
-// Boxes of the general (shell) kernel: up to eight, each flattened or tiled.
+// One scenario of a batched launch of the tiled kernel, in device memory.
+struct alignas(64) TileScen {
+  TileMaps mp;
+  TileUnit u;
+};
+// Boxes of the general (shell) kernels: up to eight, each flattened or tiled.  Boxes
+// [0, ntop) lie below the free-surface rows (PML slabs, alignment columns) and go to the
+// kernel without the free-surface terms; boxes [ntop, n) hold the free-surface rows.
 struct Boxes {
-  int n;
+  int n, ntop;
   int lo[8][3], hi[8][3];  // (i, j, k) interior-index bounds, half open
   int thin[8];             // flattened (y, z) mapping
   int start[9];            // first block of each box
 };
 // Volume work of one stage of one scenario: the box of the tiled (or plain) interior
-// kernel and the general kernel's boxes.
+// kernel, the units of the tiled PML kernel and the general kernel's boxes.
 struct VolPlan {
-  bool tiled, pmlp, plain;
+  bool tiled, plain;
   int3 lo, hi;        // interior-kernel box
+  TileSched ps;       // PML kernel units (tiled plans; ps.nunits 0: none)
+  int pgrid;          // PML kernel CTAs
   Boxes bx;
   int shell_blocks;
   long long nodes;    // nodes of the interior-kernel box
@@ -210,17 +257,38 @@ struct VolPlan {
 VolPlan plan_volume(const VolArgs& a, const TileCtx* tc);
 bool tile_feasible(const TileCtx* tc, const VolArgs& a, int3 lo, int3 hi);
 TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid);
+// units of the PML kernel around the interior tile rectangle (dfd_pml.cu)
+TileSched pml_plan(const VolArgs& a, int tja, int tjb, int tka, int tkb, int ktop, int nsm, int* grid);
+bool pml_setup();
+void launch_pml(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, const TileSched& ps, int grid,
+                cudaStream_t s);
+void launch_pml_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY, int FZ,
+                      int* err, int* sched, cudaStream_t s);
 // batched launches (dfd_volume.cu, dfd_tile.cu, dfd_fault.cu)
 void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,
-                       int FZ, bool pmlp, int* err, int* sched, cudaStream_t s);
+                       int FZ, int* err, int* sched, cudaStream_t s);
+// top: the free-surface boxes (start: per-scenario block starts of those), else the others
 void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, int FX, int FY,
-                        int FZ, cudaStream_t s);
+                        int FZ, bool top, cudaStream_t s);
 void launch_fault_node_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FY, int FZ,
                              cudaStream_t s);
 void launch_fault_band_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FX, int FY, int FZ,
                              cudaStream_t s);
 
 // scenario owning block b of a batched launch: start[s] <= b < start[s + 1]
+// Copy one scenario's argument struct of an ensemble table into shared memory, all
+// threads of the block taking part (a __syncthreads must follow): the batched kernels
+// then read their arguments from shared memory instead of global memory.
+template <class T>
+__device__ __forceinline__ void stage_args(T* dst, const T* src) {
+  static_assert(sizeof(T) % 4 == 0, "argument struct size");
+  const int* s = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(dst);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  for (int w = t; w < (int)(sizeof(T) / 4); w += nt) d[w] = __ldg(s + w);
+}
+
 __device__ __forceinline__ int scenario_of(const int* start, int n, int b, int* local) {
   int lo = 0, hi = n;
   while (hi - lo > 1) {
@@ -231,8 +299,7 @@ __device__ __forceinline__ int scenario_of(const int* start, int n, int b, int* 
   return lo;
 }
 
-// pmlp: the box contains PML nodes (the kernel variant with the PML path)
-bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi, bool pmlp,
+bool launch_tile(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, int3 lo, int3 hi,
                  cudaStream_t s);
 
 __host__ __device__ inline long long idx3(const Dims& d, int i, int j, int k) {

@@ -1,0 +1,567 @@
+// Nodes of the volume stage below the free-surface rows that the interior kernel does
+// not take, staged through shared memory by TMA: the PML slabs of all six faces and the
+// nodes that fill their tiles (the interior kernel takes whole tiles only).
+//
+// The tiles are those of the interior kernel (32 y x 8 z, frame starting at j = 0,
+// k = 0).  Units (dfd_internal.cuh, TileSched): every tile of the two x slabs, one unit
+// per slab; then, in chunks of x planes between the slabs, the tiles outside the interior
+// kernel's rectangle.  Each unit stages, per plane, the stencil input with its halo, the
+// RK registers and the ADE state of one PML face (its "own" face: x for the x slabs, else
+// y, else z); a node that also lies in another face (edges and corners of the slabs)
+// reads that face's state from global memory.  One computing warp per row of nodes
+// integrates all nine fields and their PML state.
+//
+// Right-hand side with the ADE CFS-PML as in the reference's wave.cu:8-204 and
+// pmlx.cu:8-214 / pmly.cu / pmlz.cu, the RK4 registers as rk4.cu:20-33 and 154-257.
+#include <algorithm>
+#include <cstring>
+
+#include "dfd_tma.cuh"
+
+namespace dfd {
+
+namespace {
+constexpr int PSLOT_M = 45 * PB;  // W0 9, T 9, then the face's ADE state: value 9, accumulator 9, step start 9
+constexpr int MS = 6, MP = 2, MQ = 2;  // ring depths (stencil planes, pointwise planes, unit planes)
+constexpr int PCW = TK;                 // computing warps: one per row of the tile, all nine fields
+constexpr int PTOT = PCW * 32 + 32;     // plus one copy-issuing warp
+constexpr size_t PML_SMEM =
+    (size_t)(MS * HSLOT + MP * PSLOT_M + MQ * QSLOT) * 4 + MQ * sizeof(TileUnit) + 2 * (MS + MP + MQ) * 8 + MQ * 4;
+static_assert(PML_SMEM <= 232448, "PML ring exceeds the shared memory of one CTA");
+static_assert((PSLOT_M * 4) % 128 == 0, "slot alignment");
+}  // namespace
+
+// tile origin, x range and own face (-1: none) of local unit lu
+struct PmlUnit {
+  int j0, k0, ib, ie, face;
+};
+__device__ __forceinline__ PmlUnit pml_unit(const TileSched& sc, const VolArgs& a, int lu) {
+  const Dims& d = a.d;
+  PmlUnit r;
+  const int ntile = sc.ntj * sc.ntk;
+  int tj, tk;
+  if (sc.nx1 > 0 && lu < ntile) {
+    tj = lu % sc.ntj; tk = lu / sc.ntj;
+    r.ib = 0; r.ie = sc.nx1; r.face = 0;
+  } else {
+    if (sc.nx1 > 0) lu -= ntile;
+    if (sc.nx2 > 0 && lu < ntile) {
+      tj = lu % sc.ntj; tk = lu / sc.ntj;
+      r.ib = d.ni - sc.nx2; r.ie = d.ni; r.face = 1;
+    } else {
+      if (sc.nx2 > 0) lu -= ntile;
+      const int c = lu / sc.nedge, e = lu % sc.nedge;
+      r.ib = sc.nx1 + c * sc.ci;
+      r.ie = min(r.ib + sc.ci, d.ni - sc.nx2);
+      // edge tile e: the full rows below the rectangle, the two sides of it, the full rows above
+      const int below = sc.tka * sc.ntj, side = sc.tja + (sc.ntj - sc.tjb), mid = (sc.tkb - sc.tka) * side;
+      if (e < below) {
+        tk = e / sc.ntj; tj = e % sc.ntj;
+      } else if (e < below + mid) {
+        const int m = e - below, rr = m % side;
+        tk = sc.tka + m / side;
+        tj = rr < sc.tja ? rr : sc.tjb + (rr - sc.tja);
+      } else {
+        const int m = e - below - mid;
+        tk = sc.tkb + m / sc.ntj; tj = m % sc.ntj;
+      }
+      const int j0 = tj * TJ, k0 = tk * TK;
+      r.face = (a.aux[2] && j0 < d.N) ? 2
+               : (a.aux[3] && j0 + TJ > d.nj - d.N) ? 3
+               : (a.aux[4] && k0 < d.N) ? 4
+               : (a.aux[5] && k0 + TK > d.nk - d.N) ? 5
+               : -1;
+    }
+  }
+  r.j0 = tj * TJ;
+  r.k0 = tk * TK;
+  return r;
+}
+
+// ADE update of face `face` for fields F0..F0+2 at this node (pml_update of
+// dfd_stencil.cuh, restricted to three fields): accumulates -aux/beta into p and advances
+// the state in place with the RK4 registers.  The state comes from shared memory (A, the
+// staged own face) or from global memory; every load precedes the stores, which may alias
+// them as far as the compiler knows.
+template <int F0, int AX>
+__device__ __forceinline__ void role_face(const VolArgs& a, int face, bool staged, const float* A, int i, int j,
+                                          int k, float rb, float dd, float al, const float* D, float* p) {
+  const Dims& d = a.d;
+  // face is 2 AX or 2 AX + 1: the layout branch of pml_index is known here
+  const long long fs = pml_fstride(d, 2 * AX);
+  long long qa;
+  if (AX == 0) {
+    const int ia = face == 0 ? i : i - (d.ni - d.N);
+    qa = (long long)(j + 3 + d.oy) + (long long)(k + 3) * d.py + (long long)ia * d.sx;
+  } else if (AX == 1) {
+    const int c = j + 3 + d.oy - (face == 2 ? 0 : d.yb3);
+    qa = (long long)c + (long long)(k + 3) * d.wy + (long long)i * d.wy * d.nz;
+  } else {
+    const int kz = face == 4 ? k : k - (d.nk - d.N);
+    qa = (long long)(j + 3 + d.oy) + (long long)kz * d.py + (long long)i * d.py * d.N;
+  }
+  float* base = a.aux[face];
+  const int irk = a.irk;
+  const float ad = -(al + dd);
+  float w[3], t[3], w0[3];
+#pragma unroll
+  for (int m = 0; m < 3; m++) {
+    const int f = F0 + m;
+    if (staged) {
+      w[m] = A[f * PB];
+      if (irk >= 1) t[m] = A[(9 + f) * PB];
+      if (irk == 1 || irk == 2) w0[m] = A[(18 + f) * PB];
+    } else {
+      const long long x = f * fs + qa;
+      w[m] = base[x];
+      if (irk >= 1) t[m] = base[x + 9 * fs];
+      if (irk == 1 || irk == 2) w0[m] = base[x + 18 * fs];
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 3; m++) {
+    const long long x = (F0 + m) * fs + qa;
+    p[m] += -w[m] * rb;
+    const float h = ad * w[m] + dd * D[m];
+    if (irk == 0) {
+      base[x + 18 * fs] = w[m];
+      base[x + 9 * fs] = fmaf(a.rkb, h, w[m]);
+      base[x] = fmaf(a.rka, h, w[m]);
+    } else if (irk < 3) {
+      base[x + 9 * fs] = fmaf(a.rkb, h, t[m]);
+      base[x] = fmaf(a.rka, h, w0[m]);
+    } else {
+      base[x] = fmaf(a.rkb, h, t[m]);
+    }
+  }
+}
+
+// axis contribution (axis_terms of dfd_stencil.cuh) to fields F0..F0+2 from the
+// derivatives dv[] along one axis (metric row e0 e1 e2; X0: the row has an x component --
+// the y and z rows of the separable metric have none).  F0 = 0: dv = d(Txx Tyy Tzz Txy Txz
+// Tyz); F0 = 3 (normal stresses) or 6 (shear stresses): dv = d(Vx Vy Vz).
+template <int F0, bool X0>
+__device__ __forceinline__ void role_terms(const float* dv, float e0, float e1, float e2, float lam, float mu,
+                                           float rr, float* D) {
+  if (F0 == 0) {
+    if (X0) {
+      D[0] = (dv[0] * e0 + dv[3] * e1 + dv[4] * e2) * rr;
+      D[1] = (dv[3] * e0 + dv[1] * e1 + dv[5] * e2) * rr;
+      D[2] = (dv[4] * e0 + dv[5] * e1 + dv[2] * e2) * rr;
+    } else {
+      D[0] = (dv[3] * e1 + dv[4] * e2) * rr;
+      D[1] = (dv[1] * e1 + dv[5] * e2) * rr;
+      D[2] = (dv[5] * e1 + dv[2] * e2) * rr;
+    }
+  } else if (F0 == 3) {
+    const float l2m = lam + 2.0f * mu;
+    if (X0) {
+      D[0] = dv[0] * e0 * l2m + dv[1] * e1 * lam + dv[2] * e2 * lam;
+      D[1] = dv[0] * e0 * lam + dv[1] * e1 * l2m + dv[2] * e2 * lam;
+      D[2] = dv[0] * e0 * lam + dv[1] * e1 * lam + dv[2] * e2 * l2m;
+    } else {
+      D[0] = dv[1] * e1 * lam + dv[2] * e2 * lam;
+      D[1] = dv[1] * e1 * l2m + dv[2] * e2 * lam;
+      D[2] = dv[1] * e1 * lam + dv[2] * e2 * l2m;
+    }
+  } else {
+    if (X0) {
+      D[0] = (dv[0] * e1 + dv[1] * e0) * mu;
+      D[1] = (dv[0] * e2 + dv[2] * e0) * mu;
+      D[2] = (dv[1] * e2 + dv[2] * e1) * mu;
+    } else {
+      D[0] = (dv[0] * e1) * mu;
+      D[1] = (dv[0] * e2) * mu;
+      D[2] = (dv[1] * e2 + dv[2] * e1) * mu;
+    }
+  }
+}
+
+// One node, all nine fields: the three axes with their 1/beta, the ADE state of the faces
+// the node lies in (fx, fy, fz; -1: none; own: the staged face, read from A), the RK4
+// store.  g: separable metric (xi = (1, U, V)/a(x), eta = (0, ety, etz), zeta = (0, zty,
+// ztz)) and media.
+template <int FX, int FY, int FZ>
+__device__ __forceinline__ void pml_node(const VolArgs& a, const float* x0, const float* x1, const float* x2,
+                                         const float* x3, const float* x4, const float* cur, const NodeMetric& g,
+                                         int i, int j, int k, int fx, int fy, int fz, int own, const float* A,
+                                         long long q, const float* P, float damp) {
+  const float r = a.rDH;
+  float hv[9], p[9], D[9], dv[9];
+#pragma unroll
+  for (int f = 0; f < 9; f++) p[f] = 0.0f;
+  // x
+  {
+#pragma unroll
+    for (int f = 0; f < 9; f++) {
+      const int o = f * HBOX;
+      dv[f] = d5v<FX>(x0[o], x1[o], x2[o], x3[o], x4[o]) * r;
+    }
+    role_terms<0, true>(dv + 3, g.ex0, g.ex1, g.ex2, g.lam, g.mu, g.rrho, D);
+    role_terms<3, true>(dv, g.ex0, g.ex1, g.ex2, g.lam, g.mu, g.rrho, D + 3);
+    role_terms<6, true>(dv, g.ex0, g.ex1, g.ex2, g.lam, g.mu, g.rrho, D + 6);
+    const float rb = __ldg(a.rBx + i);
+#pragma unroll
+    for (int f = 0; f < 9; f++) hv[f] = D[f] * rb;
+    if (fx >= 0) {
+      const bool st = fx == own;
+      const float dd = __ldg(a.Dpx + i), al = __ldg(a.Apx + i);
+      role_face<0, 0>(a, fx, st, A, i, j, k, rb, dd, al, D, p);
+      role_face<3, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 3, p + 3);
+      role_face<6, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 6, p + 6);
+    }
+  }
+  // y
+  {
+#pragma unroll
+    for (int f = 0; f < 9; f++) dv[f] = d5s<FY, 1>(cur + f * HBOX) * r;
+    role_terms<0, false>(dv + 3, 0.0f, g.ey1, g.ey2, g.lam, g.mu, g.rrho, D);
+    role_terms<3, false>(dv, 0.0f, g.ey1, g.ey2, g.lam, g.mu, g.rrho, D + 3);
+    role_terms<6, false>(dv, 0.0f, g.ey1, g.ey2, g.lam, g.mu, g.rrho, D + 6);
+    const float rb = __ldg(a.rBy + j);
+#pragma unroll
+    for (int f = 0; f < 9; f++) hv[f] += D[f] * rb;
+    if (fy >= 0) {
+      const bool st = fy == own;
+      const float dd = __ldg(a.Dpy + j), al = __ldg(a.Apy + j);
+      role_face<0, 1>(a, fy, st, A, i, j, k, rb, dd, al, D, p);
+      role_face<3, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 3, p + 3);
+      role_face<6, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 6, p + 6);
+    }
+  }
+  // z
+  {
+#pragma unroll
+    for (int f = 0; f < 9; f++) dv[f] = d5s<FZ, HW>(cur + f * HBOX) * r;
+    role_terms<0, false>(dv + 3, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D);
+    role_terms<3, false>(dv, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D + 3);
+    role_terms<6, false>(dv, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D + 6);
+    const float rb = __ldg(a.rBz + k);
+#pragma unroll
+    for (int f = 0; f < 9; f++) hv[f] += D[f] * rb;
+    if (fz >= 0) {
+      const bool st = fz == own;
+      const float dd = __ldg(a.Dpz + k), al = __ldg(a.Apz + k);
+      role_face<0, 2>(a, fz, st, A, i, j, k, rb, dd, al, D, p);
+      role_face<3, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 3, p + 3);
+      role_face<6, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 6, p + 6);
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 9; f++) hv[f] += p[f];
+  rk_tile_store<0, 9>(a, a.d.nxyz, q, cur, P, hv, damp);
+}
+
+// Warp PCW issues the copies; warps 0..PCW-1 compute, one per row of nodes, all nine
+// fields (the lean interior path for a warp whose nodes lie in no PML slab).  The nine warps
+// allow 168 registers a thread (three warps on one of the SM's four 16 K-register
+// partitions), what the ADE path needs without spilling.  Rings as in the interior
+// kernel, with shallower stencil and pointwise rings: a pointwise slot also holds the own
+// face's ADE state, so it is 2.5 times larger.
+// BATCH: the units of the nscen scenarios of tab in one launch; mp0, a0, sc0 describe
+// scenario 0 and give the stage's common values.
+template <int FX, int FY, int FZ, bool BATCH>
+__global__ void __maxnreg__(168)
+    volume_pml_kernel(const __grid_constant__ TileMaps mp0, const __grid_constant__ VolArgs a0,
+                      const __grid_constant__ TileSched sc0, const TileScen* __restrict__ tab, int nscen, int nunits,
+                      int* err, int* sched) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  float* win = reinterpret_cast<float*>(smraw);
+  float* pw = win + MS * HSLOT;
+  float* qs = pw + MP * PSLOT_M;
+  TileUnit* uarg = reinterpret_cast<TileUnit*>(qs + MQ * QSLOT);
+  uint64_t* full_w = reinterpret_cast<uint64_t*>(uarg + MQ);
+  uint64_t* empty_w = full_w + MS;
+  uint64_t* full_p = empty_w + MS;
+  uint64_t* empty_p = full_p + MP;
+  uint64_t* full_q = empty_p + MP;
+  uint64_t* empty_q = full_q + MQ;
+  int* qunit = reinterpret_cast<int*>(empty_q + MQ);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int XLO = FX == 1 ? -1 : -3;
+  constexpr int RZ = FZ == 1 ? 1 : 3;
+  const int irk = a0.irk;
+  const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1;
+  const int naux = irk == 0 ? 9 : irk == 3 ? 18 : 27;  // ADE fields staged per plane
+  const int G = gridDim.x;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < MS; s++) { mbar_init(full_w + s, 1); mbar_init(empty_w + s, PCW); }
+    for (int s = 0; s < MP; s++) { mbar_init(full_p + s, 1); mbar_init(empty_p + s, PCW); }
+    for (int s = 0; s < MQ; s++) { mbar_init(full_q + s, 1); mbar_init(empty_q + s, PCW); }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_async_shared();
+  }
+  __syncthreads();
+
+  if (warp == PCW) {
+    // ---------------- copy-issuing warp (one lane)
+    if (lane != 0) return;
+    Ring wr, pr, qr;
+    int wcount = 0, pcount = 0, qcount = 0;
+    bool ok = true;
+    while (ok) {
+      const int u = atomicAdd(sched, 1);
+      if (qcount >= MQ && !(ok = mbar_wait(empty_q + qr.slot, qr.phase ^ 1))) break;
+      if (u >= nunits) {
+        qunit[qr.slot] = -1;
+        mbar_arrive(full_q + qr.slot);
+        break;
+      }
+      const int scn = BATCH ? tile_scenario(tab, nscen, u) : 0;
+      const TileMaps& mp = BATCH ? tab[scn].mp : mp0;
+      const VolArgs& a = BATCH ? tab[scn].u.a : a0;
+      const TileSched& sc = BATCH ? tab[scn].u.sc : sc0;
+      const Dims& d = a.d;
+      const PmlUnit pu = pml_unit(sc, a, BATCH ? u - tab[scn].u.unit0 : u);
+      const int cw0 = pu.j0 + 3 + d.oy - 4, cw1 = pu.k0 + 3 - RZ, cp0 = pu.j0 + 3 + d.oy, cp1 = pu.k0 + 3;
+      const int nst = pu.ie - pu.ib;
+      const int na = pu.face >= 0 ? naux : 0;
+      const bool usep = needW0 || needT || na > 0;
+      const unsigned ptx = ((needW0 ? 9 : 0) + (needT ? 9 : 0) + na) * PB * 4;
+      // own-face state coordinates: column, row, plane offset
+      int ac0 = cp0, ac1 = cp1, aoff = 0;
+      if (pu.face == 1) aoff = d.ni - d.N;
+      if (pu.face == 3) ac0 = cp0 - d.yb3;
+      if (pu.face == 4) ac1 = pu.k0;
+      if (pu.face == 5) ac1 = pu.k0 - (d.nk - d.N);
+      qunit[qr.slot] = u;
+      if (BATCH) {
+        mbar_expect_tx(full_q + qr.slot, QSLOT * 4 + (unsigned)sizeof(TileUnit));
+        bulk_load(uarg + qr.slot, &tab[scn].u, (unsigned)sizeof(TileUnit), full_q + qr.slot);
+      } else {
+        mbar_expect_tx(full_q + qr.slot, QSLOT * 4);
+      }
+      tma_load3(qs + qr.slot * QSLOT, &mp.plane, cp0, cp1, 0, full_q + qr.slot);
+      qr.next<MQ>();
+      qcount++;
+      for (int m = 0; m < nst + 4 && ok; m++) {
+        if (wcount >= MS && !(ok = mbar_wait(empty_w + wr.slot, wr.phase ^ 1))) break;
+        mbar_expect_tx(full_w + wr.slot, HSLOT * 4);
+        tma_load4(win + wr.slot * HSLOT, &mp.win, cw0, cw1, pu.ib + XLO + m + 3, 0, full_w + wr.slot);
+        wr.next<MS>();
+        wcount++;
+        if (m < 4 || !usep) continue;
+        if (pcount >= MP && !(ok = mbar_wait(empty_p + pr.slot, pr.phase ^ 1))) break;
+        uint64_t* b = full_p + pr.slot;
+        float* dst = pw + pr.slot * PSLOT_M;
+        const int i = pu.ib + (m - 4);
+        mbar_expect_tx(b, ptx);
+        if (needW0) tma_load4(dst, &mp.w0, cp0, cp1, i + 3, 0, b);
+        if (needT) tma_load4(dst + 9 * PB, &mp.t, cp0, cp1, i + 3, 0, b);
+        for (int fb = 0; fb < na; fb += 9) tma_load4(dst + (18 + fb) * PB, &mp.aux[pu.face], ac0, ac1, i - aoff, fb, b);
+        pr.next<MP>();
+        pcount++;
+      }
+    }
+    if (!ok) {
+      atomicExch(err, 1);
+      for (int c = max(0, wcount - MS); c < wcount; c++) mbar_wait(full_w + c % MS, (c / MS) & 1);
+      for (int c = max(0, pcount - MP); c < pcount; c++) mbar_wait(full_p + c % MP, (c / MP) & 1);
+      for (int c = max(0, qcount - MQ); c < qcount; c++) mbar_wait(full_q + c % MQ, (c / MQ) & 1);
+    }
+    __threadfence();
+    if (atomicAdd(sched + 1, 1) == G - 1) {
+      atomicExch(sched, 0);
+      atomicExch(sched + 1, 0);
+    }
+    return;
+  }
+
+  // ---------------- computing warps
+  const int ty = warp;
+  const int hc = (ty + RZ) * HW + lane + 4;
+  const int pc = ty * TJ + lane;
+  Ring wr, pr, qr;
+  int sb = 0;
+  for (;;) {
+    if (!__all_sync(0xffffffffu, mbar_wait(full_q + qr.slot, qr.phase))) {
+      if (lane == 0) atomicExch(err, 1);
+      return;
+    }
+    const int u = qunit[qr.slot];
+    if (u < 0) break;
+    const TileUnit& ua = uarg[qr.slot];
+    const VolArgs& a = BATCH ? ua.a : a0;
+    const TileSched& sc = BATCH ? ua.sc : sc0;
+    const Dims& d = a.d;
+    const PmlUnit pu = pml_unit(sc, a, BATCH ? u - ua.unit0 : u);
+    const int j = pu.j0 + lane, k = pu.k0 + ty;
+    const bool active = j < d.nj && k < sc.ktop;
+    const bool band = active && a.united && !a.united[j + k * d.nj];
+    const int fy = (a.aux[2] && j < d.N) ? 2 : (a.aux[3] && j >= d.nj - d.N) ? 3 : -1;
+    const int fz = (a.aux[4] && k < d.N) ? 4 : (a.aux[5] && k >= d.nk - d.N) ? 5 : -1;
+    float dyz = 1.0f;
+    if (active && a.dampx) dyz = fminf(__ldg(a.dampy + j + 3), __ldg(a.dampz + k + 3));
+    const long long qyz = idx3(d, 0, j + 3, k + 3);
+    const int nst = pu.ie - pu.ib;
+    const bool usep = needW0 || needT || pu.face >= 0;
+    const float* Q = qs + qr.slot * QSLOT + pc;
+    for (int s = 0; s < nst; s++) {
+      bool ok = true;
+      for (int c = s == 0 ? 5 : 1; c > 0; c--) {
+        ok = ok && mbar_wait(full_w + wr.slot, wr.phase);
+        wr.next<MS>();
+      }
+      if (usep) ok = ok && mbar_wait(full_p + pr.slot, pr.phase);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicExch(err, 1);
+        return;
+      }
+      const int i = pu.ib + s;
+      const float* P = pw + pr.slot * PSLOT_M + pc;
+      const bool node = active && !(band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3);
+      const int fx = (a.aux[0] && i < d.N) ? 0 : (a.aux[1] && i >= d.ni - d.N) ? 1 : -1;
+      // a warp none of whose nodes lies in a PML slab in this plane takes the lean path
+      const bool pml = __any_sync(0xffffffffu, node && (fx >= 0 || fy >= 0 || fz >= 0));
+      if (node) {
+        const int s1 = sb + 1 == MS ? 0 : sb + 1;
+        const int s2 = s1 + 1 == MS ? 0 : s1 + 1;
+        const int s3 = s2 + 1 == MS ? 0 : s2 + 1;
+        const int s4 = s3 + 1 == MS ? 0 : s3 + 1;
+        const float* x0 = win + sb * HSLOT + hc;
+        const float* x1 = win + s1 * HSLOT + hc;
+        const float* x2 = win + s2 * HSLOT + hc;
+        const float* x3 = win + s3 * HSLOT + hc;
+        const float* x4 = win + s4 * HSLOT + hc;
+        const float* cur = FX == 1 ? x1 : x3;
+        NodeMetric g;
+        const float rA = __ldg(a.rxa + i + 3);
+        g.ex0 = rA; g.ex1 = Q[0] * rA; g.ex2 = Q[PB] * rA;
+        g.ey1 = Q[2 * PB]; g.ey2 = Q[3 * PB]; g.ez1 = Q[4 * PB]; g.ez2 = Q[5 * PB];
+        const int side = i + 3 < a.nxhalf ? 6 : 9;
+        g.lam = Q[side * PB]; g.mu = Q[(side + 1) * PB]; g.rrho = 1.0f / Q[(side + 2) * PB];
+        const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
+        const long long q = qyz + (long long)(i + 3) * d.sx;
+        if (pml) {
+          pml_node<FX, FY, FZ>(a, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face, P + 18 * PB, q, P, damp);
+        } else {
+          float hv[9];
+          lean_velocity<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);
+          lean_stress<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);
+          rk_tile_store<0, 9>(a, d.nxyz, q, cur, P, hv, damp);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        if (s + 1 < nst) {
+          mbar_arrive(empty_w + sb);
+        } else {
+          for (int m = 0, sl = sb; m < 5; m++, sl = sl + 1 == MS ? 0 : sl + 1) mbar_arrive(empty_w + sl);
+          mbar_arrive(empty_q + qr.slot);
+        }
+        if (usep) mbar_arrive(empty_p + pr.slot);
+      }
+      if (usep) pr.next<MP>();
+      sb += s + 1 < nst ? 1 : 5;
+      if (sb >= MS) sb -= MS;
+    }
+    qr.next<MQ>();
+  }
+}
+
+// ---------------- host side
+
+template <int FX, int FY, int FZ>
+static bool pml_smem() {
+  auto one = [](const void* f) {
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PML_SMEM) == cudaSuccess;
+  };
+  return one((const void*)volume_pml_kernel<FX, FY, FZ, false>) &&
+         one((const void*)volume_pml_kernel<FX, FY, FZ, true>);
+}
+
+bool pml_setup() {
+  return pml_smem<-1, -1, -1>() && pml_smem<-1, -1, 1>() && pml_smem<-1, 1, -1>() && pml_smem<-1, 1, 1>() &&
+         pml_smem<1, -1, -1>() && pml_smem<1, -1, 1>() && pml_smem<1, 1, -1>() && pml_smem<1, 1, 1>();
+}
+
+// Units around the interior tile rectangle [tja, tjb) x [tka, tkb) (empty: tja == tjb):
+// the x slabs whole, the middle x range in chunks chosen as in tile_plan.  nunits 0 when
+// there is nothing to do, -1 when the slabs overlap (the general kernel then takes all).
+TileSched pml_plan(const VolArgs& a, int tja, int tjb, int tka, int tkb, int ktop, int nsm, int* grid) {
+  const Dims& d = a.d;
+  TileSched s;
+  memset(&s, 0, sizeof s);
+  s.ntj = (d.nj + TJ - 1) / TJ;
+  s.ntk = (ktop + TK - 1) / TK;
+  s.tja = tja; s.tjb = tjb; s.tka = tka; s.tkb = tkb;
+  s.nx1 = a.aux[0] ? d.N : 0;
+  s.nx2 = a.aux[1] ? d.N : 0;
+  s.ktop = ktop;
+  *grid = 0;
+  if (s.nx1 + s.nx2 > d.ni || ktop <= 0) {
+    s.nunits = -1;
+    return s;
+  }
+  const int ntile = s.ntj * s.ntk;
+  s.nedge = ntile - (tjb - tja) * (tkb - tka);
+  const int slab = (s.nx1 > 0 ? ntile : 0) + (s.nx2 > 0 ? ntile : 0);
+  const int nxm = d.ni - s.nx1 - s.nx2;
+  s.ci = std::max(nxm, 1);
+  s.nunits = slab;
+  if (nxm > 0 && s.nedge > 0) {
+    long long best = -1;
+    for (int nch = 1; nch <= 64 && nch <= nxm; nch++) {
+      int ci = (nxm + nch - 1) / nch;
+      int nchr = (nxm + ci - 1) / ci;
+      long long units = (long long)s.nedge * nchr + slab;
+      long long g = std::min<long long>(units, nsm);
+      long long cost = (units + g - 1) / g * (ci + 4);
+      if (best < 0 || cost < best) { best = cost; s.ci = ci; s.nunits = (int)units; }
+    }
+  }
+  *grid = std::min(s.nunits, nsm);
+  return s;
+}
+
+template <int FX, int FY, int FZ>
+static void launch_p(const TileCtx& tc, const VolArgs& a, int bin, const TileSched& ps, int grid, cudaStream_t s) {
+  TileMaps mp;
+  mp.win = tc.halo[bin];
+  mp.w0 = tc.centre[0];
+  mp.t = tc.centre[3];
+  mp.plane = tc.plane;
+  for (int f = 0; f < 6; f++) mp.aux[f] = tc.aux[f];
+  volume_pml_kernel<FX, FY, FZ, false>
+      <<<grid, PTOT, PML_SMEM, s>>>(mp, a, ps, nullptr, 1, ps.nunits, tc.err, tc.sched);
+}
+
+void launch_pml(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, const TileSched& ps, int grid,
+                cudaStream_t s) {
+  if (ps.nunits <= 0 || grid <= 0) return;
+  int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: launch_p<-1, -1, -1>(*tc, a, bin, ps, grid, s); break;
+    case 1: launch_p<-1, -1, 1>(*tc, a, bin, ps, grid, s); break;
+    case 2: launch_p<-1, 1, -1>(*tc, a, bin, ps, grid, s); break;
+    case 3: launch_p<-1, 1, 1>(*tc, a, bin, ps, grid, s); break;
+    case 4: launch_p<1, -1, -1>(*tc, a, bin, ps, grid, s); break;
+    case 5: launch_p<1, -1, 1>(*tc, a, bin, ps, grid, s); break;
+    case 6: launch_p<1, 1, -1>(*tc, a, bin, ps, grid, s); break;
+    default: launch_p<1, 1, 1>(*tc, a, bin, ps, grid, s); break;
+  }
+}
+
+template <int FX, int FY, int FZ>
+static void launch_pb(const TileScen& f, const TileScen* tab, int n, int nunits, int grid, int* err, int* sched,
+                      cudaStream_t s) {
+  volume_pml_kernel<FX, FY, FZ, true><<<grid, PTOT, PML_SMEM, s>>>(f.mp, f.u.a, f.u.sc, tab, n, nunits, err, sched);
+}
+void launch_pml_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY, int FZ,
+                      int* err, int* sched, cudaStream_t s) {
+  if (nunits <= 0 || grid <= 0) return;
+  int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
+  switch (code) {
+    case 0: launch_pb<-1, -1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 1: launch_pb<-1, -1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 2: launch_pb<-1, 1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 3: launch_pb<-1, 1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 4: launch_pb<1, -1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 5: launch_pb<1, -1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 6: launch_pb<1, 1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
+    default: launch_pb<1, 1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
+  }
+}
+
+}  // namespace dfd

@@ -10,6 +10,8 @@
 // Nodes of the seven x-layers around the fault whose (j,k) is not "united" are left
 // to the band kernel (dfd_fault.cu), exactly the nodes whose right-hand side the
 // reference overwrites in fault_dvelo / fault_dstrs.
+#include <cstring>
+
 #include "dfd_stencil.cuh"
 
 namespace dfd {
@@ -42,8 +44,9 @@ __device__ __forceinline__ void traction(const float* __restrict__ W, const floa
 }
 
 // General node update: every boundary treatment (PML faces, free-surface rows and
-// traction image, sponge).  Used for the shell of the domain outside the interior box.
-template <int FX, int FY, int FZ>
+// traction image, sponge).  Used for the shell of the domain outside the interior box;
+// TOP = false leaves out the free-surface terms (nodes below the top three rows).
+template <int FX, int FY, int FZ, bool TOP>
 __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, int j, int k) {
   const Dims& d = a.d;
   int i1 = i + 3, j1 = j + 3, k1 = k + 3;
@@ -60,7 +63,9 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 #pragma unroll
   for (int f = 0; f < 9; f++) p[f] = 0.0f;
   float dxv[3], dyv[3];
-  const bool top = a.freenode && k == d.nk - 1;
+  // free-surface rows (only in the TOP variant; the other boxes lie below them)
+  const bool fs = TOP && a.freenode && k >= d.nk - 3;
+  const bool top = fs && k == d.nk - 1;
   const bool px1 = a.aux[0] && i < d.N, px2 = a.aux[1] && i >= d.ni - d.N;
   const bool py1 = a.aux[2] && j < d.N, py2 = a.aux[3] && j >= d.nj - d.N;
   const bool pz1 = a.aux[4] && k < d.N, pz2 = a.aux[5] && k >= d.nk - d.N;
@@ -80,10 +85,9 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 #pragma unroll
       for (int r = 0; r < 3; r++) dz[r] = m[3 * r] * dxv[0] + m[3 * r + 1] * dxv[1] + m[3 * r + 2] * dxv[2];
     }
-    long long st = (long long)d.N * d.nj * d.nk;
-    int ia = px1 ? i : i - (d.ni - d.N);
-    long long qa = j + (long long)k * d.nj + (long long)ia * d.nj * d.nk;
-    pml_face(a, px1 ? 0 : 1, qa, st, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D,
+    const int fc = px1 ? 0 : 1;
+    const long long st = pml_fstride(d, fc), qa = pml_index(d, fc, i, j, k);
+    pml_face(a, fc, qa, st, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D,
              top ? dz : nullptr, ez0, ez1, ez2, lam, mu, p);
   }
   // ---- y ----
@@ -100,10 +104,9 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 #pragma unroll
       for (int r = 0; r < 3; r++) dz[r] = m[3 * r] * dyv[0] + m[3 * r + 1] * dyv[1] + m[3 * r + 2] * dyv[2];
     }
-    long long st = (long long)d.N * d.nk * d.ni;
-    int ja = py1 ? j : j - (d.nj - d.N);
-    long long qa = ja + (long long)k * d.N + (long long)i * d.N * d.nk;
-    pml_face(a, py1 ? 2 : 3, qa, st, rb2, __ldg(a.By + j), __ldg(a.Dpy + j), __ldg(a.Apy + j), D,
+    const int fc = py1 ? 2 : 3;
+    const long long st = pml_fstride(d, fc), qa = pml_index(d, fc, i, j, k);
+    pml_face(a, fc, qa, st, rb2, __ldg(a.By + j), __ldg(a.Dpy + j), __ldg(a.Apy + j), D,
              top ? dz : nullptr, ez0, ez1, ez2, lam, mu, p);
   }
   // ---- z ----
@@ -113,7 +116,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
   axis_terms(dv, ez0, ez1, ez2, lam, mu, rrho, Dz_plain);
 #pragma unroll
   for (int f = 0; f < 9; f++) D[f] = Dz_plain[f];
-  if (a.freenode && k >= d.nk - 3) {
+  if (fs) {
     // velocity z-derivatives on the top rows (wave.cu:205-245)
     float dz[3];
     if (k == d.nk - 1) {
@@ -149,14 +152,13 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 #pragma unroll
   for (int f = 0; f < 9; f++) h[f] += D[f] * rb3;
   if (pz1 || pz2) {
-    long long st = (long long)d.N * d.ni * d.nj;
-    int ka = pz1 ? k : k - (d.nk - d.N);
-    long long qa = j + (long long)ka * d.nj + (long long)i * d.nj * d.N;
-    pml_face(a, pz1 ? 4 : 5, qa, st, rb3, __ldg(a.Bz + k), __ldg(a.Dpz + k), __ldg(a.Apz + k), Dz_plain, nullptr,
+    const int fc = pz1 ? 4 : 5;
+    const long long st = pml_fstride(d, fc), qa = pml_index(d, fc, i, j, k);
+    pml_face(a, fc, qa, st, rb3, __ldg(a.Bz + k), __ldg(a.Dpz + k), __ldg(a.Apz + k), Dz_plain, nullptr,
              ez0, ez1, ez2, lam, mu, p);
   }
   // ---- traction image for the momentum equation on the top three rows (wave.cu:398-487)
-  if (a.freenode && k >= d.nk - 3) {
+  if (fs) {
     int ik = d.nk - 1 - k;
     float rrhojac = rrho / __ldg(M + 9 * n + q);
     float v1[3][7], v2[3][7], v3[3][7];
@@ -184,20 +186,25 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 }
 
 
-// Shell kernel: the general update on up to eight boxes (PML slabs, free-surface rows) that
-// surround the interior box; one 1-D grid of 128-thread blocks is split over the boxes
-// (small blocks fit beside a CTA of the tiled interior kernel, so the two kernels share
-// the SMs).  A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z) per block; a
+// Shell kernels: the general update on up to eight boxes (PML slabs, free-surface rows)
+// that surround the interior box; one 1-D grid of 128-thread blocks is split over the
+// boxes below the free-surface rows (at most 170 registers, three blocks per SM: the PML
+// path needs about 160) and a second over the rows themselves (the traction image needs
+// about 230).  A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z) per block; a
 // thinner box (the y slabs of the PML, the free-surface rows) is flattened over (y, z)
 // with y fastest, so that no thread idles and the y-face PML state (y fastest over N
 // nodes, then z) is read contiguously.
 constexpr int SHELL_THREADS = 128;
 
-// block blk of the shell grid of one scenario
-template <int FX, int FY, int FZ>
+// block blk of the shell grid of one scenario: of the boxes below the free-surface rows
+// (TOP = false, blk counted from box 0) or of the free-surface boxes (TOP, blk counted
+// from box ntop)
+template <int FX, int FY, int FZ, bool TOP>
 __device__ __forceinline__ void volume_shell_body(const VolArgs& a, const Boxes& bx, int blk) {
-  int b = 0;
-  while (b + 1 < bx.n && blk >= bx.start[b + 1]) b++;
+  int b = TOP ? bx.ntop : 0;
+  const int bend = TOP ? bx.n : bx.ntop;
+  if (TOP) blk += bx.start[bx.ntop];
+  while (b + 1 < bend && blk >= bx.start[b + 1]) b++;
   int loc = blk - bx.start[b];
   int ni = bx.hi[b][0] - bx.lo[b][0], nj = bx.hi[b][1] - bx.lo[b][1], nk = bx.hi[b][2] - bx.lo[b][2];
   int i, j, k;
@@ -216,21 +223,28 @@ __device__ __forceinline__ void volume_shell_body(const VolArgs& a, const Boxes&
     i = bi;
     if (i >= ni || j >= nj || k >= nk) return;
   }
-  volume_point_general<FX, FY, FZ>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
+  volume_point_general<FX, FY, FZ, TOP>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
 }
-template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(SHELL_THREADS, 4)
+template <int FX, int FY, int FZ, bool TOP>
+__global__ void __launch_bounds__(SHELL_THREADS, TOP ? 2 : 3)
     volume_shell_kernel(const __grid_constant__ VolArgs a, const __grid_constant__ Boxes bx) {
-  volume_shell_body<FX, FY, FZ>(a, bx, blockIdx.x);
+  volume_shell_body<FX, FY, FZ, TOP>(a, bx, blockIdx.x);
 }
 // all scenarios of an ensemble in one launch: scenario s owns blocks [start[s], start[s+1])
-template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(SHELL_THREADS, 4)
+template <int FX, int FY, int FZ, bool TOP>
+__global__ void __launch_bounds__(SHELL_THREADS, TOP ? 2 : 3)
     volume_shell_batch(const VolArgs* __restrict__ tab, const Boxes* __restrict__ boxes,
                        const int* __restrict__ start, int n) {
+  __shared__ __align__(16) unsigned char raw_a[sizeof(VolArgs)];
+  __shared__ __align__(16) unsigned char raw_b[sizeof(Boxes)];
+  VolArgs* sa = reinterpret_cast<VolArgs*>(raw_a);
+  Boxes* sb = reinterpret_cast<Boxes*>(raw_b);
   int loc;
   const int sc = scenario_of(start, n, blockIdx.x, &loc);
-  volume_shell_body<FX, FY, FZ>(tab[sc], boxes[sc], loc);
+  stage_args(sa, tab + sc);
+  stage_args(sb, boxes + sc);
+  __syncthreads();
+  volume_shell_body<FX, FY, FZ, TOP>(*sa, *sb, loc);
 }
 
 // Interior kernel: no PML (beta = 1, no auxiliary state), no free-surface rows.  Each
@@ -291,15 +305,17 @@ __global__ void __launch_bounds__(256, 3) volume_interior_kernel(VolArgs a, int3
   }
 }
 
-// Volume work of one stage: which box the tiled (or plain) interior kernel takes and the
-// boxes of the general kernel around it.
+// Volume work of one stage: which box the tiled (or plain) interior kernel takes, the
+// units of the tiled PML kernel and the boxes of the general kernel.
 VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
   const Dims& d = a.d;
   VolPlan pl;
-  pl.tiled = pl.pmlp = pl.plain = false;
+  pl.tiled = pl.plain = false;
   pl.nodes = 0;
+  pl.pgrid = 0;
+  memset(&pl.ps, 0, sizeof pl.ps);
   Boxes& bx = pl.bx;
-  bx.n = 0;
+  bx.n = bx.ntop = 0;
   auto add = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
     if (i1 <= i0 || j1 <= j0 || k1 <= k0) return;
     bx.lo[bx.n][0] = i0; bx.lo[bx.n][1] = j0; bx.lo[bx.n][2] = k0;
@@ -312,46 +328,47 @@ VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
   int nz0 = a.aux[4] ? d.N : 0, nz1 = a.aux[5] ? d.N : (a.freenode ? 3 : 0);
   int3 lo = make_int3(nx0, ny0, nz0), hi = make_int3(d.ni - nx1, d.nj - ny1, d.nk - nz1);
   const int ktop = a.freenode ? d.nk - 3 : d.nk;
-  if (tc && tc->ok && tc->pml == 1 && tile_feasible(tc, a, make_int3(0, 0, 0), make_int3(d.ni, d.nj, ktop))) {
-    // TMA-tiled kernel over every node below the free-surface rows; the general kernel
-    // takes the free-surface rows
-    pl.tiled = pl.pmlp = true;
-    pl.lo = make_int3(0, 0, 0);
-    pl.hi = make_int3(d.ni, d.nj, ktop);
-    add(0, d.ni, 0, d.nj, ktop, d.nk);
-  } else {
-    // interior box by the TMA-tiled kernel (or the plain interior kernel), the shell
-    // around it by the general kernel.  The tiles start on a 16-byte boundary in y: the
-    // tiled box starts at the next boundary, and the general kernel takes the (at most
-    // three) interior columns before it.
-    int3 tlo = lo, thi = hi;
-    tlo.y += (4 - (lo.y + 3 + d.oy) % 4) % 4;
-    const bool xslabs = tc && tc->pml == 3;
-    if (xslabs) {
-      // the tiles also cover the two x slabs of the PML
-      tlo.x = 0;
-      thi.x = d.ni;
+  bool done = false;
+  if (tc && tc->ok) {
+    // the interior kernel takes the whole tiles (frame at j = 0, k = 0) inside the interior
+    // box; the PML kernel every other node below the free-surface rows
+    int tja = (lo.y + TILE_J - 1) / TILE_J, tjb = hi.y / TILE_J;
+    int tka = (lo.z + TILE_K - 1) / TILE_K, tkb = hi.z / TILE_K;
+    if (tja >= tjb || tka >= tkb || lo.x >= hi.x) tja = tjb = tka = tkb = 0;
+    int grid = 0;
+    TileSched ps = pml_plan(a, tja, tjb, tka, tkb, ktop, tc->nsm, &grid);
+    const int3 rlo = make_int3(lo.x, tja * TILE_J, tka * TILE_K), rhi = make_int3(hi.x, tjb * TILE_J, tkb * TILE_K);
+    if (ps.nunits >= 0 && (tja == tjb || tile_feasible(tc, a, rlo, rhi))) {
+      done = true;
+      pl.ps = ps;
+      pl.pgrid = grid;
+      if (tja < tjb) {
+        pl.tiled = true;
+        pl.lo = rlo;
+        pl.hi = rhi;
+      }
+      add(0, d.ni, 0, d.nj, ktop, d.nk);  // the free-surface rows
     }
+  }
+  if (!done) {
+    // the plain interior kernel on the interior box, the general kernel on the slabs
+    // around it, then on the free-surface rows
     const bool some = hi.x > lo.x && hi.y > lo.y && hi.z > lo.z;
-    if (some && thi.y > tlo.y && tile_feasible(tc, a, tlo, thi)) {
-      pl.tiled = true;
-      pl.pmlp = xslabs;
-      pl.lo = tlo;
-      pl.hi = thi;
-      add(tlo.x, thi.x, lo.y, tlo.y, lo.z, hi.z);
-      lo.x = tlo.x;
-      hi.x = thi.x;
-    } else if (some) {
+    if (some) {
       pl.plain = true;
       pl.lo = lo;
       pl.hi = hi;
+    } else {
+      lo = hi = make_int3(0, 0, 0);
     }
-    add(0, lo.x, 0, d.nj, 0, d.nk);
-    add(hi.x, d.ni, 0, d.nj, 0, d.nk);
-    add(lo.x, hi.x, 0, lo.y, 0, d.nk);
-    add(lo.x, hi.x, hi.y, d.nj, 0, d.nk);
+    add(0, lo.x, 0, d.nj, 0, ktop);
+    add(hi.x, d.ni, 0, d.nj, 0, ktop);
+    add(lo.x, hi.x, 0, lo.y, 0, ktop);
+    add(lo.x, hi.x, hi.y, d.nj, 0, ktop);
     add(lo.x, hi.x, lo.y, hi.y, 0, lo.z);
-    add(lo.x, hi.x, lo.y, hi.y, hi.z, d.nk);
+    add(lo.x, hi.x, lo.y, hi.y, hi.z, ktop);
+    bx.ntop = bx.n;
+    add(0, d.ni, 0, d.nj, ktop, d.nk);
   }
   if (pl.tiled || pl.plain) pl.nodes = (long long)(pl.hi.x - pl.lo.x) * (pl.hi.y - pl.lo.y) * (pl.hi.z - pl.lo.z);
   int tot = 0;
@@ -368,11 +385,12 @@ VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
 
 template <int FX, int FY, int FZ>
 static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin,
-                              cudaEvent_t* kb, cudaEvent_t* ke) {
+                              cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out) {
   const VolPlan pl = plan_volume(a, tc);
+  if (out) *out = pl;
   if (kb) cudaEventRecord(*kb, s);
   if (pl.tiled) {
-    launch_tile(tc, a, FX, FY, FZ, bin, pl.lo, pl.hi, pl.pmlp, s);
+    launch_tile(tc, a, FX, FY, FZ, bin, pl.lo, pl.hi, s);
   } else if (pl.plain) {
     const int chunk = 8;
     dim3 block(32, 8, 1);
@@ -380,28 +398,32 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, pl.lo, pl.hi, chunk);
   }
   if (ke) cudaEventRecord(*ke, s);
-  if (pl.shell_blocks > 0) volume_shell_kernel<FX, FY, FZ><<<pl.shell_blocks, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
+  if (pl.ps.nunits > 0) launch_pml(tc, a, FX, FY, FZ, bin, pl.ps, pl.pgrid, s);
+  const int below = pl.bx.start[pl.bx.ntop], above = pl.bx.start[pl.bx.n] - below;
+  if (below > 0) volume_shell_kernel<FX, FY, FZ, false><<<below, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
+  if (above > 0) volume_shell_kernel<FX, FY, FZ, true><<<above, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
   return pl.nodes;
 }
 
 template <int FX, int FY, int FZ>
-static void shell_batch_t(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks,
+static void shell_batch_t(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, bool top,
                           cudaStream_t s) {
-  volume_shell_batch<FX, FY, FZ><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n);
+  if (top) volume_shell_batch<FX, FY, FZ, true><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n);
+  else volume_shell_batch<FX, FY, FZ, false><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n);
 }
 void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, int FX, int FY,
-                        int FZ, cudaStream_t s) {
+                        int FZ, bool top, cudaStream_t s) {
   if (blocks <= 0) return;
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: shell_batch_t<-1, -1, -1>(tab, boxes, start, n, blocks, s); break;
-    case 1: shell_batch_t<-1, -1, 1>(tab, boxes, start, n, blocks, s); break;
-    case 2: shell_batch_t<-1, 1, -1>(tab, boxes, start, n, blocks, s); break;
-    case 3: shell_batch_t<-1, 1, 1>(tab, boxes, start, n, blocks, s); break;
-    case 4: shell_batch_t<1, -1, -1>(tab, boxes, start, n, blocks, s); break;
-    case 5: shell_batch_t<1, -1, 1>(tab, boxes, start, n, blocks, s); break;
-    case 6: shell_batch_t<1, 1, -1>(tab, boxes, start, n, blocks, s); break;
-    default: shell_batch_t<1, 1, 1>(tab, boxes, start, n, blocks, s); break;
+    case 0: shell_batch_t<-1, -1, -1>(tab, boxes, start, n, blocks, top, s); break;
+    case 1: shell_batch_t<-1, -1, 1>(tab, boxes, start, n, blocks, top, s); break;
+    case 2: shell_batch_t<-1, 1, -1>(tab, boxes, start, n, blocks, top, s); break;
+    case 3: shell_batch_t<-1, 1, 1>(tab, boxes, start, n, blocks, top, s); break;
+    case 4: shell_batch_t<1, -1, -1>(tab, boxes, start, n, blocks, top, s); break;
+    case 5: shell_batch_t<1, -1, 1>(tab, boxes, start, n, blocks, top, s); break;
+    case 6: shell_batch_t<1, 1, -1>(tab, boxes, start, n, blocks, top, s); break;
+    default: shell_batch_t<1, 1, 1>(tab, boxes, start, n, blocks, top, s); break;
   }
 }
 
@@ -409,17 +431,17 @@ void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start
 // before and after the interior (tiled) kernel.  Returns the nodes of the box that kernel
 // covers.
 long long launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
-                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke) {
+                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out) {
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: return launch_flags<-1, -1, -1>(a, s, s_shell, tc, bin, kb, ke);
-    case 1: return launch_flags<-1, -1, 1>(a, s, s_shell, tc, bin, kb, ke);
-    case 2: return launch_flags<-1, 1, -1>(a, s, s_shell, tc, bin, kb, ke);
-    case 3: return launch_flags<-1, 1, 1>(a, s, s_shell, tc, bin, kb, ke);
-    case 4: return launch_flags<1, -1, -1>(a, s, s_shell, tc, bin, kb, ke);
-    case 5: return launch_flags<1, -1, 1>(a, s, s_shell, tc, bin, kb, ke);
-    case 6: return launch_flags<1, 1, -1>(a, s, s_shell, tc, bin, kb, ke);
-    default: return launch_flags<1, 1, 1>(a, s, s_shell, tc, bin, kb, ke);
+    case 0: return launch_flags<-1, -1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
+    case 1: return launch_flags<-1, -1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
+    case 2: return launch_flags<-1, 1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
+    case 3: return launch_flags<-1, 1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
+    case 4: return launch_flags<1, -1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
+    case 5: return launch_flags<1, -1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
+    case 6: return launch_flags<1, 1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
+    default: return launch_flags<1, 1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
   }
 }
 
