@@ -1,6 +1,6 @@
 /* NetCDF-classic shim -- test infrastructure only.
- * Declares the entry points the reference calls (SURVEY of the reference:
- * nc_open .. nc_put_var_int).  The reading side is implemented from the public
+ * Declares the entry points the reference's sources call (nc_open ..
+ * nc_put_var_int).  The reading side is implemented from the public
  * classic (CDF-1 / CDF-2) format description; the writing side is not needed by
  * the harness and reports an error if reached. */
 #ifndef DFD_REFSHIM_NETCDF_H
