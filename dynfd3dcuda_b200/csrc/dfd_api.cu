@@ -1079,8 +1079,10 @@ int dfd_output_close(dfd_ctx* ctx) {
 // the scenarios' own contexts, so results are read with the usual getters.
 struct EnsStage {
   FaultArgs* fault = nullptr;  // rupture scenarios
-  int* fstart = nullptr;       // (nf + 1) block starts of the fault kernels
+  int* fstart = nullptr;       // (nf + 1) block starts of the fault node kernel
   int fblocks = 0;
+  int* bstart = nullptr;       // (nf + 1) block starts of the fault band kernel
+  int bblocks = 0;
   VolArgs* vol = nullptr;      // all scenarios
   Boxes* boxes = nullptr;
   int* sstart = nullptr;       // (n + 1) block starts of the shell kernel, boxes below the top rows
@@ -1149,14 +1151,17 @@ static int ens_build(dfd_ens* e) {
       int sg = (irk % 2) ? -1 : 1;
       S.FX = kFlags[pat][0] * sg; S.FY = kFlags[pat][1] * sg; S.FZ = kFlags[pat][2] * sg;
       std::vector<FaultArgs> fa;
-      std::vector<int> fs(1, 0);
+      std::vector<int> fs(1, 0), bs(1, 0);
       for (int r : e->rup) {
         FaultArgs a = fault_args(e->sc[r], pat, irk);
         a.it_dev = e->it_dev;  // one step counter for the whole ensemble
         fa.push_back(a);
-        fs.push_back(fs.back() + ((a.d.nj + 31) / 32) * ((a.d.nk + 3) / 4));
+        const int g = ((a.d.nj + 31) / 32) * ((a.d.nk + 3) / 4);
+        fs.push_back(fs.back() + g);
+        bs.push_back(bs.back() + 7 * g);  // the band kernel: seven parts per column block
       }
       S.fblocks = fs.back();
+      S.bblocks = bs.back();
       std::vector<VolArgs> va;
       std::vector<Boxes> bx;
       std::vector<int> ss(1, 0), tt(1, 0);
@@ -1209,6 +1214,7 @@ static int ens_build(dfd_ens* e) {
       if (!e->rup.empty()) {
         r = r ? r : ens_upload(e, &S.fault, fa);
         r = r ? r : ens_upload(e, &S.fstart, fs);
+        r = r ? r : ens_upload(e, &S.bstart, bs);
       }
       r = r ? r : ens_upload(e, &S.vol, va);
       r = r ? r : ens_upload(e, &S.boxes, bx);
@@ -1231,14 +1237,14 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
     launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
     launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, e->s0);
     launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s0);
-    if (nr) launch_fault_band_batch(S.fault, S.fstart, nr, S.fblocks, S.FX, S.FY, S.FZ, e->s0);
+    if (nr) launch_fault_band_batch(S.fault, S.bstart, nr, S.bblocks, S.FX, S.FY, S.FZ, e->s0);
     cudaError_t ce = cudaGetLastError();
     return ce == cudaSuccess ? DFD_OK : ens_fail(e, DFD_ERR_CUDA, std::string("ensemble stage: ") + cudaGetErrorString(ce));
   }
   cudaEventRecord(e->ev_fork, e->s0);
   if (nr) {
     cudaStreamWaitEvent(e->s1, e->ev_fork, 0);
-    launch_fault_band_batch(S.fault, S.fstart, nr, S.fblocks, S.FX, S.FY, S.FZ, e->s1);
+    launch_fault_band_batch(S.fault, S.bstart, nr, S.bblocks, S.FX, S.FY, S.FZ, e->s1);
     cudaEventRecord(e->ev_join, e->s1);
   }
   cudaStreamWaitEvent(e->s2, e->ev_fork, 0);

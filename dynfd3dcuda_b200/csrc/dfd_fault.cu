@@ -5,8 +5,9 @@
 //   trial traction + slip-weakening (trial_slipweakening.cu:23-732) or rate-and-state
 //   FP64 Newton solve (trial_ratestate.cu:20-893), then the split-node -> volume transfer
 //   of the fault plane (transform.cu:224-403).
-// fault_band_kernel (one thread per non-united fault node), concurrent with the volume
-//   kernel: velocity RHS on the six off-fault layers and both split sides
+// fault_band_kernel (seven threads per non-united fault node: one per off-fault layer,
+//   one for the split nodes), after the volume kernels: velocity RHS on the six off-fault
+//   layers and both split sides
 //   (fault_dvelo.cu:17-389), stress RHS (fault_dstrs_f.cu / fault_dstrs_b.cu), the RK4
 //   update of those band nodes and of the split nodes (rk4.cu:573-789), the RK-weighted
 //   on-fault outputs (rk4.cu:466-571), the end-of-stage transfer and the sponge.
@@ -99,6 +100,42 @@ __device__ void fault_to_volume(const FaultArgs& a, const float* FW, float* Wdst
     for (int c = 0; c < 3; c++) sg[r][c] = (tr[r][0] * im[0][c] + tr[r][1] * im[1][c] + tr[r][2] * im[2][c]) * rj;
 #pragma unroll
   for (int c = 0; c < 3; c++) Wdst[c * n + q] = (FW[c * 2 * nyz + pf] + FW[c * 2 * nyz + nyz + pf]) * 0.5f * damp;
+  Wdst[3 * n + q] = sg[0][0] * damp;
+  Wdst[4 * n + q] = sg[1][1] * damp;
+  Wdst[5 * n + q] = sg[2][2] * damp;
+  Wdst[6 * n + q] = (sg[0][1] + sg[1][0]) * 0.5f * damp;
+  Wdst[7 * n + q] = (sg[0][2] + sg[2][0]) * 0.5f * damp;
+  Wdst[8 * n + q] = (sg[1][2] + sg[2][1]) * 0.5f * damp;
+}
+
+// fault_to_volume with the split-node values of the stage (fw[field][side]) in registers
+// and every load issued before the first store
+__device__ __forceinline__ void fault_to_volume_r(const FaultArgs& a, const float (*fw)[2], float* Wdst, int j1,
+                                                  int k1, float damp) {
+  const Dims& d = a.d;
+  long long n = d.nxyz, nyz = d.nyz, pf = j1 + (long long)k1 * d.ny;
+  long long q = idx3(d, d.i0, j1, k1);
+  float met[3][3], im[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) met[r][c] = a.M[(3 * c + r) * n + q];
+  float rj = 1.0f / a.M[9 * n + q];
+  float tr[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    tr[c][0] = a.T1[(c * 7 + 3) * nyz + pf];
+    tr[c][1] = (fw[3 + c][0] + fw[3 + c][1]) * 0.5f;
+    tr[c][2] = (fw[6 + c][0] + fw[6 + c][1]) * 0.5f;
+  }
+  inv3(met, im);
+  float sg[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) sg[r][c] = (tr[r][0] * im[0][c] + tr[r][1] * im[1][c] + tr[r][2] * im[2][c]) * rj;
+#pragma unroll
+  for (int c = 0; c < 3; c++) Wdst[c * n + q] = (fw[c][0] + fw[c][1]) * 0.5f * damp;
   Wdst[3 * n + q] = sg[0][0] * damp;
   Wdst[4 * n + q] = sg[1][1] * damp;
   Wdst[5 * n + q] = sg[2][2] * damp;
@@ -487,23 +524,42 @@ __device__ __forceinline__ void hooke(const float* M, long long n, long long q, 
   hT[5] = (ex2 * X[1] + ex1 * X[2] + ey2 * Y[1] + ey1 * Y[2] + ez2 * Z[1] + ez1 * Z[2]) * mu;
 }
 
-__device__ __forceinline__ void rk_store(const FaultArgs& a, long long x, float h, float damp) {
-  float w;
-  if (a.irk == 0) {
-    float w0 = a.Win[x];
-    a.T[x] = fmaf(a.rkb, h, w0);
-    w = fmaf(a.rka, h, w0);
-  } else if (a.irk < 3) {
-    a.T[x] = fmaf(a.rkb, h, a.T[x]);
-    w = fmaf(a.rka, h, a.W0[x]);
-  } else {
-    w = fmaf(a.rkb, h, a.T[x]);
+// RK4 registers and stage output of the nine fields of volume node q, every load before
+// the first store (rk4.cu:20-33)
+__device__ __forceinline__ void rk_store9(const FaultArgs& a, long long q, const float* h, float damp) {
+  const long long n = a.d.nxyz;
+  float r0[9], r1[9];
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    const long long x = f * n + q;
+    if (a.irk == 0) {
+      r0[f] = a.Win[x];
+    } else if (a.irk < 3) {
+      r1[f] = a.T[x];
+      r0[f] = a.W0[x];
+    } else {
+      r1[f] = a.T[x];
+    }
   }
-  a.Wout[x] = w * damp;
+#pragma unroll
+  for (int f = 0; f < 9; f++) {
+    const long long x = f * n + q;
+    float w;
+    if (a.irk == 0) {
+      a.T[x] = fmaf(a.rkb, h[f], r0[f]);
+      w = fmaf(a.rka, h[f], r0[f]);
+    } else if (a.irk < 3) {
+      a.T[x] = fmaf(a.rkb, h[f], r1[f]);
+      w = fmaf(a.rka, h[f], r0[f]);
+    } else {
+      w = fmaf(a.rkb, h[f], r1[f]);
+    }
+    a.Wout[x] = w * damp;
+  }
 }
 
 template <int FX, int FY, int FZ>
-__device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int by) {
+__device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int by, int part) {
   const Dims& d = a.d;
   int j = bx * blockDim.x + threadIdx.x;
   int k = by * blockDim.y + threadIdx.y;
@@ -512,7 +568,7 @@ __device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int 
   if (a.united[q2]) {
     // welded nodes: the RK-weighted outputs run over every node in the reference
     // (rk4.cu:521-569) and are zero there (no trial traction, no split velocity)
-    if (a.irk == 0) {
+    if (a.irk == 0 && part == 6) {
       a.Tn[q2] = 0.0f; a.Ts1[q2] = 0.0f; a.Ts2[q2] = 0.0f;
       a.Vs1[q2] = 0.0f; a.Vs2[q2] = 0.0f; a.hslip[q2] = 0.0f;
     }
@@ -529,9 +585,9 @@ __device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int 
   float dampyz = 1.0f;
   if (a.dampx) dampyz = fminf(a.dampy[j1], a.dampz[k1]);
 
-  // ---------------- volume nodes of the six off-fault layers
-  for (int l = -3; l <= 3; l++) {
-    if (l == 0) continue;
+  // ---------------- volume nodes of one of the six off-fault layers (parts 0..5)
+  if (part < 6) {
+    const int l = part < 3 ? part - 3 : part - 2;
     const int i = i0 + l;
     const long long q = idx3(d, i, j1, k1);
     // velocity RHS (fault_dvelo.cu:153-254), traction image across the fault
@@ -612,13 +668,12 @@ __device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int 
     float hT[6];
     hooke(M, n, q, X, Y, Z, hT);
     float damp = a.dampx ? fminf(a.dampx[i], dampyz) : 1.0f;
-#pragma unroll
-    for (int c = 0; c < 3; c++) rk_store(a, c * n + q, hv[c], damp);
-#pragma unroll
-    for (int c = 0; c < 6; c++) rk_store(a, (3 + c) * n + q, hT[c], damp);
+    const float h9[9] = {hv[0], hv[1], hv[2], hT[0], hT[1], hT[2], hT[3], hT[4], hT[5]};
+    rk_store9(a, q, h9, damp);
   }
 
-  // ---------------- split nodes
+  // ---------------- split nodes (part 6)
+  if (part != 6) return;
   float hF[9][2];
   // velocity RHS on both sides (fault_dvelo.cu:260-385)
 #pragma unroll
@@ -724,37 +779,58 @@ __device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int 
         for (int c = 0; c < 3; c++) hF[3 + 3 * g + c][m] = o1[c] + o2[c] + o3[c];
       }
   }
-  // split-node RK4 + viscosity (rk4.cu:656-727)
-  float vis = a.viscosity * a.DT;
+  // split-node RK4 + viscosity (rk4.cu:656-727), then the RK-weighted on-fault outputs
+  // (rk4.cu:521-569) and the fault plane of the stage output (transform.cu via
+  // main.cu:504).  Every load comes before the first store: the compiler cannot prove the
+  // buffers distinct, and a load behind a store would wait a memory round trip each.
+  float r0[9][2], r1[9][2];
 #pragma unroll
   for (int f = 0; f < 9; f++)
 #pragma unroll
     for (int m = 0; m < 2; m++) {
-      long long x = f * 2 * nyz + m * nyz + pf;
-      float h = hF[f][m], w;
+      const long long x = f * 2 * nyz + m * nyz + pf;
       if (a.irk == 0) {
-        float w0 = FW[x];
-        a.Fm[x] = w0;
-        a.Ft[x] = fmaf(a.rkb, h, w0);
-        w = fmaf(a.rka, h, w0);
+        r0[f][m] = FW[x];
       } else if (a.irk < 3) {
-        a.Ft[x] = fmaf(a.rkb, h, a.Ft[x]);
-        w = fmaf(a.rka, h, a.Fm[x]);
+        r0[f][m] = a.Fm[x];
+        r1[f][m] = a.Ft[x];
       } else {
-        w = fmaf(a.rkb, h, a.Ft[x]);
+        r1[f][m] = a.Ft[x];
+      }
+    }
+  float s1[3], s2[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) { s1[c] = a.vecs1[c * nyz + pf]; s2[c] = a.vecs2[c * nyz + pf]; }
+  const float tts1 = a.tTs1[q2], tts2 = a.tTs2[q2], ttn = a.tTn[q2];
+  float ts1 = 0.0f, ts2 = 0.0f, tn = 0.0f;
+  if (a.irk != 0) { ts1 = a.Ts1[q2]; ts2 = a.Ts2[q2]; tn = a.Tn[q2]; }
+  const float vis = a.viscosity * a.DT;
+  float wv[9][2];
+#pragma unroll
+  for (int f = 0; f < 9; f++)
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const long long x = f * 2 * nyz + m * nyz + pf;
+      const float h = hF[f][m];
+      float w;
+      if (a.irk == 0) {
+        a.Fm[x] = r0[f][m];
+        a.Ft[x] = fmaf(a.rkb, h, r0[f][m]);
+        w = fmaf(a.rka, h, r0[f][m]);
+      } else if (a.irk < 3) {
+        a.Ft[x] = fmaf(a.rkb, h, r1[f][m]);
+        w = fmaf(a.rka, h, r0[f][m]);
+      } else {
+        w = fmaf(a.rkb, h, r1[f][m]);
       }
       if (f >= 3) w += vis * h;
       a.FWout[x] = w;
+      wv[f][m] = w;
     }
-  // RK-weighted on-fault outputs (rk4.cu:521-569)
   {
-    const float* F2 = a.FWout;
     float dV[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) dV[c] = F2[c * 2 * nyz + nyz + pf] - F2[c * 2 * nyz + pf];
-    float s1[3], s2[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) { s1[c] = a.vecs1[c * nyz + pf]; s2[c] = a.vecs2[c * nyz + pf]; }
+    for (int c = 0; c < 3; c++) dV[c] = wv[c][1] - wv[c][0];
     float vs1 = dV[0] * s1[0] + dV[1] * s1[1] + dV[2] * s1[2];
     float vs2 = dV[0] * s2[0] + dV[1] * s2[1] + dV[2] * s2[2];
     a.hslip[q2] = sqrtf(vs2 * vs2 + vs1 * vs1);
@@ -762,14 +838,13 @@ __device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int 
     a.Vs2[q2] = vs2;
     float rkb1 = a.rkb / a.DT;
     if (a.irk == 0) {
-      a.Ts1[q2] = rkb1 * a.tTs1[q2]; a.Ts2[q2] = rkb1 * a.tTs2[q2]; a.Tn[q2] = rkb1 * a.tTn[q2];
+      a.Ts1[q2] = rkb1 * tts1; a.Ts2[q2] = rkb1 * tts2; a.Tn[q2] = rkb1 * ttn;
     } else {
-      a.Ts1[q2] += rkb1 * a.tTs1[q2]; a.Ts2[q2] += rkb1 * a.tTs2[q2]; a.Tn[q2] += rkb1 * a.tTn[q2];
+      a.Ts1[q2] = ts1 + rkb1 * tts1; a.Ts2[q2] = ts2 + rkb1 * tts2; a.Tn[q2] = tn + rkb1 * ttn;
     }
   }
-  // fault plane of the stage output (transform.cu via main.cu:504) and the sponge
   float damp0 = a.dampx ? fminf(a.dampx[i0], dampyz) : 1.0f;
-  fault_to_volume(a, a.FWout, a.Wout, j1, k1, damp0);
+  fault_to_volume_r(a, wv, a.Wout, j1, k1, damp0);
 }
 
 template <int FY, int FZ>
@@ -777,9 +852,11 @@ __global__ void __launch_bounds__(128) fault_node_kernel(const __grid_constant__
   __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
   fault_node_body<FY, FZ>(a, blockIdx.x, blockIdx.y, snet);
 }
+// grid z: the part (six off-fault layers, then the split nodes), so that the seven
+// independent pieces of a fault column run in parallel
 template <int FX, int FY, int FZ>
 __global__ void __launch_bounds__(128) fault_band_kernel(const __grid_constant__ FaultArgs a) {
-  fault_band_body<FX, FY, FZ>(a, blockIdx.x, blockIdx.y);
+  fault_band_body<FX, FY, FZ>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Batched launches over the scenarios of an ensemble: scenario s owns the blocks
@@ -808,8 +885,9 @@ __global__ void __launch_bounds__(128) fault_band_batch(const FaultArgs* __restr
   stage_args(sa, tab + sc);
   __syncthreads();
   const FaultArgs& a = *sa;
-  const int gx = (a.d.nj + 31) / 32;
-  fault_band_body<FX, FY, FZ>(a, loc % gx, loc / gx);
+  const int gx = (a.d.nj + 31) / 32, gxy = gx * ((a.d.nk + 3) / 4);
+  // the scenario's blocks: seven parts of its (32, 4)-block grid
+  fault_band_body<FX, FY, FZ>(a, (loc % gxy) % gx, (loc % gxy) / gx, loc / gxy);
 }
 
 void launch_fault_node(const FaultArgs& a, cudaStream_t s) {
@@ -826,7 +904,7 @@ void launch_fault_node(const FaultArgs& a, cudaStream_t s) {
 
 void launch_fault_band(const FaultArgs& a, cudaStream_t s) {
   dim3 block(32, 4, 1);
-  dim3 grid((a.d.nj + 31) / 32, (a.d.nk + 3) / 4, 1);
+  dim3 grid((a.d.nj + 31) / 32, (a.d.nk + 3) / 4, 7);
   int code = (a.FX > 0) * 4 + (a.FY > 0) * 2 + (a.FZ > 0);
   switch (code) {
     case 0: fault_band_kernel<-1, -1, -1><<<grid, block, 0, s>>>(a); break;
