@@ -1188,11 +1188,7 @@ static int ens_build(dfd_ens* e) {
           }
         }
         TileScen& t = ts[i];
-        t.mp.win = c->tile.halo[bin[irk]];
-        t.mp.w0 = c->tile.centre[0];
-        t.mp.t = c->tile.centre[3];
-        t.mp.plane = c->tile.plane;
-        for (int f = 0; f < 6; f++) t.mp.aux[f] = c->tile.aux[f];
+        t.mp = tile_maps(c->tile, bin[irk]);
         t.u.a = a;
         t.u.sc = sch;
         t.u.unit0 = units;

@@ -185,8 +185,9 @@ struct GridArgs {
   double lam1, mu1, rho1, lam2, mu2, rho2;
 };
 
-// Tile of the TMA-staged kernels: 32 nodes along y (one warp) by 8 along z.
-constexpr int TILE_J = 32, TILE_K = 8;
+// Tile of the TMA-staged kernels: 32 nodes along y (one warp) by 8 along z; the PML
+// kernel's y-slab units use strip tiles of 16 by 16 (half a warp per row).
+constexpr int TILE_J = 32, TILE_K = 8, STRIP = 16;
 
 // TMA tensor maps handed to the tiled kernels (dfd_tile.cu, dfd_pml.cu)
 struct TileMaps {
@@ -195,6 +196,8 @@ struct TileMaps {
   CUtensorMap t;    // RK accumulator, pointwise box
   CUtensorMap plane;  // separable metric / media planes (12, nz, py)
   CUtensorMap aux[6];  // PML state of each face (27 fields), pointwise box of 9 fields
+  // the same for the 16 x 16 strip tiles (halo box 24 x 20)
+  CUtensorMap win_s, w0_s, t_s, plane_s, auxy_s[2];
 };
 // Per-context state of the tiled kernels: maps of the four volume buffers, of the metric
 // and of the PML state (fixed addresses, encoded once), the error flag, the SM count.
@@ -203,6 +206,7 @@ struct TileCtx {
   CUtensorMap centre[4];
   CUtensorMap plane;
   CUtensorMap aux[6];
+  CUtensorMap halo_s[4], centre_s[4], plane_s, auxy_s[2];  // strip tiles
   int* err = nullptr;
   int* sched = nullptr;  // unit counter and finished-CTA counter (zero between launches)
   int nsm = 0;
@@ -210,17 +214,23 @@ struct TileCtx {
 };
 bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, float* const aux[6], int* err,
                 int* sched, int device);
-// Units of a tiled kernel: tile columns (32 y x 8 z) times chunks of x planes.
-//   interior kernel: the tiles of the box lo..hi;
-//   PML kernel: over the nodes below the free-surface rows (k < ktop) outside the
-//   interior kernel's tile rectangle [tja, tjb) x [tka, tkb) (tile indices of the frame
-//   starting at j = 0, k = 0): every tile of the x slabs [0, nx1) and [ni - nx2, ni), then
-//   in chunks of ci planes over [nx1, ni - nx2) the nedge tiles outside the rectangle.
+// every map the tiled kernels read at a stage whose stencil input is buffer `bin`
+TileMaps tile_maps(const TileCtx& tc, int bin);
+// Units of a tiled kernel: tile columns times chunks of x planes.
+//   interior kernel: the 32 x 8 tiles of the box lo..hi (the last ones partial);
+//   PML kernel: the nodes below the free-surface rows (k < ktop) outside the interior
+//   box [nx1, ni - nx2) x [ya, yb) x [za, zb): every 32 x 8 tile of the two x slabs
+//   (frame at j = 0, k = 0), then in chunks of ci planes over [nx1, ni - nx2) the nedge
+//   tiles of the edges: the 16 x 16 strip tiles of the y slabs, ny1 strips from j = 0
+//   and ny2 from j = yb, each over the nrs strip rows of [0, ktop); the 32 x 8 tiles of
+//   the z slabs, ntz tiles from j = ya over the nz1 tile rows from k = 0 (below za) and
+//   the nz2 tile rows from k = zb (up to ktop).
 struct TileSched {
   int lo_x, lo_y, lo_z, hi_x, hi_y, hi_z;  // tiled box, interior indices, half open
   int ntj, ntk, ci, nunits;               // tiles in y and z, planes per chunk, units
-  int tja, tjb, tka, tkb;                 // PML kernel: the interior kernel's tile rectangle
   int nx1, nx2, ktop, nedge;              // PML kernel: x slab widths, top row bound, edge tiles
+  int ya, yb, za, zb;                     // PML kernel: the interior box in y and z
+  int ny1, ny2, nrs, ntz, nz1, nz2;       // PML kernel: edge tile counts
 };
 // Values of one scenario of a batched (ensemble) launch of the tiled kernel that the
 // computing warps read; a CTA copies them into shared memory with each unit's planes.
@@ -257,8 +267,8 @@ struct VolPlan {
 VolPlan plan_volume(const VolArgs& a, const TileCtx* tc);
 bool tile_feasible(const TileCtx* tc, const VolArgs& a, int3 lo, int3 hi);
 TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid);
-// units of the PML kernel around the interior tile rectangle (dfd_pml.cu)
-TileSched pml_plan(const VolArgs& a, int tja, int tjb, int tka, int tkb, int ktop, int nsm, int* grid);
+// units of the PML kernel around the interior box (dfd_pml.cu)
+TileSched pml_plan(const VolArgs& a, int ya, int yb, int za, int zb, int ktop, int nsm, int* grid);
 bool pml_setup();
 void launch_pml(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, const TileSched& ps, int grid,
                 cudaStream_t s);

@@ -2,13 +2,14 @@
 // not take, staged through shared memory by TMA: the PML slabs of all six faces and the
 // nodes that fill their tiles (the interior kernel takes whole tiles only).
 //
-// The tiles are those of the interior kernel (32 y x 8 z, frame starting at j = 0,
-// k = 0).  Units (dfd_internal.cuh, TileSched): every tile of the two x slabs, one unit
-// per slab; then, in chunks of x planes between the slabs, the tiles outside the interior
-// kernel's rectangle.  Each unit stages, per plane, the stencil input with its halo, the
-// RK registers and the ADE state of one PML face (its "own" face: x for the x slabs, else
-// y, else z); a node that also lies in another face (edges and corners of the slabs)
-// reads that face's state from global memory.  One computing warp per row of nodes
+// Units (dfd_internal.cuh, TileSched): every 32 x 8 tile of the two x slabs, one unit
+// per tile and slab; then, in chunks of x planes between the slabs, the 16 x 16 strip
+// tiles of the y slabs (a y slab is 12 to 20 nodes wide: a 32-wide tile would leave most
+// lanes without a PML node) and the 32 x 8 tiles of the z slabs.  Each unit stages, per
+// plane, the stencil input with its halo, the RK registers and the ADE state of one PML
+// face (its "own" face: x for the x slabs, y for the strips, z for the z tiles); a node
+// that also lies in another face (edges and corners of the slabs) reads that face's
+// state from global memory.  One computing warp per row of nodes
 // integrates all nine fields and their PML state.
 //
 // Right-hand side with the ADE CFS-PML as in the reference's wave.cu:8-204 and
@@ -31,50 +32,61 @@ static_assert(PML_SMEM <= 232448, "PML ring exceeds the shared memory of one CTA
 static_assert((PSLOT_M * 4) % 128 == 0, "slot alignment");
 }  // namespace
 
-// tile origin, x range and own face (-1: none) of local unit lu
+// tile origin, x range, own face (-1: none), node bounds (j < jhi, k < khi) and shape
+// (strip: 16 x 16, else 32 x 8) of local unit lu
 struct PmlUnit {
-  int j0, k0, ib, ie, face;
+  int j0, k0, ib, ie, face, jhi, khi;
+  bool strip;
 };
 __device__ __forceinline__ PmlUnit pml_unit(const TileSched& sc, const VolArgs& a, int lu) {
   const Dims& d = a.d;
   PmlUnit r;
+  r.strip = false;
   const int ntile = sc.ntj * sc.ntk;
-  int tj, tk;
-  if (sc.nx1 > 0 && lu < ntile) {
-    tj = lu % sc.ntj; tk = lu / sc.ntj;
-    r.ib = 0; r.ie = sc.nx1; r.face = 0;
-  } else {
-    if (sc.nx1 > 0) lu -= ntile;
-    if (sc.nx2 > 0 && lu < ntile) {
-      tj = lu % sc.ntj; tk = lu / sc.ntj;
-      r.ib = d.ni - sc.nx2; r.ie = d.ni; r.face = 1;
-    } else {
-      if (sc.nx2 > 0) lu -= ntile;
-      const int c = lu / sc.nedge, e = lu % sc.nedge;
-      r.ib = sc.nx1 + c * sc.ci;
-      r.ie = min(r.ib + sc.ci, d.ni - sc.nx2);
-      // edge tile e: the full rows below the rectangle, the two sides of it, the full rows above
-      const int below = sc.tka * sc.ntj, side = sc.tja + (sc.ntj - sc.tjb), mid = (sc.tkb - sc.tka) * side;
-      if (e < below) {
-        tk = e / sc.ntj; tj = e % sc.ntj;
-      } else if (e < below + mid) {
-        const int m = e - below, rr = m % side;
-        tk = sc.tka + m / side;
-        tj = rr < sc.tja ? rr : sc.tjb + (rr - sc.tja);
-      } else {
-        const int m = e - below - mid;
-        tk = sc.tkb + m / sc.ntj; tj = m % sc.ntj;
-      }
-      const int j0 = tj * TJ, k0 = tk * TK;
-      r.face = (a.aux[2] && j0 < d.N) ? 2
-               : (a.aux[3] && j0 + TJ > d.nj - d.N) ? 3
-               : (a.aux[4] && k0 < d.N) ? 4
-               : (a.aux[5] && k0 + TK > d.nk - d.N) ? 5
-               : -1;
-    }
+  if ((sc.nx1 > 0 && lu < ntile) || (sc.nx2 > 0 && lu < ntile + (sc.nx1 > 0 ? ntile : 0))) {
+    // a tile of an x slab
+    const bool second = !(sc.nx1 > 0 && lu < ntile);
+    if (second && sc.nx1 > 0) lu -= ntile;
+    r.j0 = (lu % sc.ntj) * TJ;
+    r.k0 = (lu / sc.ntj) * TK;
+    r.ib = second ? d.ni - sc.nx2 : 0;
+    r.ie = second ? d.ni : sc.nx1;
+    r.face = second ? 1 : 0;
+    r.jhi = d.nj;
+    r.khi = sc.ktop;
+    return r;
   }
-  r.j0 = tj * TJ;
-  r.k0 = tk * TK;
+  if (sc.nx1 > 0) lu -= ntile;
+  if (sc.nx2 > 0) lu -= ntile;
+  const int c = lu / sc.nedge;
+  int e = lu % sc.nedge;
+  r.ib = sc.nx1 + c * sc.ci;
+  r.ie = min(r.ib + sc.ci, d.ni - sc.nx2);
+  const int ns = sc.ny1 + sc.ny2;
+  if (e < ns * sc.nrs) {
+    // a strip tile of a y slab
+    const int st = e % ns;
+    r.strip = true;
+    r.j0 = st < sc.ny1 ? st * STRIP : sc.yb + (st - sc.ny1) * STRIP;
+    r.k0 = (e / ns) * STRIP;
+    r.jhi = d.nj;
+    r.khi = sc.ktop;
+    r.face = (a.aux[2] && r.j0 < d.N) ? 2 : (a.aux[3] && r.j0 + STRIP > d.nj - d.N) ? 3 : -1;
+    return r;
+  }
+  // a tile of a z slab
+  e -= ns * sc.nrs;
+  const int zt = e % sc.ntz, zr = e / sc.ntz;
+  r.j0 = sc.ya + zt * TJ;
+  r.jhi = sc.yb;
+  if (zr < sc.nz1) {
+    r.k0 = zr * TK;
+    r.khi = sc.za;
+  } else {
+    r.k0 = sc.zb + (zr - sc.nz1) * TK;
+    r.khi = sc.ktop;
+  }
+  r.face = (a.aux[4] && r.k0 < d.N) ? 4 : (a.aux[5] && r.k0 + TK > d.nk - d.N) ? 5 : -1;
   return r;
 }
 
@@ -179,10 +191,17 @@ __device__ __forceinline__ void role_terms(const float* dv, float e0, float e1, 
 
 // One node, all nine fields: the three axes with their 1/beta, the ADE state of the faces
 // the node lies in (fx, fy, fz; -1: none; own: the staged face, read from A), the RK4
-// store.  g: separable metric (xi = (1, U, V)/a(x), eta = (0, ety, etz), zeta = (0, zty,
+// store.  PW: row pitch of the stencil box (40 for 32 x 8 tiles, 24 for strips).  g: separable metric (xi = (1, U, V)/a(x), eta = (0, ety, etz), zeta = (0, zty,
 // ztz)) and media.
+// one-sided 5-point operator along a shared-memory line with a runtime stride
+template <int F>
+__device__ __forceinline__ float d5r(const float* p, int S) {
+  if (F == 1) return d5v<1>(p[-S], p[0], p[S], p[2 * S], p[3 * S]);
+  else return d5v<-1>(p[-3 * S], p[-2 * S], p[-S], p[0], p[S]);
+}
+
 template <int FX, int FY, int FZ>
-__device__ __forceinline__ void pml_node(const VolArgs& a, const float* x0, const float* x1, const float* x2,
+__device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* x0, const float* x1, const float* x2,
                                          const float* x3, const float* x4, const float* cur, const NodeMetric& g,
                                          int i, int j, int k, int fx, int fy, int fz, int own, const float* A,
                                          long long q, const float* P, float damp) {
@@ -232,7 +251,7 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, const float* x0, cons
   // z
   {
 #pragma unroll
-    for (int f = 0; f < 9; f++) dv[f] = d5s<FZ, HW>(cur + f * HBOX) * r;
+    for (int f = 0; f < 9; f++) dv[f] = d5r<FZ>(cur + f * HBOX, PW) * r;
     role_terms<0, false>(dv + 3, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D);
     role_terms<3, false>(dv, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D + 3);
     role_terms<6, false>(dv, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D + 6);
@@ -325,6 +344,11 @@ __global__ void __maxnreg__(168)
       if (pu.face == 3) ac0 = cp0 - d.yb3;
       if (pu.face == 4) ac1 = pu.k0;
       if (pu.face == 5) ac1 = pu.k0 - (d.nk - d.N);
+      // the unit's maps: 32 x 8 tiles or 16 x 16 strips (same box sizes in floats)
+      const CUtensorMap* m_win = pu.strip ? &mp.win_s : &mp.win;
+      const CUtensorMap* m_w0 = pu.strip ? &mp.w0_s : &mp.w0;
+      const CUtensorMap* m_t = pu.strip ? &mp.t_s : &mp.t;
+      const CUtensorMap* m_aux = pu.face < 0 ? nullptr : pu.strip ? &mp.auxy_s[pu.face - 2] : &mp.aux[pu.face];
       qunit[qr.slot] = u;
       if (BATCH) {
         mbar_expect_tx(full_q + qr.slot, QSLOT * 4 + (unsigned)sizeof(TileUnit));
@@ -332,13 +356,13 @@ __global__ void __maxnreg__(168)
       } else {
         mbar_expect_tx(full_q + qr.slot, QSLOT * 4);
       }
-      tma_load3(qs + qr.slot * QSLOT, &mp.plane, cp0, cp1, 0, full_q + qr.slot);
+      tma_load3(qs + qr.slot * QSLOT, pu.strip ? &mp.plane_s : &mp.plane, cp0, cp1, 0, full_q + qr.slot);
       qr.next<MQ>();
       qcount++;
       for (int m = 0; m < nst + 4 && ok; m++) {
         if (wcount >= MS && !(ok = mbar_wait(empty_w + wr.slot, wr.phase ^ 1))) break;
         mbar_expect_tx(full_w + wr.slot, HSLOT * 4);
-        tma_load4(win + wr.slot * HSLOT, &mp.win, cw0, cw1, pu.ib + XLO + m + 3, 0, full_w + wr.slot);
+        tma_load4(win + wr.slot * HSLOT, m_win, cw0, cw1, pu.ib + XLO + m + 3, 0, full_w + wr.slot);
         wr.next<MS>();
         wcount++;
         if (m < 4 || !usep) continue;
@@ -347,9 +371,9 @@ __global__ void __maxnreg__(168)
         float* dst = pw + pr.slot * PSLOT_M;
         const int i = pu.ib + (m - 4);
         mbar_expect_tx(b, ptx);
-        if (needW0) tma_load4(dst, &mp.w0, cp0, cp1, i + 3, 0, b);
-        if (needT) tma_load4(dst + 9 * PB, &mp.t, cp0, cp1, i + 3, 0, b);
-        for (int fb = 0; fb < na; fb += 9) tma_load4(dst + (18 + fb) * PB, &mp.aux[pu.face], ac0, ac1, i - aoff, fb, b);
+        if (needW0) tma_load4(dst, m_w0, cp0, cp1, i + 3, 0, b);
+        if (needT) tma_load4(dst + 9 * PB, m_t, cp0, cp1, i + 3, 0, b);
+        for (int fb = 0; fb < na; fb += 9) tma_load4(dst + (18 + fb) * PB, m_aux, ac0, ac1, i - aoff, fb, b);
         pr.next<MP>();
         pcount++;
       }
@@ -368,10 +392,11 @@ __global__ void __maxnreg__(168)
     return;
   }
 
-  // ---------------- computing warps
-  const int ty = warp;
-  const int hc = (ty + RZ) * HW + lane + 4;
-  const int pc = ty * TJ + lane;
+  // ---------------- computing warps.  32 x 8 tiles: warp = row, lane = column.  16 x 16
+  // strips: the two half-warps take rows two apart (their stencil rows then fall on
+  // disjoint shared-memory banks), lane & 15 the column.
+  const int hl = lane >> 4, jl = lane & 15;
+  const int srow = (warp >> 1) * 4 + (warp & 1) + 2 * hl;
   Ring wr, pr, qr;
   int sb = 0;
   for (;;) {
@@ -386,8 +411,11 @@ __global__ void __maxnreg__(168)
     const TileSched& sc = BATCH ? ua.sc : sc0;
     const Dims& d = a.d;
     const PmlUnit pu = pml_unit(sc, a, BATCH ? u - ua.unit0 : u);
-    const int j = pu.j0 + lane, k = pu.k0 + ty;
-    const bool active = j < d.nj && k < sc.ktop;
+    const int row = pu.strip ? srow : warp, col = pu.strip ? jl : lane;
+    const int hc = pu.strip ? (row + RZ) * (STRIP + 8) + col + 4 : (row + RZ) * HW + col + 4;
+    const int pc = pu.strip ? row * STRIP + col : row * TJ + col;
+    const int j = pu.j0 + col, k = pu.k0 + row;
+    const bool active = j < pu.jhi && k < pu.khi;
     const bool band = active && a.united && !a.united[j + k * d.nj];
     const int fy = (a.aux[2] && j < d.N) ? 2 : (a.aux[3] && j >= d.nj - d.N) ? 3 : -1;
     const int fz = (a.aux[4] && k < d.N) ? 4 : (a.aux[5] && k >= d.nk - d.N) ? 5 : -1;
@@ -433,8 +461,10 @@ __global__ void __maxnreg__(168)
         g.lam = Q[side * PB]; g.mu = Q[(side + 1) * PB]; g.rrho = 1.0f / Q[(side + 2) * PB];
         const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
         const long long q = qyz + (long long)(i + 3) * d.sx;
-        if (pml) {
-          pml_node<FX, FY, FZ>(a, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face, P + 18 * PB, q, P, damp);
+        if (pu.strip || pml) {
+          // (strips hold y-slab nodes and the few interior columns beside them)
+          pml_node<FX, FY, FZ>(a, pu.strip ? STRIP + 8 : HW, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face,
+                               P + 18 * PB, q, P, damp);
         } else {
           float hv[9];
           lean_velocity<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);
@@ -476,26 +506,35 @@ bool pml_setup() {
          pml_smem<1, -1, -1>() && pml_smem<1, -1, 1>() && pml_smem<1, 1, -1>() && pml_smem<1, 1, 1>();
 }
 
-// Units around the interior tile rectangle [tja, tjb) x [tka, tkb) (empty: tja == tjb):
-// the x slabs whole, the middle x range in chunks chosen as in tile_plan.  nunits 0 when
-// there is nothing to do, -1 when the slabs overlap (the general kernel then takes all).
-TileSched pml_plan(const VolArgs& a, int tja, int tjb, int tka, int tkb, int ktop, int nsm, int* grid) {
+// Units around the interior box [nx1, ni - nx2) x [ya, yb) x [za, zb): the x slabs
+// whole, then the y strips and z tiles of the middle x range in chunks chosen as in
+// tile_plan.  ya is a multiple of 16 (the y1 strips end there), yb a multiple of 4 (the
+// y2 strips start there); ya == yb: no interior columns, the strips take every column
+// from 0; za == zb: no interior rows, the z tiles take every row from 0.  nunits 0 when
+// there is nothing to do, -1 when the x slabs overlap (the general kernel then takes all).
+TileSched pml_plan(const VolArgs& a, int ya, int yb, int za, int zb, int ktop, int nsm, int* grid) {
   const Dims& d = a.d;
   TileSched s;
   memset(&s, 0, sizeof s);
   s.ntj = (d.nj + TJ - 1) / TJ;
   s.ntk = (ktop + TK - 1) / TK;
-  s.tja = tja; s.tjb = tjb; s.tka = tka; s.tkb = tkb;
   s.nx1 = a.aux[0] ? d.N : 0;
   s.nx2 = a.aux[1] ? d.N : 0;
   s.ktop = ktop;
+  s.ya = ya; s.yb = yb; s.za = za; s.zb = zb;
   *grid = 0;
   if (s.nx1 + s.nx2 > d.ni || ktop <= 0) {
     s.nunits = -1;
     return s;
   }
+  s.ny1 = ya / STRIP;
+  s.ny2 = (d.nj - yb + STRIP - 1) / STRIP;
+  s.nrs = (ktop + STRIP - 1) / STRIP;
+  s.ntz = (yb - ya + TJ - 1) / TJ;
+  s.nz1 = (za + TK - 1) / TK;
+  s.nz2 = (ktop - zb + TK - 1) / TK;
+  s.nedge = (s.ny1 + s.ny2) * s.nrs + s.ntz * (s.nz1 + s.nz2);
   const int ntile = s.ntj * s.ntk;
-  s.nedge = ntile - (tjb - tja) * (tkb - tka);
   const int slab = (s.nx1 > 0 ? ntile : 0) + (s.nx2 > 0 ? ntile : 0);
   const int nxm = d.ni - s.nx1 - s.nx2;
   s.ci = std::max(nxm, 1);
@@ -517,12 +556,7 @@ TileSched pml_plan(const VolArgs& a, int tja, int tjb, int tka, int tkb, int kto
 
 template <int FX, int FY, int FZ>
 static void launch_p(const TileCtx& tc, const VolArgs& a, int bin, const TileSched& ps, int grid, cudaStream_t s) {
-  TileMaps mp;
-  mp.win = tc.halo[bin];
-  mp.w0 = tc.centre[0];
-  mp.t = tc.centre[3];
-  mp.plane = tc.plane;
-  for (int f = 0; f < 6; f++) mp.aux[f] = tc.aux[f];
+  const TileMaps mp = tile_maps(tc, bin);
   volume_pml_kernel<FX, FY, FZ, false>
       <<<grid, PTOT, PML_SMEM, s>>>(mp, a, ps, nullptr, 1, ps.nunits, tc.err, tc.sched);
 }

@@ -176,7 +176,6 @@ __global__ void __maxnreg__(96)
     const TileSched& sc = BATCH ? ua.sc : sc0;
     const Dims& d = a.d;
     const long long n = d.nxyz;
-    const float r = a.rDH;
     const int lu = BATCH ? u - ua.unit0 : u;
     const int ntile = sc.ntj * sc.ntk;
     const int tc = lu / ntile, ru = lu % ntile;
@@ -288,13 +287,13 @@ static bool set_smem() {
          one((const void*)volume_tile_kernel<FX, FY, FZ, true>);
 }
 
-// 3-D map over the 12 metric / media planes (py, nz, 12) with box (32, 8, 12)
-static bool make_plane_map(CUtensorMap* m, const Dims& d, const float* base) {
+// 3-D map over the 12 metric / media planes (py, nz, 12) with box (bw, bh, 12)
+static bool make_plane_map(CUtensorMap* m, const Dims& d, const float* base, int bw, int bh) {
   auto fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[3] = {(cuuint64_t)d.py, (cuuint64_t)d.nz, 12};
   cuuint64_t strides[2] = {(cuuint64_t)d.py * 4, (cuuint64_t)d.py * d.nz * 4};
-  cuuint32_t box[3] = {(cuuint32_t)TJ, (cuuint32_t)TK, 12};
+  cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 12};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -303,8 +302,8 @@ static bool make_plane_map(CUtensorMap* m, const Dims& d, const float* base) {
 }
 
 // 4-D map over the 27-field PML state of face f (columns, rows, planes, fields; the
-// layouts of pml_index) with box (32, 8, 1, 9)
-static bool make_aux_map(CUtensorMap* m, const Dims& d, int f, const float* base) {
+// layouts of pml_index) with box (bw, bh, 1, 9)
+static bool make_aux_map(CUtensorMap* m, const Dims& d, int f, const float* base, int bw, int bh) {
   auto fn = encode_fn();
   if (!fn) return false;
   cuuint64_t w = f < 2 ? d.py : f < 4 ? d.wy : d.py;
@@ -312,7 +311,7 @@ static bool make_aux_map(CUtensorMap* m, const Dims& d, int f, const float* base
   cuuint64_t planes = f < 2 ? d.N : d.ni;
   cuuint64_t dims[4] = {w, rows, planes, 27};
   cuuint64_t strides[3] = {w * 4, w * rows * 4, (cuuint64_t)pml_fstride(d, f) * 4};
-  cuuint32_t box[4] = {(cuuint32_t)TJ, (cuuint32_t)TK, 1, 9};
+  cuuint32_t box[4] = {(cuuint32_t)bw, (cuuint32_t)bh, 1, 9};
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -330,11 +329,19 @@ bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* plan
   for (int b = 0; b < 4 && ok; b++) {
     ok = make_map(&tc->halo[b], d, W[b], 9, HW, HH, 9);
     ok = ok && make_map(&tc->centre[b], d, W[b], 9, TJ, TK, 9);
+    // strip tiles of the PML kernel: 16 x 16 nodes, halo box 24 x 20
+    ok = ok && make_map(&tc->halo_s[b], d, W[b], 9, STRIP + 8, STRIP + 4, 9);
+    ok = ok && make_map(&tc->centre_s[b], d, W[b], 9, STRIP, STRIP, 9);
   }
-  ok = ok && make_plane_map(&tc->plane, d, planes);
+  ok = ok && make_plane_map(&tc->plane, d, planes, TJ, TK);
+  ok = ok && make_plane_map(&tc->plane_s, d, planes, STRIP, STRIP);
   for (int f = 0; f < 6 && ok; f++) {
     memset(&tc->aux[f], 0, sizeof(CUtensorMap));
-    if (aux[f]) ok = make_aux_map(&tc->aux[f], d, f, aux[f]);
+    if (aux[f]) ok = make_aux_map(&tc->aux[f], d, f, aux[f], TJ, TK);
+  }
+  for (int f = 2; f < 4 && ok; f++) {
+    memset(&tc->auxy_s[f - 2], 0, sizeof(CUtensorMap));
+    if (aux[f]) ok = make_aux_map(&tc->auxy_s[f - 2], d, f, aux[f], STRIP, STRIP);
   }
   ok = ok && set_smem<-1, -1, -1>() && set_smem<-1, -1, 1>() && set_smem<-1, 1, -1>() && set_smem<-1, 1, 1>();
   ok = ok && set_smem<1, -1, -1>() && set_smem<1, -1, 1>() && set_smem<1, 1, -1>() && set_smem<1, 1, 1>();
@@ -365,14 +372,26 @@ TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid) {
   return s;
 }
 
-template <int FX, int FY, int FZ>
-static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
+TileMaps tile_maps(const TileCtx& tc, int bin) {
   TileMaps mp;
   memset(&mp, 0, sizeof mp);
   mp.win = tc.halo[bin];
   mp.w0 = tc.centre[0];
   mp.t = tc.centre[3];
   mp.plane = tc.plane;
+  for (int f = 0; f < 6; f++) mp.aux[f] = tc.aux[f];
+  mp.win_s = tc.halo_s[bin];
+  mp.w0_s = tc.centre_s[0];
+  mp.t_s = tc.centre_s[3];
+  mp.plane_s = tc.plane_s;
+  mp.auxy_s[0] = tc.auxy_s[0];
+  mp.auxy_s[1] = tc.auxy_s[1];
+  return mp;
+}
+
+template <int FX, int FY, int FZ>
+static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
+  const TileMaps mp = tile_maps(tc, bin);
   int grid = 0;
   TileSched sc = tile_plan(lo, hi, tc.nsm, &grid);
   volume_tile_kernel<FX, FY, FZ, false>

@@ -143,13 +143,14 @@ struct NodeMetric {
 // Lean right-hand side of a node outside every PML slab and below the free-surface rows
 // (rB = 1, no ADE state): momentum (velocity rates, hv[0..2]) and constitutive law (stress
 // rates, hv[3..8]) from the one-sided derivatives on the shared-memory stencil planes
-// (xs0..xs4 the five x planes, cur the node's plane).  The x row of the metric has three
+// (xs0..xs4 the five x planes, cur the node's plane, PW the row pitch of the stencil box).
+// The x row of the metric has three
 // components; the y and z rows have no x component, so the terms with it (exact zeros)
 // and the derivative of Txx along y and z drop out.  Reference wave.cu:8-204.
 #define DFD_DERX(f) d5v<FX>(xs0[(f) * HBOX], xs1[(f) * HBOX], xs2[(f) * HBOX], xs3[(f) * HBOX], xs4[(f) * HBOX])
 #define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HBOX)
-#define DFD_DERZ(f) d5s<FZ, HW>(cur + (f) * HBOX)
-template <int FX, int FY, int FZ>
+#define DFD_DERZ(f) d5s<FZ, PW>(cur + (f) * HBOX)
+template <int FX, int FY, int FZ, int PW = HW>
 __device__ __forceinline__ void lean_velocity(const float* xs0, const float* xs1, const float* xs2, const float* xs3,
                                               const float* xs4, const float* cur, const NodeMetric& g, float r,
                                               float* hv) {
@@ -181,7 +182,7 @@ __device__ __forceinline__ void lean_velocity(const float* xs0, const float* xs1
 #undef DFD_VAXIS0
   hv[0] = h0; hv[1] = h1; hv[2] = h2;
 }
-template <int FX, int FY, int FZ>
+template <int FX, int FY, int FZ, int PW = HW>
 __device__ __forceinline__ void lean_stress(const float* xs0, const float* xs1, const float* xs2, const float* xs3,
                                             const float* xs4, const float* cur, const NodeMetric& g, float r,
                                             float* hv) {

@@ -330,19 +330,24 @@ VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
   const int ktop = a.freenode ? d.nk - 3 : d.nk;
   bool done = false;
   if (tc && tc->ok) {
-    // the interior kernel takes the whole tiles (frame at j = 0, k = 0) inside the interior
-    // box; the PML kernel every other node below the free-surface rows
-    int tja = (lo.y + TILE_J - 1) / TILE_J, tjb = hi.y / TILE_J;
-    int tka = (lo.z + TILE_K - 1) / TILE_K, tkb = hi.z / TILE_K;
-    if (tja >= tjb || tka >= tkb || lo.x >= hi.x) tja = tjb = tka = tkb = 0;
+    // the interior kernel takes the box between the slabs (its y start a multiple of 16,
+    // where the PML kernel's y1 strips end; its y end a multiple of 4, where the y2
+    // strips start); the PML kernel every other node below the free-surface rows
+    int ya = a.aux[2] ? (d.N + STRIP - 1) / STRIP * STRIP : 0;
+    int yb = a.aux[3] ? (d.nj - d.N) / 4 * 4 : d.nj;
+    int za = a.aux[4] ? d.N : 0;
+    int zb = a.aux[5] ? d.nk - d.N : ktop;
+    if (yb <= ya) ya = yb = 0;     // no interior column: strips over every column
+    if (zb <= za) za = zb = ktop;  // no interior row: z tiles over every row
     int grid = 0;
-    TileSched ps = pml_plan(a, tja, tjb, tka, tkb, ktop, tc->nsm, &grid);
-    const int3 rlo = make_int3(lo.x, tja * TILE_J, tka * TILE_K), rhi = make_int3(hi.x, tjb * TILE_J, tkb * TILE_K);
-    if (ps.nunits >= 0 && (tja == tjb || tile_feasible(tc, a, rlo, rhi))) {
+    TileSched ps = pml_plan(a, ya, yb, za, zb, ktop, tc->nsm, &grid);
+    const int3 rlo = make_int3(lo.x, ya, za), rhi = make_int3(hi.x, yb, zb);
+    const bool inner = rhi.x > rlo.x && rhi.y > rlo.y && rhi.z > rlo.z;
+    if (ps.nunits >= 0 && (!inner || tile_feasible(tc, a, rlo, rhi))) {
       done = true;
       pl.ps = ps;
       pl.pgrid = grid;
-      if (tja < tjb) {
+      if (inner) {
         pl.tiled = true;
         pl.lo = rlo;
         pl.hi = rhi;
