@@ -210,6 +210,7 @@ def lib():
             "dfd_output_open": [V, ctypes.c_char_p], "dfd_output_write": [V, I], "dfd_output_close": [V],
             "dfd_set_guess_net": [V, V, I], "dfd_fetch_outputs": [V, V],
             "dfd_run_timed": [V, I, I, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)],
+            "dfd_run_graph_timed": [V, I, I, P(ctypes.c_float)],
             "dfd_interior_stats": [V, P(ctypes.c_float), P(ctypes.c_longlong)],
             "dfd_ens_create": [V, I, P(ctypes.c_void_p)], "dfd_ens_destroy": [V], "dfd_ens_run": [V, I, I],
             "dfd_ens_synchronize": [V], "dfd_ens_run_timed": [V, I, I, P(ctypes.c_float)],
@@ -372,6 +373,12 @@ class Simulation:
         t, v, f = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         self._check(lib().dfd_run_timed(self.h, it0, nsteps, ctypes.byref(t), ctypes.byref(v), ctypes.byref(f)))
         return t.value, v.value, f.value
+
+    def run_graph_timed(self, it0, nsteps):
+        """Replay nsteps steps from the CUDA graphs (all built beforehand); device time in ms."""
+        ms = ctypes.c_float()
+        self._check(lib().dfd_run_graph_timed(self.h, it0, nsteps, ctypes.byref(ms)))
+        return ms.value
 
     def interior_stats(self):
         """(ms, nodes): interior-kernel device time of the last run_timed and nodes per stage."""

@@ -95,6 +95,8 @@ struct dfd_ctx {
   long long interior_nodes = 0;   // nodes the interior kernel updates per stage
   long long n_band_columns = 0;   // non-united (j, k) fault columns
   std::vector<int> united_h;      // (NZ, NY) host copy of the united plane
+  int inodes_box[6] = {0, 0, 0, 0, 0, 0};  // box of the cached interior node count
+  long long inodes_cached = -1;
   float interior_ms = 0;          // interior kernel time of the last dfd_run_timed
   float node_ms = 0;              // fault node kernel time of the last dfd_run_timed
   // host-side inputs
@@ -442,6 +444,7 @@ int dfd_precompute(dfd_ctx* ctx) {
     ctx->n_band_columns = 0;
     for (int v : h.united) ctx->n_band_columns += v == 0;
     ctx->united_h = h.united;
+    ctx->inodes_cached = -1;
     for (auto& u : iup)
       CK(cudaMemcpyAsync(ctx->ipl + u.plane * nf, u.v->data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s));
     for (int b = 0; b < 2; b++) CK(cudaMemsetAsync(ctx->FW[b], 0, sizeof(float) * 18 * d.nyz, s));
@@ -556,8 +559,10 @@ static VolArgs vol_args(dfd_ctx* ctx, int pattern, int irk) {
 }
 
 // nodes the interior kernel updates in a stage: its box less the fault-band nodes in it
-static long long interior_nodes(const dfd_ctx* ctx, const VolPlan& pl) {
+static long long interior_nodes(dfd_ctx* ctx, const VolPlan& pl) {
   if (!(pl.tiled || pl.plain)) return 0;
+  const int box[6] = {pl.lo.x, pl.lo.y, pl.lo.z, pl.hi.x, pl.hi.y, pl.hi.z};
+  if (ctx->inodes_cached >= 0 && std::equal(box, box + 6, ctx->inodes_box)) return ctx->inodes_cached;
   long long n = pl.nodes;
   const Dims& d = ctx->d;
   if (ctx->p.rupture && !ctx->united_h.empty() && pl.lo.x + 3 <= d.i0 + 3 && pl.hi.x + 3 > d.i0 - 3) {
@@ -567,6 +572,8 @@ static long long interior_nodes(const dfd_ctx* ctx, const VolPlan& pl) {
     const int x0 = std::max(pl.lo.x + 3, d.i0 - 3), x1 = std::min(pl.hi.x + 3, d.i0 + 4);
     n -= cols * std::max(0, x1 - x0);
   }
+  std::copy(box, box + 6, ctx->inodes_box);
+  ctx->inodes_cached = n;
   return n;
 }
 
@@ -664,6 +671,33 @@ int dfd_run(dfd_ctx* ctx, int it0, int nsteps) {
 }
 
 int dfd_step(dfd_ctx* ctx, int it) { return dfd_run(ctx, it, 1); }
+
+static int tile_status(dfd_ctx* ctx);
+
+int dfd_run_graph_timed(dfd_ctx* ctx, int it0, int nsteps, float* ms) {
+  if (!ctx || !ms || nsteps < 1) return DFD_ERR_PARAM;
+  if (ctx->sticky) return ctx->sticky;
+  if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
+  if (ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "a step is half done (dfd_stage)");
+  cudaSetDevice(ctx->device);
+  for (int pat = 0; pat < 8; pat++)
+    if (!ctx->graph[pat]) {
+      int r = build_graph(ctx, pat);
+      if (r) return r;
+    }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, ctx->s0));
+  int r = dfd_run(ctx, it0, nsteps);
+  CK(cudaEventRecord(e1, ctx->s0));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  return tile_status(ctx);
+}
 
 // error flag of the tiled interior kernel (a TMA copy that did not complete in time)
 static int tile_status(dfd_ctx* ctx) {

@@ -125,6 +125,11 @@ int dfd_fetch_outputs(dfd_ctx *ctx, float *host);
 /* nsteps steps issued stage by stage with CUDA events around every volume-kernel launch:
  * total device time, time inside the volume kernels, and the rest (milliseconds) */
 int dfd_run_timed(dfd_ctx *ctx, int it0, int nsteps, float *total_ms, float *volume_ms, float *fault_ms);
+/* dfd_run with its device time: the graphs of all eight flag patterns are built first,
+ * then nsteps steps are replayed between two CUDA events on the context's stream; *ms is
+ * their elapsed time (a measurement aid for the production path, which dfd_run_timed's
+ * per-kernel events perturb) */
+int dfd_run_graph_timed(dfd_ctx *ctx, int it0, int nsteps, float *ms);
 /* device time spent in the interior (TMA-tiled) volume kernel during the last
  * dfd_run_timed (CUDA events on its stream, summed over all stages), and the nodes that
  * kernel updates per stage (the interior box minus the fault band); a measurement aid
