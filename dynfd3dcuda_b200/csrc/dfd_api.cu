@@ -14,7 +14,8 @@
 
 namespace dfd {
 long long launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
-                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out);
+                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out,
+                              cudaEvent_t* fork);
 void launch_fault_node(const FaultArgs& a, cudaStream_t s);
 void launch_fault_band(const FaultArgs& a, cudaStream_t s);
 void launch_fault_coef(const Dims& d, const float* M, float* tab, float* tabf, float* vecn, float* vecs1,
@@ -593,13 +594,17 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   }
   if (vb) cudaEventRecord(*vb, ctx->s0);
   if (ctx->serial) {
-    // one stream: interior kernel, shell kernel, fault band
+    // interior and PML kernels on s0; then the general kernel (free-surface rows) on s2
+    // beside the fault band kernel on s0: two small latency-bound kernels that fit on the
+    // SMs together
     VolArgs va = vol_args(ctx, pattern, irk);
     VolPlan pl;
-    launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s0, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke,
-                        &pl);
+    launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke,
+                        &pl, &ctx->ev_fork);
     ctx->interior_nodes = interior_nodes(ctx, pl);
+    cudaEventRecord(ctx->ev_join2, ctx->s2);
     if (p.rupture) launch_fault_band(fa, ctx->s0);
+    cudaStreamWaitEvent(ctx->s0, ctx->ev_join2, 0);
     if (ve) cudaEventRecord(*ve, ctx->s0);
     return cuda_check(ctx, cudaGetLastError(), "stage launch");
   }
@@ -613,7 +618,8 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
   VolArgs va = vol_args(ctx, pattern, irk);
   VolPlan pl;
-  launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke, &pl);
+  launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], kb, ke, &pl,
+                      nullptr);
   ctx->interior_nodes = interior_nodes(ctx, pl);
   cudaEventRecord(ctx->ev_join2, ctx->s2);
   if (p.rupture) cudaStreamWaitEvent(ctx->s0, ctx->ev_join, 0);
@@ -1265,9 +1271,14 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
   if (e->sc[0]->serial) {
     launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
     launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
-    launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, e->s0);
-    launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s0);
+    // the general kernel beside the fault band kernel
+    cudaEventRecord(e->ev_fork, e->s0);
+    cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
+    launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, e->s2);
+    launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s2);
+    cudaEventRecord(e->ev_join2, e->s2);
     if (nr) launch_fault_band_batch(S.fault, S.bstart, nr, S.bblocks, S.FX, S.FY, S.FZ, e->s0);
+    cudaStreamWaitEvent(e->s0, e->ev_join2, 0);
     cudaError_t ce = cudaGetLastError();
     return ce == cudaSuccess ? DFD_OK : ens_fail(e, DFD_ERR_CUDA, std::string("ensemble stage: ") + cudaGetErrorString(ce));
   }

@@ -390,7 +390,7 @@ VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
 
 template <int FX, int FY, int FZ>
 static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_shell, const TileCtx* tc, int bin,
-                              cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out) {
+                              cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out, cudaEvent_t* fork) {
   const VolPlan pl = plan_volume(a, tc);
   if (out) *out = pl;
   if (kb) cudaEventRecord(*kb, s);
@@ -404,6 +404,11 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
   }
   if (ke) cudaEventRecord(*ke, s);
   if (pl.ps.nunits > 0) launch_pml(tc, a, FX, FY, FZ, bin, pl.ps, pl.pgrid, s);
+  if (fork && s_shell != s) {
+    // the general kernel on s_shell once the tiled kernels are done
+    cudaEventRecord(*fork, s);
+    cudaStreamWaitEvent(s_shell, *fork, 0);
+  }
   const int below = pl.bx.start[pl.bx.ntop], above = pl.bx.start[pl.bx.n] - below;
   if (below > 0) volume_shell_kernel<FX, FY, FZ, false><<<below, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
   if (above > 0) volume_shell_kernel<FX, FY, FZ, true><<<above, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
@@ -433,20 +438,22 @@ void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start
 }
 
 // Launches the volume kernels of one stage; kb/ke (optional) are recorded on s right
-// before and after the interior (tiled) kernel.  Returns the nodes of the box that kernel
-// covers.
+// before and after the interior (tiled) kernel; with fork (and s_shell != s) the general
+// kernel runs on s_shell after the tiled kernels, else on s_shell right away.  Returns the
+// nodes of the box the interior kernel covers.
 long long launch_volume_stage(const VolArgs& a, int FX, int FY, int FZ, cudaStream_t s, cudaStream_t s_shell,
-                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out) {
+                              const TileCtx* tc, int bin, cudaEvent_t* kb, cudaEvent_t* ke, VolPlan* out,
+                              cudaEvent_t* fork) {
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: return launch_flags<-1, -1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
-    case 1: return launch_flags<-1, -1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
-    case 2: return launch_flags<-1, 1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
-    case 3: return launch_flags<-1, 1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
-    case 4: return launch_flags<1, -1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
-    case 5: return launch_flags<1, -1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
-    case 6: return launch_flags<1, 1, -1>(a, s, s_shell, tc, bin, kb, ke, out);
-    default: return launch_flags<1, 1, 1>(a, s, s_shell, tc, bin, kb, ke, out);
+    case 0: return launch_flags<-1, -1, -1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
+    case 1: return launch_flags<-1, -1, 1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
+    case 2: return launch_flags<-1, 1, -1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
+    case 3: return launch_flags<-1, 1, 1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
+    case 4: return launch_flags<1, -1, -1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
+    case 5: return launch_flags<1, -1, 1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
+    case 6: return launch_flags<1, 1, -1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
+    default: return launch_flags<1, 1, 1>(a, s, s_shell, tc, bin, kb, ke, out, fork);
   }
 }
 
