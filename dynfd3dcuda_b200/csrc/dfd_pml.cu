@@ -204,7 +204,7 @@ template <int FX, int FY, int FZ>
 __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* x0, const float* x1, const float* x2,
                                          const float* x3, const float* x4, const float* cur, const NodeMetric& g,
                                          int i, int j, int k, int fx, int fy, int fz, int own, const float* A,
-                                         long long q, const float* P, float damp) {
+                                         long long q, const float* P, float damp, float rbx, float ddx, float alx) {
   const float r = a.rDH;
   float hv[9], p[9], D[9], dv[9];
 #pragma unroll
@@ -219,12 +219,12 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
     role_terms<0, true>(dv + 3, g.ex0, g.ex1, g.ex2, g.lam, g.mu, g.rrho, D);
     role_terms<3, true>(dv, g.ex0, g.ex1, g.ex2, g.lam, g.mu, g.rrho, D + 3);
     role_terms<6, true>(dv, g.ex0, g.ex1, g.ex2, g.lam, g.mu, g.rrho, D + 6);
-    const float rb = __ldg(a.rBx + i);
+    const float rb = rbx;
 #pragma unroll
     for (int f = 0; f < 9; f++) hv[f] = D[f] * rb;
     if (fx >= 0) {
       const bool st = fx == own;
-      const float dd = __ldg(a.Dpx + i), al = __ldg(a.Apx + i);
+      const float dd = ddx, al = alx;
       role_face<0, 0>(a, fx, st, A, i, j, k, rb, dd, al, D, p);
       role_face<3, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 3, p + 3);
       role_face<6, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 6, p + 6);
@@ -425,6 +425,9 @@ __global__ void __maxnreg__(168)
     const int nst = pu.ie - pu.ib;
     const bool usep = needW0 || needT || pu.face >= 0;
     const float* Q = qs + qr.slot * QSLOT + pc;
+    // per-plane 1-D factors, loaded one plane ahead so that their latency overlaps a plane
+    float nx_rA = __ldg(a.rxa + pu.ib + 3), nx_dx = a.dampx ? __ldg(a.dampx + pu.ib + 3) : 1.0f;
+    float nx_rb = __ldg(a.rBx + pu.ib), nx_dd = __ldg(a.Dpx + pu.ib), nx_al = __ldg(a.Apx + pu.ib);
     for (int s = 0; s < nst; s++) {
       bool ok = true;
       for (int c = s == 0 ? 5 : 1; c > 0; c--) {
@@ -438,6 +441,14 @@ __global__ void __maxnreg__(168)
       }
       const int i = pu.ib + s;
       const float* P = pw + pr.slot * PSLOT_M + pc;
+      const float rA = nx_rA, dx = nx_dx, rbx = nx_rb, ddx = nx_dd, alx = nx_al;
+      if (s + 1 < nst) {
+        nx_rA = __ldg(a.rxa + i + 4);
+        if (a.dampx) nx_dx = __ldg(a.dampx + i + 4);
+        nx_rb = __ldg(a.rBx + i + 1);
+        nx_dd = __ldg(a.Dpx + i + 1);
+        nx_al = __ldg(a.Apx + i + 1);
+      }
       const bool node = active && !(band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3);
       const int fx = (a.aux[0] && i < d.N) ? 0 : (a.aux[1] && i >= d.ni - d.N) ? 1 : -1;
       // a warp none of whose nodes lies in a PML slab in this plane takes the lean path
@@ -454,17 +465,16 @@ __global__ void __maxnreg__(168)
         const float* x4 = win + s4 * HSLOT + hc;
         const float* cur = FX == 1 ? x1 : x3;
         NodeMetric g;
-        const float rA = __ldg(a.rxa + i + 3);
         g.ex0 = rA; g.ex1 = Q[0] * rA; g.ex2 = Q[PB] * rA;
         g.ey1 = Q[2 * PB]; g.ey2 = Q[3 * PB]; g.ez1 = Q[4 * PB]; g.ez2 = Q[5 * PB];
         const int side = i + 3 < a.nxhalf ? 6 : 9;
         g.lam = Q[side * PB]; g.mu = Q[(side + 1) * PB]; g.rrho = 1.0f / Q[(side + 2) * PB];
-        const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
+        const float damp = a.dampx ? fminf(dx, dyz) : 1.0f;
         const long long q = qyz + (long long)(i + 3) * d.sx;
         if (pu.strip || pml) {
           // (strips hold y-slab nodes and the few interior columns beside them)
           pml_node<FX, FY, FZ>(a, pu.strip ? STRIP + 8 : HW, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face,
-                               P + 18 * PB, q, P, damp);
+                               P + 18 * PB, q, P, damp, rbx, ddx, alx);
         } else {
           float hv[9];
           lean_velocity<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);

@@ -189,6 +189,9 @@ __global__ void __maxnreg__(96)
     const int nst = ie - ib;
     const float* Q = qs + qr.slot * QSLOT + pc;
     const float mU = Q[0], mV = Q[PB], ety = Q[2 * PB], etz = Q[3 * PB], zty = Q[4 * PB], ztz = Q[5 * PB];
+    // per-plane 1-D factors, loaded one plane ahead so that their latency overlaps a plane
+    float rA_next = __ldg(a.rxa + ib + 3);
+    float dx_next = a.dampx ? __ldg(a.dampx + ib + 3) : 1.0f;
     for (int s = 0; s < nst; s++) {
       bool ok = true;
       for (int c = s == 0 ? 5 : 1; c > 0; c--) {
@@ -202,6 +205,11 @@ __global__ void __maxnreg__(96)
       }
       const int i = ib + s;
       const float* P = pw + pr.slot * PSLOT + pc;
+      const float rA = rA_next, dx = dx_next;
+      if (s + 1 < nst) {
+        rA_next = __ldg(a.rxa + i + 4);
+        if (a.dampx) dx_next = __ldg(a.dampx + i + 4);
+      }
       if (active && !(band && i + 3 >= d.i0 - 3 && i + 3 <= d.i0 + 3)) {
         const int s1 = sb + 1 == NS ? 0 : sb + 1;
         const int s2 = s1 + 1 == NS ? 0 : s1 + 1;
@@ -215,12 +223,11 @@ __global__ void __maxnreg__(96)
         const float* cur = FX == 1 ? xs1 : xs3;  // plane x itself
         // metric (xi row from the 1-D factor) and media of the side of the bimaterial split
         NodeMetric g;
-        const float rA = __ldg(a.rxa + i + 3);
         g.ex0 = rA; g.ex1 = mU * rA; g.ex2 = mV * rA;
         g.ey1 = ety; g.ey2 = etz; g.ez1 = zty; g.ez2 = ztz;
         const int side = i + 3 < a.nxhalf ? 6 : 9;
         g.lam = Q[side * PB]; g.mu = Q[(side + 1) * PB]; g.rrho = 1.0f / Q[(side + 2) * PB];
-        const float damp = a.dampx ? fminf(__ldg(a.dampx + i + 3), dyz) : 1.0f;
+        const float damp = a.dampx ? fminf(dx, dyz) : 1.0f;
         const long long q = qyz + (long long)(i + 3) * d.sx;
         float hv[9];
         if (role == 0) {
