@@ -435,29 +435,39 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int 
     double Vtn = sqrt(Vt1 * Vt1 + Vt2 * Vt2);
     double Ttn = sqrt(Tl[1] * Tl[1] + Tl[2] * Tl[2]);
     double Rn = sqrt(Rl[1] * Rl[1] + Rl[2] * Rl[2]);
-    double x0 = asinh(exp(st / ra) * Rn / (2.0 * 1e-6));
+    const double es = exp(st / ra);
     int its = 0, its2 = 0;
     bool ok = false;
     double xn;
-    const float fin[4] = {(float)(st / ra), (float)log10(fmax(Vtn, 1e-30)), (float)log10(fmax(coef, 1e-30)),
-                          (float)ra};
+    // network inputs (FP32, as the network computes), needed by the learned guess and by
+    // the sample recording only
+    auto features = [&](float* fin) {
+      fin[0] = (float)(st / ra);
+      fin[1] = log10f(fmaxf((float)Vtn, 1e-30f));
+      fin[2] = log10f(fmaxf((float)coef, 1e-30f));
+      fin[3] = (float)ra;
+    };
     if (a.rs_guess && a.guess_net) {
       // learned guess: the root without radiation damping corrected by the network, then
       // the same Newton iteration (capped); the plain solve from the reference's guess
       // takes over whenever it does not converge
-      double xa = asinh(Vtn * exp(st / ra) / (2.0 * 1e-6));
+      float fin[4];
+      features(fin);
+      double xa = asinh(Vtn * es / (2.0 * 1e-6));
       double xg = xa + (double)mlp_residual(snet, fin);
       xn = newton_rs(xg, st, ra, Vtn, coef, 12, &its, &ok);
-      if (!ok || !isfinite(xn)) xn = newton_rs(x0, st, ra, Vtn, coef, 100, &its2, &ok);
+      if (!ok || !isfinite(xn)) xn = newton_rs(asinh(es * Rn / (2.0 * 1e-6)), st, ra, Vtn, coef, 100, &its2, &ok);
     } else {
-      xn = newton_rs(x0, st, ra, Vtn, coef, 100, &its, &ok);
+      xn = newton_rs(asinh(es * Rn / (2.0 * 1e-6)), st, ra, Vtn, coef, 100, &its, &ok);
       if (a.rec && ok && ((unsigned)q2 * 7919u + (unsigned)it * 4u + (unsigned)a.irk) % (unsigned)a.rec_every == 0) {
         // training sample: inputs and the residual target of the converged solve
         unsigned slot = atomicAdd(a.rec_n, 1u);
         if (slot < (unsigned)a.rec_cap) {
+          float fin[4];
+          features(fin);
           float* o = a.rec + 5ull * slot;
           o[0] = fin[0]; o[1] = fin[1]; o[2] = fin[2]; o[3] = fin[3];
-          o[4] = (float)(xn - asinh(Vtn * exp(st / ra) / (2.0 * 1e-6)));
+          o[4] = (float)(xn - asinh(Vtn * es / (2.0 * 1e-6)));
         }
       }
     }
