@@ -338,7 +338,15 @@ VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
     int za = a.aux[4] ? d.N : 0;
     int zb = a.aux[5] ? d.nk - d.N : ktop;
     if (yb <= ya) ya = yb = 0;     // no interior column: strips over every column
-    if (zb <= za) za = zb = ktop;  // no interior row: z tiles over every row
+    // whole 8-row tiles in z: the rows left over go to the PML kernel's z tiles (whose
+    // second tile row over a 12-row slab has room for them), not to a nearly empty row of
+    // interior tiles
+    const int zr = (zb - za) % TILE_K;
+    if (zb - za >= TILE_K && zr) {
+      if (a.aux[4]) za += zr;
+      else zb -= zr;
+    }
+    if (zb <= za || zb - za < TILE_K) za = zb = ktop;  // no interior row: z tiles over every row
     int grid = 0;
     TileSched ps = pml_plan(a, ya, yb, za, zb, ktop, tc->nsm, &grid);
     const int3 rlo = make_int3(lo.x, ya, za), rhi = make_int3(hi.x, yb, zb);

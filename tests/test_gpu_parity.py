@@ -139,6 +139,8 @@ TILED_CASES = [
     ("vol_curved", {"NX": 40, "NY": 100, "NZ": 52, "FreeSurface": 0}),  # PML on the top face
     ("vol_curved", {"NX": 40, "NY": 100, "NZ": 52, "usePML": 0}),       # no PML: filler tiles only
     ("vol_curved", {"NX": 36, "NY": 90, "NZ": 44, "useCerjan": 1, "DAMP_N": 8}),
+    ("vol_curved", {"NX": 48, "NY": 110, "NZ": 60, "PML_N": 20}),  # two 16-wide strips per y slab
+    ("vol_curved", {"NX": 40, "NY": 101, "NZ": 53, "PML_N": 13}),  # slab widths not multiples of 4
 ]
 
 
