@@ -863,9 +863,11 @@ __global__ void __launch_bounds__(128) fault_node_kernel(const __grid_constant__
   fault_node_body<FY, FZ>(a, blockIdx.x, blockIdx.y, snet);
 }
 // grid z: the part (six off-fault layers, then the split nodes), so that the seven
-// independent pieces of a fault column run in parallel
+// independent pieces of a fault column run in parallel.  At most 128 registers (four
+// blocks per SM): this latency-bound kernel gains more from the resident warps than it
+// loses to the few spilled values (measured: 3, 4, 5, 6 blocks per SM).
 template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(128) fault_band_kernel(const __grid_constant__ FaultArgs a) {
+__global__ void __launch_bounds__(128, 4) fault_band_kernel(const __grid_constant__ FaultArgs a) {
   fault_band_body<FX, FY, FZ>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -886,7 +888,7 @@ __global__ void __launch_bounds__(128) fault_node_batch(const FaultArgs* __restr
   fault_node_body<FY, FZ>(a, loc % gx, loc / gx, snet);
 }
 template <int FX, int FY, int FZ>
-__global__ void __launch_bounds__(128) fault_band_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
+__global__ void __launch_bounds__(128, 4) fault_band_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
                                                         int n) {
   __shared__ __align__(16) unsigned char raw[sizeof(FaultArgs)];
   FaultArgs* sa = reinterpret_cast<FaultArgs*>(raw);
