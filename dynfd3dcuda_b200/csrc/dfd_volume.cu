@@ -188,9 +188,10 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
 
 // Shell kernels: the general update on up to eight boxes (PML slabs, free-surface rows)
 // that surround the interior box; one 1-D grid of 128-thread blocks is split over the
-// boxes below the free-surface rows (at most 170 registers, three blocks per SM: the PML
-// path needs about 160) and a second over the rows themselves (the traction image needs
-// about 230).  A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z) per block; a
+// boxes below the free-surface rows and a second over the rows themselves.  At most 170
+// registers, three blocks per SM: the PML path needs about 160; the traction image of the
+// free-surface rows would take about 230, but the third resident block is worth more than
+// the few values it spills (measured against two and four blocks per SM).  A box at least 32 nodes wide in y and 4 in z is tiled (32 y, 4 z) per block; a
 // thinner box (the y slabs of the PML, the free-surface rows) is flattened over (y, z)
 // with y fastest, so that no thread idles and the y-face PML state (y fastest over N
 // nodes, then z) is read contiguously.
@@ -226,13 +227,13 @@ __device__ __forceinline__ void volume_shell_body(const VolArgs& a, const Boxes&
   volume_point_general<FX, FY, FZ, TOP>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
 }
 template <int FX, int FY, int FZ, bool TOP>
-__global__ void __launch_bounds__(SHELL_THREADS, TOP ? 2 : 3)
+__global__ void __launch_bounds__(SHELL_THREADS, 3)
     volume_shell_kernel(const __grid_constant__ VolArgs a, const __grid_constant__ Boxes bx) {
   volume_shell_body<FX, FY, FZ, TOP>(a, bx, blockIdx.x);
 }
 // all scenarios of an ensemble in one launch: scenario s owns blocks [start[s], start[s+1])
 template <int FX, int FY, int FZ, bool TOP>
-__global__ void __launch_bounds__(SHELL_THREADS, TOP ? 2 : 3)
+__global__ void __launch_bounds__(SHELL_THREADS, 3)
     volume_shell_batch(const VolArgs* __restrict__ tab, const Boxes* __restrict__ boxes,
                        const int* __restrict__ start, int n) {
   __shared__ __align__(16) unsigned char raw_a[sizeof(VolArgs)];
