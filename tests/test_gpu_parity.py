@@ -185,3 +185,19 @@ def test_tiled_kernels_match_plain_kernels_with_fault(monkeypatch, name):
     assert rel(tiled.fault("slip"), plain.fault("slip")) < 5e-5
     plain.close()
     tiled.close()
+
+def test_three_streams_equal_one_stream(monkeypatch):
+    """DFD_STREAMS=3 runs the free-surface and band kernels on two more streams beside the
+    interior kernel; the kernels and their outputs are the same, only the order differs,
+    so the results are bit for bit those of the default ordering."""
+    a, *_ = make_sim("sw_curved")
+    monkeypatch.setenv("DFD_STREAMS", "3")
+    b, *_ = make_sim("sw_curved")
+    monkeypatch.delenv("DFD_STREAMS")
+    a.run(0, 8)
+    b.run(0, 8)
+    b.synchronize()
+    assert np.array_equal(a.wave(), b.wave())
+    assert np.array_equal(a.fault("slip"), b.fault("slip"))
+    a.close()
+    b.close()
