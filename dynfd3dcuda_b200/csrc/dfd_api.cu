@@ -6,7 +6,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dfd_host.h"
@@ -58,6 +62,30 @@ enum Plane {
   P_FRIC, NPLANE
 };
 enum IPlane { I_T0FLAG, I_FLAGRUP, I_UNITED, I_FAULTGRID, I_RUPY, I_RUPZ, NIPLANE };
+
+// Asynchronous output (dfd_output_write): the record is copied on the stepping stream
+// into one of two device staging sets (a snapshot the next step cannot change), the
+// staging set goes to pinned host memory on a side stream, and a writer thread puts the
+// finished record into the NetCDF files while the GPU keeps stepping.  Record layout in
+// floats: the seven per-step fault planes, init_t0, the two rupture-index planes (int32),
+// then the three wave slices (3 components each).
+struct OutState {
+  size_t nf = 0, bytes = 0;
+  size_t slice_off[3] = {0, 0, 0}, slice_n[3] = {0, 0, 0};
+  float* dev[2] = {nullptr, nullptr};
+  float* host[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};  // the slot's copy to the host has finished
+  cudaEvent_t snap = nullptr;                // the snapshot on the stepping stream is done
+  cudaStream_t s = nullptr;
+  std::thread writer;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::pair<int, int>> q;  // (record index, slot) waiting for the writer
+  bool busy[2] = {false, false};      // the slot holds a record not yet written
+  bool stop = false;
+  int err = 0;
+  int next = 0;
+};
 
 struct dfd_ctx {
   dfd_params p;
@@ -112,6 +140,7 @@ struct dfd_ctx {
   NcWriter ncf, ncw[3];
   int vf[24] = {}, vw[3][3] = {};
   bool out_open = false;
+  OutState* out = nullptr;
 };
 
 static int fail(dfd_ctx* c, int code, const std::string& m) {
@@ -969,6 +998,49 @@ int dfd_newton_samples(dfd_ctx* ctx, float* host, int max, int* n) {
 }
 
 // ------------------------------------------------------------------ output --
+// the writer thread: puts each finished record into the files, in order
+static void out_writer(dfd_ctx* ctx) {
+  OutState& o = *ctx->out;
+  cudaSetDevice(ctx->device);
+  const size_t nf = o.nf;
+  std::vector<float> zero(ctx->p.rupture ? nf : 0, 0.0f);
+  for (;;) {
+    std::pair<int, int> r;
+    {
+      std::unique_lock<std::mutex> lk(o.mu);
+      o.cv.wait(lk, [&] { return o.stop || !o.q.empty(); });
+      if (o.q.empty()) break;
+      r = o.q.front();
+      o.q.pop_front();
+    }
+    const int rec = r.first, slot = r.second;
+    int e = cudaEventSynchronize(o.done[slot]) == cudaSuccess ? 0 : DFD_ERR_CUDA;
+    const float* h = o.host[slot];
+    bool ok = true;
+    if (!e && ctx->p.rupture) {
+      for (int i = 0; i < 7; i++) ok = ok && ctx->ncf.put_record(ctx->vf[10 + i], rec, h + i * nf);
+      ok = ok && ctx->ncf.put_fixed(ctx->vf[3], h + 7 * nf);
+      ok = ok && ctx->ncf.put_record(17, rec, h + 8 * nf);
+      ok = ok && ctx->ncf.put_record(18, rec, h + 9 * nf);
+      for (int v = 19; v < 22; v++) ok = ok && ctx->ncf.put_record(v, rec, zero.data());
+      ok = ok && ctx->ncf.sync();
+    }
+    for (int a = 0; a < 3 && !e; a++) {
+      if (!o.slice_n[a]) continue;
+      for (int c = 0; c < 3; c++)
+        ok = ok && ctx->ncw[a].put_record(ctx->vw[a][c], rec, h + o.slice_off[a] + c * o.slice_n[a]);
+      ok = ok && ctx->ncw[a].sync();
+    }
+    if (!e && !ok) e = DFD_ERR_IO;
+    {
+      std::lock_guard<std::mutex> lk(o.mu);
+      o.busy[slot] = false;
+      if (e && !o.err) o.err = e;
+    }
+    o.cv.notify_all();
+  }
+}
+
 int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
   if (!ctx || !outdir) return DFD_ERR_PARAM;
   if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
@@ -1058,54 +1130,103 @@ int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
     w.put_fixed(cz, Z.data());
     w.sync();
   }
+  // staging sets, pinned host buffers, side stream and the writer thread
+  OutState* o = new OutState();
+  ctx->out = o;
+  o->nf = (size_t)d.nj * d.nk;
+  size_t off = p.rupture ? 10 * o->nf : 0;
+  for (int a = 0; a < 3; a++) {
+    if (idx[a] < 0 || idx[a] >= lim[a]) continue;
+    const int na = a == 0 ? d.nk : d.ni, nb = a == 1 ? d.nk : d.nj;
+    o->slice_off[a] = off;
+    o->slice_n[a] = (size_t)na * nb;
+    off += 3 * o->slice_n[a];
+  }
+  o->bytes = std::max<size_t>(off, 1) * sizeof(float);
+  for (int b = 0; b < 2; b++) {
+    CK(cudaMalloc(&o->dev[b], o->bytes));
+    CK(cudaMallocHost(&o->host[b], o->bytes));
+    CK(cudaEventCreateWithFlags(&o->done[b], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&o->snap, cudaEventDisableTiming));
+  CK(cudaStreamCreateWithFlags(&o->s, cudaStreamNonBlocking));
+  o->writer = std::thread(out_writer, ctx);
   ctx->out_open = true;
   return DFD_OK;
 }
 
-// one output record (the reference writes it before the step, main.cu:425-437)
+// one output record (the reference writes it before the step, main.cu:425-437): a
+// snapshot on the stepping stream, the copy to the host and the file writes behind it
+static const int kOutPlanes[7] = {P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_SLIP, P_STATE};
+
 int dfd_output_write(dfd_ctx* ctx, int it_skip) {
-  if (!ctx || !ctx->out_open) return DFD_ERR_STATE;
+  if (!ctx || !ctx->out_open || !ctx->out) return DFD_ERR_STATE;
+  if (ctx->sticky) return ctx->sticky;
+  OutState& o = *ctx->out;
+  const int slot = o.next;
+  {
+    // wait until the writer has put this slot's previous record into the files
+    std::unique_lock<std::mutex> lk(o.mu);
+    o.cv.wait(lk, [&] { return !o.busy[slot] || o.err; });
+    if (o.err) return fail(ctx, o.err, "output: a record could not be written");
+  }
+  cudaSetDevice(ctx->device);
   const Dims& d = ctx->d;
-  size_t nf = (size_t)d.nj * d.nk;
+  const size_t nf = o.nf;
+  float* dst = o.dev[slot];
   if (ctx->p.rupture) {
-    CK(cudaStreamSynchronize(ctx->s0));
-    static const int rec[7] = {P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_SLIP, P_STATE};
-    std::vector<float> t(nf);
-    for (int i = 0; i < 7; i++) {
-      CK(cudaMemcpy(t.data(), ctx->pl + rec[i] * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
-      ctx->ncf.put_record(ctx->vf[10 + i], it_skip, t.data());
-    }
-    CK(cudaMemcpy(t.data(), ctx->pl + P_T0 * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
-    ctx->ncf.put_fixed(ctx->vf[3], t.data());
-    std::vector<int> u(nf);
-    CK(cudaMemcpy(u.data(), ctx->ipl + I_RUPY * nf, sizeof(int) * nf, cudaMemcpyDeviceToHost));
-    ctx->ncf.put_record(17, it_skip, u.data());
-    CK(cudaMemcpy(u.data(), ctx->ipl + I_RUPZ * nf, sizeof(int) * nf, cudaMemcpyDeviceToHost));
-    ctx->ncf.put_record(18, it_skip, u.data());
-    std::fill(t.begin(), t.end(), 0.0f);
-    for (int v = 19; v < 22; v++) ctx->ncf.put_record(v, it_skip, t.data());
-    ctx->ncf.sync();
+    for (int i = 0; i < 7; i++)
+      CK(cudaMemcpyAsync(dst + i * nf, ctx->pl + kOutPlanes[i] * nf, sizeof(float) * nf, cudaMemcpyDeviceToDevice,
+                         ctx->s0));
+    CK(cudaMemcpyAsync(dst + 7 * nf, ctx->pl + P_T0 * nf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
+    CK(cudaMemcpyAsync(dst + 8 * nf, ctx->ipl + I_RUPY * nf, sizeof(int) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
+    CK(cudaMemcpyAsync(dst + 9 * nf, ctx->ipl + I_RUPZ * nf, sizeof(int) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
   }
-  int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y, ctx->p.EXPORT_WAVE_SLICE_Z};
-  int lim[3] = {d.ni, d.nj, d.nk};
-  for (int a = 0; a < 3; a++) {
-    if (idx[a] < 0 || idx[a] >= lim[a]) continue;
-    int na = a == 0 ? d.nk : d.ni, nb = a == 1 ? d.nk : d.nj;
-    std::vector<float> buf((size_t)3 * na * nb);
-    int r = dfd_get_slice(ctx, a, idx[a], buf.data());
-    if (r) return r;
-    for (int c = 0; c < 3; c++) ctx->ncw[a].put_record(ctx->vw[a][c], it_skip, buf.data() + (size_t)c * na * nb);
-    ctx->ncw[a].sync();
+  const int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y, ctx->p.EXPORT_WAVE_SLICE_Z};
+  for (int a = 0; a < 3; a++)
+    if (o.slice_n[a])
+      dfd::slice_kernel<<<(unsigned)((o.slice_n[a] + 255) / 256), 256, 0, ctx->s0>>>(d, ctx->W[0], a, idx[a],
+                                                                                      dst + o.slice_off[a]);
+  CK(cudaEventRecord(o.snap, ctx->s0));
+  CK(cudaStreamWaitEvent(o.s, o.snap, 0));
+  CK(cudaMemcpyAsync(o.host[slot], dst, o.bytes, cudaMemcpyDeviceToHost, o.s));
+  CK(cudaEventRecord(o.done[slot], o.s));
+  {
+    std::lock_guard<std::mutex> lk(o.mu);
+    o.busy[slot] = true;
+    o.q.emplace_back(it_skip, slot);
   }
+  o.cv.notify_all();
+  o.next = slot ^ 1;
   return DFD_OK;
 }
 
 int dfd_output_close(dfd_ctx* ctx) {
   if (!ctx) return DFD_ERR_PARAM;
+  int err = 0;
+  if (ctx->out) {
+    OutState* o = ctx->out;
+    {
+      std::lock_guard<std::mutex> lk(o->mu);
+      o->stop = true;
+    }
+    o->cv.notify_all();
+    if (o->writer.joinable()) o->writer.join();
+    err = o->err;
+    for (int b = 0; b < 2; b++) {
+      if (o->dev[b]) cudaFree(o->dev[b]);
+      if (o->host[b]) cudaFreeHost(o->host[b]);
+      if (o->done[b]) cudaEventDestroy(o->done[b]);
+    }
+    if (o->snap) cudaEventDestroy(o->snap);
+    if (o->s) cudaStreamDestroy(o->s);
+    delete o;
+    ctx->out = nullptr;
+  }
   ctx->ncf.close();
   for (auto& w : ctx->ncw) w.close();
   ctx->out_open = false;
-  return DFD_OK;
+  return err ? fail(ctx, err, "output: a record could not be written") : DFD_OK;
 }
 
 }  // extern "C"

@@ -154,7 +154,13 @@ int dfd_check_finite(dfd_ctx *ctx);
 int dfd_newton_stats(dfd_ctx *ctx, long long *iterations, long long *capped);
 
 /* ---- NetCDF-classic output with the reference layout (io_fault.cu:16-285,
- *      io_wave_xy.cu:9-188): fault_mpi000000.nc and wave_{xy,xz,yz}_mpi000000.nc ---- */
+ *      io_wave_xy.cu:9-188): fault_mpi000000.nc and wave_{xy,xz,yz}_mpi000000.nc ----
+ * dfd_output_write queues record it_skip of the current state (the reference writes it
+ * before the step, main.cu:425-437) and returns: the state is copied on the context's
+ * stream, the files are written by a writer thread while the steps go on.  It blocks
+ * only while two earlier records still wait for the writer.  dfd_output_close writes
+ * every queued record, then closes the files; an error of the writer is returned by the
+ * next dfd_output_write or by dfd_output_close. */
 int dfd_output_open(dfd_ctx *ctx, const char *outdir);
 int dfd_output_write(dfd_ctx *ctx, int it_skip);
 int dfd_output_close(dfd_ctx *ctx);
