@@ -141,6 +141,13 @@ struct dfd_ctx {
   int vf[24] = {}, vw[3][3] = {};
   bool out_open = false;
   OutState* out = nullptr;
+  // dfd_fetch_outputs: two device staging copies of the outputs and a side stream that
+  // takes them to the host while the next steps run
+  float* fetch_stage[2] = {nullptr, nullptr};
+  cudaEvent_t fetch_snap = nullptr, fetch_done[2] = {nullptr, nullptr};
+  cudaStream_t s_fetch = nullptr;
+  int fetch_k = 0;
+  bool fetch_used[2] = {false, false};
 };
 
 static int fail(dfd_ctx* c, int code, const std::string& m) {
@@ -325,6 +332,15 @@ int dfd_destroy(dfd_ctx* ctx) {
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->ev_join2) cudaEventDestroy(ctx->ev_join2);
+  if (ctx->s_fetch) {
+    cudaStreamSynchronize(ctx->s_fetch);
+    for (int b = 0; b < 2; b++) {
+      cudaFree(ctx->fetch_stage[b]);
+      cudaEventDestroy(ctx->fetch_done[b]);
+    }
+    cudaEventDestroy(ctx->fetch_snap);
+    cudaStreamDestroy(ctx->s_fetch);
+  }
   if (ctx->s0) cudaStreamDestroy(ctx->s0);
   if (ctx->s1) cudaStreamDestroy(ctx->s1);
   if (ctx->s2) cudaStreamDestroy(ctx->s2);
@@ -749,6 +765,7 @@ int dfd_synchronize(dfd_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->s0));
   CK(cudaStreamSynchronize(ctx->s1));
   CK(cudaStreamSynchronize(ctx->s2));
+  if (ctx->s_fetch) CK(cudaStreamSynchronize(ctx->s_fetch));
   return tile_status(ctx);
 }
 
@@ -884,8 +901,27 @@ int dfd_newton_stats(dfd_ctx* ctx, long long* iterations, long long* capped) {
 int dfd_fetch_outputs(dfd_ctx* ctx, float* host) {
   if (!ctx || !host) return DFD_ERR_PARAM;
   if (!ctx->p.rupture) return fail(ctx, DFD_ERR_STATE, "rupture is off");
-  size_t nf = (size_t)ctx->d.nj * ctx->d.nk;
-  CK(cudaMemcpyAsync(host, ctx->pl, sizeof(float) * 8 * nf, cudaMemcpyDeviceToHost, ctx->s0));
+  cudaSetDevice(ctx->device);
+  const size_t bytes = sizeof(float) * 8 * (size_t)ctx->d.nj * ctx->d.nk;
+  if (!ctx->s_fetch) {
+    for (int b = 0; b < 2; b++) {
+      CK(cudaMalloc(&ctx->fetch_stage[b], bytes));
+      CK(cudaEventCreateWithFlags(&ctx->fetch_done[b], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&ctx->fetch_snap, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&ctx->s_fetch, cudaStreamNonBlocking));
+  }
+  // a device copy on the stepping stream (the next step cannot change it), then the copy
+  // to the host on the side stream beside the next steps
+  const int k = ctx->fetch_k;
+  ctx->fetch_k ^= 1;
+  if (ctx->fetch_used[k]) CK(cudaStreamWaitEvent(ctx->s0, ctx->fetch_done[k], 0));
+  CK(cudaMemcpyAsync(ctx->fetch_stage[k], ctx->pl, bytes, cudaMemcpyDeviceToDevice, ctx->s0));
+  CK(cudaEventRecord(ctx->fetch_snap, ctx->s0));
+  CK(cudaStreamWaitEvent(ctx->s_fetch, ctx->fetch_snap, 0));
+  CK(cudaMemcpyAsync(host, ctx->fetch_stage[k], bytes, cudaMemcpyDeviceToHost, ctx->s_fetch));
+  CK(cudaEventRecord(ctx->fetch_done[k], ctx->s_fetch));
+  ctx->fetch_used[k] = true;
   return DFD_OK;
 }
 

@@ -103,3 +103,27 @@ def test_async_output_matches_state(tmp_path):
             for c, comp in enumerate(("Vx", "Vy", "Vz")):
                 np.testing.assert_array_equal(np.asarray(f.variables[comp][:]), np.stack([s[ax][c] for s in slices]),
                                               err_msg=f"{name}/{comp}")
+
+
+def test_fetch_outputs_matches_state():
+    """dfd_fetch_outputs snapshots the eight per-step output planes on the stepping
+    stream and copies them to the host on a side stream: six fetches, each followed by a
+    step, hold the state a second run reads before the same steps."""
+    import dynfd3dcuda_b200 as dfd
+
+    p, fx, st, _, _, _ = cases.get_case("sw_flat")
+    a = dfd.Simulation(dict(p), fx, st, None)
+    nf = p["NY"] * p["NZ"]
+    bufs = [np.zeros((8, nf), np.float32) for _ in range(6)]
+    for it in range(6):
+        a.fetch_outputs(bufs[it].ctypes.data)
+        a.run(it, 1)
+    a.synchronize()
+    a.close()
+    b = dfd.Simulation(dict(p), fx, st, None)
+    names = ("Vs1", "Vs2", "Tn", "Ts1", "Ts2", "slip", "State", "init_t0")
+    for it in range(6):
+        for r, k in enumerate(names):
+            np.testing.assert_array_equal(bufs[it][r], b.fault(k).ravel(), err_msg=f"step {it} {k}")
+        b.run(it, 1)
+    b.close()
