@@ -59,7 +59,7 @@ enum Plane {
   P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_SLIP, P_STATE, P_T0,
   P_MSLIP, P_TSLIP, P_HSLIP, P_MSTATE, P_TSTATE, P_TTN, P_TTS1,
   P_TTS2, P_SX, P_SY, P_SZ, P_T0X, P_T0Y, P_T0Z, P_DT0X, P_DT0Y, P_DT0Z, P_PEAK, P_DC, P_C0, P_A, P_B, P_L, P_VW,
-  P_FRIC, NPLANE
+  P_FRIC, P_CSLIP, P_CSTATE, NPLANE  // last two: compensation terms of slip and state
 };
 enum IPlane { I_T0FLAG, I_FLAGRUP, I_UNITED, I_FAULTGRID, I_RUPY, I_RUPZ, NIPLANE };
 
@@ -485,6 +485,7 @@ int dfd_precompute(dfd_ctx* ctx) {
         {P_TN, &h.Tn}, {P_TS1, &h.Ts1}, {P_TS2, &h.Ts2}, {P_T0, &h.init_t0}};
     for (auto& u : up)
       CK(cudaMemcpyAsync(ctx->pl + u.plane * nf, u.v->data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(ctx->pl + P_CSLIP * nf, 0, sizeof(float) * 2 * nf, s));
     struct { int plane; std::vector<int>* v; } iup[] = {
         {I_UNITED, &h.united}, {I_FAULTGRID, &h.faultgrid}, {I_RUPY, &h.rupy}, {I_RUPZ, &h.rupz}};
     ctx->n_band_columns = 0;
@@ -547,6 +548,7 @@ static FaultArgs fault_args(dfd_ctx* ctx, int pattern, int irk) {
     auto pl = [&](int k) { return P_ + k * nf; };
     fa.slip = pl(P_SLIP); fa.mslip = pl(P_MSLIP); fa.tslip = pl(P_TSLIP); fa.hslip = pl(P_HSLIP);
     fa.State = pl(P_STATE); fa.mState = pl(P_MSTATE); fa.tState = pl(P_TSTATE);
+    fa.cslip = pl(P_CSLIP); fa.cState = pl(P_CSTATE);
     fa.Vs1 = pl(P_VS1); fa.Vs2 = pl(P_VS2); fa.Tn = pl(P_TN); fa.Ts1 = pl(P_TS1); fa.Ts2 = pl(P_TS2);
     fa.tTn = pl(P_TTN); fa.tTs1 = pl(P_TTS1); fa.tTs2 = pl(P_TTS2);
     fa.sx = pl(P_SX); fa.sy = pl(P_SY); fa.sz = pl(P_SZ);

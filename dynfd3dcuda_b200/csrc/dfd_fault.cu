@@ -144,6 +144,14 @@ __device__ __forceinline__ void fault_to_volume_r(const FaultArgs& a, const floa
   Wdst[8 * n + q] = (sg[1][2] + sg[2][1]) * 0.5f * damp;
 }
 
+// compensated sum s + inc with the running compensation term *c (Kahan summation)
+__device__ __forceinline__ float kahan_add(float s, float inc, float* c) {
+  const float y = __fsub_rn(inc, *c);
+  const float t = __fadd_rn(s, y);
+  *c = __fsub_rn(__fsub_rn(t, s), y);
+  return t;
+}
+
 __device__ __forceinline__ double gt_func(double t, double T) {  // device.cu:134-143
   if (t < T) {
     double t1 = t - T, t2 = t - 2.0 * T;
@@ -270,17 +278,21 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int 
         hState = (float)(-V / rl * (st - psiss));
       }
     }
+    // the accumulator holds the step's increment only; the last stage adds it to the
+    // step-start value with a compensation term (Kahan), so that FP32 rounding does not
+    // build up over the thousands of steps of a rupture (the reference sums into the value
+    // itself, rk4.cu:833-935)
     if (a.irk == 0) {
       float st0 = a.State[q2], sl0 = a.slip[q2];
-      a.mState[q2] = st0; a.tState[q2] = fmaf(a.rkb, hState, st0);
-      a.mslip[q2] = sl0; a.tslip[q2] = fmaf(a.rkb, hs, sl0);
+      a.mState[q2] = st0; a.tState[q2] = a.rkb * hState;
+      a.mslip[q2] = sl0; a.tslip[q2] = a.rkb * hs;
     } else if (a.irk < 3) {
       a.tState[q2] = fmaf(a.rkb, hState, a.tState[q2]);
       a.tslip[q2] = fmaf(a.rkb, hs, a.tslip[q2]);
     }
     if (a.irk == 3) {
-      a.State[q2] = fmaf(a.rkb, hState, a.tState[q2]);
-      a.slip[q2] = fmaf(a.rkb, hs, a.tslip[q2]);
+      a.State[q2] = kahan_add(a.mState[q2], fmaf(a.rkb, hState, a.tState[q2]), a.cState + q2);
+      a.slip[q2] = kahan_add(a.mslip[q2], fmaf(a.rkb, hs, a.tslip[q2]), a.cslip + q2);
     } else {
       a.State[q2] = fmaf(a.rka, hState, a.mState[q2]);
       a.slip[q2] = fmaf(a.rka, hs, a.mslip[q2]);

@@ -151,6 +151,7 @@ struct FaultArgs {
   const float* __restrict__ rhof;  // (2, nz, ny)
   // (NZ, NY) planes
   float *slip, *mslip, *tslip, *hslip, *State, *mState, *tState;
+  float *cslip, *cState;           // compensation terms of the step-to-step sums of slip and state
   float *Vs1, *Vs2, *Tn, *Ts1, *Ts2, *tTn, *tTs1, *tTs2;
   float *sx, *sy, *sz;             // str_init
   const float *T0x, *T0y, *T0z, *dT0x, *dT0y, *dT0z;

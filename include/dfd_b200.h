@@ -61,7 +61,7 @@ typedef struct dfd_params {
 
 typedef struct dfd_ctx dfd_ctx;
 
-/* Named on-fault / split-node / layer arrays for dfd_get_fault / dfd_set_fault. */
+/* Named on-fault / split-node / layer arrays for dfd_get_fault. */
 enum {
   DFD_F_SLIP = 0, DFD_F_HSLIP, DFD_F_VS1, DFD_F_VS2, DFD_F_TN, DFD_F_TS1, DFD_F_TS2, DFD_F_STATE,
   DFD_F_INIT_T0, DFD_F_TTN, DFD_F_TTS1, DFD_F_TTS2, DFD_F_STR_PEAK, DFD_F_FRICTION,
