@@ -6,6 +6,7 @@ dynfd3dcuda_b200/build.py).  The job dictionary uses the reference's params.json
 
     fxyz    (3, NZ, NY) float32   Fault_geometry x, y, z
     stress  (15, NZ, NY) float32  Fault_init_stress Tx Ty Tz dTx dTy dTz mu_s mu_d Dc C0 a b L Vw State
+            (16, NZ, NY)          the same plus TP_hy, for Friction_type 3
     layers  (n, 4) float32        Media1D rows depth rho vp vs
 
 There is no CPU fallback: constructing a Simulation without the CUDA library or without
@@ -22,7 +23,7 @@ LIBPATH = os.path.join(_HERE, "libdfd_b200.so")
 _lib = None
 
 FIELDS = ["slip", "hslip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State", "init_t0", "tTn", "tTs1", "tTs2",
-          "str_peak", "friction", "united", "faultgrid", "split", "T1", "hT1"]
+          "str_peak", "friction", "united", "faultgrid", "split", "T1", "hT1", "TP_T", "TP_P"]
 STATUS = {0: "ok", 1: "bad or unsupported parameter", 2: "CUDA error", 3: "file missing or malformed",
           4: "call out of order", 5: "DT above the stability limit", 6: "non-finite fault state",
           7: "Newton solve hit its iteration cap"}
@@ -181,6 +182,7 @@ class DfdParams(ctypes.Structure):
         ("use_cerjan", ctypes.c_int), ("normal_refine", ctypes.c_int), ("rs_guess", ctypes.c_int),
         ("OUT", ctypes.c_char * 1024), ("Fault_geometry", ctypes.c_char * 1024),
         ("Fault_init_stress", ctypes.c_char * 1024), ("Media1D", ctypes.c_char * 1024),
+        ("TP_n", ctypes.c_int),
     ]
 
 
@@ -203,6 +205,7 @@ def lib():
             "dfd_params_default": [P(DfdParams)], "dfd_params_load_json": [ctypes.c_char_p, P(DfdParams)],
             "dfd_create": [P(DfdParams), I, P(V)], "dfd_destroy": [V], "dfd_dims": [V, P(I), P(I), P(I)],
             "dfd_load_fault_geometry": [V, V], "dfd_load_media1d": [V, I, V], "dfd_load_fault_init": [V, V],
+            "dfd_load_tp_hy": [V, V], "dfd_get_tp_columns": [V, I, V],
             "dfd_precompute": [V], "dfd_stage": [V, I, I], "dfd_step": [V, I], "dfd_run": [V, I, I],
             "dfd_synchronize": [V], "dfd_get_wave": [V, V], "dfd_set_wave": [V, V], "dfd_get_metric": [V, V],
             "dfd_get_fault": [V, I, V], "dfd_get_slice": [V, I, I, V], "dfd_get_slice_noalloc": [V, I, I, V], "dfd_check_finite": [V],
@@ -276,7 +279,10 @@ class Simulation:
             self._check(L.dfd_load_fault_geometry(self.h, a.ctypes.data))
         if stress is not None:
             a = np.ascontiguousarray(stress, np.float32)
-            self._check(L.dfd_load_fault_init(self.h, a.ctypes.data))
+            self._check(L.dfd_load_fault_init(self.h, a[:15].ctypes.data))
+            if a.shape[0] > 15:  # TP_hy, the 16th variable of the init file (Friction_type 3)
+                hy = np.ascontiguousarray(a[15])
+                self._check(L.dfd_load_tp_hy(self.h, hy.ctypes.data))
         if layers is not None:
             a = np.ascontiguousarray(layers, np.float32)
             self._check(L.dfd_load_media1d(self.h, a.shape[0], a.ctypes.data))
@@ -339,6 +345,12 @@ class Simulation:
         else:
             out = np.empty((self.NZ, self.NY), np.float32)
         self._check(lib().dfd_get_fault(self.h, f, out.ctypes.data))
+        return out
+
+    def tp_columns(self, name):
+        """Thermal-pressurisation columns "TP_T" or "TP_P", (TP_n, NZ, NY), point 0 on the fault."""
+        out = np.empty((self.p.TP_n, self.NZ, self.NY), np.float32)
+        self._check(lib().dfd_get_tp_columns(self.h, ("TP_T", "TP_P").index(name), out.ctypes.data))
         return out
 
     def slice(self, axis, index):

@@ -59,7 +59,9 @@ enum Plane {
   P_VS1, P_VS2, P_TN, P_TS1, P_TS2, P_SLIP, P_STATE, P_T0,
   P_MSLIP, P_TSLIP, P_HSLIP, P_MSTATE, P_TSTATE, P_TTN, P_TTS1,
   P_TTS2, P_SX, P_SY, P_SZ, P_T0X, P_T0Y, P_T0Z, P_DT0X, P_DT0Y, P_DT0Z, P_PEAK, P_DC, P_C0, P_A, P_B, P_L, P_VW,
-  P_FRIC, P_CSLIP, P_CSTATE, NPLANE  // last two: compensation terms of slip and state
+  P_FRIC, P_CSLIP, P_CSTATE,  // the two compensation terms of slip and state
+  P_TPT0, P_TPP0,              // thermal pressurisation: T and P at the fault
+  NPLANE
 };
 enum IPlane { I_T0FLAG, I_FLAGRUP, I_UNITED, I_FAULTGRID, I_RUPY, I_RUPZ, NIPLANE };
 
@@ -106,6 +108,10 @@ struct dfd_ctx {
   float *tab = nullptr, *tabf = nullptr, *vecn = nullptr, *vecs1 = nullptr, *vecs2 = nullptr, *rhof = nullptr;
   float* pl = nullptr;
   int* ipl = nullptr;
+  // thermal pressurisation (Friction_type 3): node-major columns of TP_n points per fault
+  // node and the diffusivity
+  float *tp_T = nullptr, *tp_P = nullptr, *tp_hy = nullptr;
+  std::vector<float> tp_hy_h;
   unsigned long long* newton = nullptr;
   int* it_dev = nullptr;
   int* flag_dev = nullptr;
@@ -294,6 +300,11 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
     if (!rc) rc = dalloc(ctx, &ctx->rhof, 2 * d.nyz);
     if (!rc) rc = dalloc(ctx, &ctx->pl, (long long)NPLANE * d.nj * d.nk);
     if (!rc) rc = dalloc(ctx, &ctx->ipl, (long long)NIPLANE * d.nj * d.nk);
+    if (q.Friction_type == 3) {
+      if (!rc) rc = dalloc(ctx, &ctx->tp_T, (long long)q.TP_n * d.nj * d.nk);
+      if (!rc) rc = dalloc(ctx, &ctx->tp_P, (long long)q.TP_n * d.nj * d.nk);
+      if (!rc) rc = dalloc(ctx, &ctx->tp_hy, (long long)d.nj * d.nk);
+    }
   }
   if (!rc) rc = dalloc(ctx, &ctx->newton, 2);
   if (!rc) rc = dalloc(ctx, &ctx->it_dev, 1);
@@ -373,6 +384,14 @@ int dfd_load_fault_init(dfd_ctx* ctx, const float* planes) {
   if (!ctx || !planes) return DFD_ERR_PARAM;
   size_t n = 15ull * ctx->p.NY * ctx->p.NZ;
   ctx->planes.assign(planes, planes + n);
+  ctx->ready = false;
+  return DFD_OK;
+}
+
+int dfd_load_tp_hy(dfd_ctx* ctx, const float* tp_hy) {
+  if (!ctx || !tp_hy) return DFD_ERR_PARAM;
+  if (ctx->p.Friction_type != 3) return fail(ctx, DFD_ERR_STATE, "TP_hy is read for Friction_type 3 only");
+  ctx->tp_hy_h.assign(tp_hy, tp_hy + (size_t)ctx->p.NY * ctx->p.NZ);
   ctx->ready = false;
   return DFD_OK;
 }
@@ -486,6 +505,15 @@ int dfd_precompute(dfd_ctx* ctx) {
     for (auto& u : up)
       CK(cudaMemcpyAsync(ctx->pl + u.plane * nf, u.v->data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(ctx->pl + P_CSLIP * nf, 0, sizeof(float) * 2 * nf, s));
+    if (ctx->tp_T) {
+      // zero columns (alloc.cu:117-118); the diffusivity from dfd_load_tp_hy, else zero
+      CK(cudaMemsetAsync(ctx->tp_T, 0, sizeof(float) * p.TP_n * nf, s));
+      CK(cudaMemsetAsync(ctx->tp_P, 0, sizeof(float) * p.TP_n * nf, s));
+      if (ctx->tp_hy_h.size() == nf)
+        CK(cudaMemcpyAsync(ctx->tp_hy, ctx->tp_hy_h.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
+      else
+        CK(cudaMemsetAsync(ctx->tp_hy, 0, sizeof(float) * nf, s));
+    }
     struct { int plane; std::vector<int>* v; } iup[] = {
         {I_UNITED, &h.united}, {I_FAULTGRID, &h.faultgrid}, {I_RUPY, &h.rupy}, {I_RUPZ, &h.rupz}};
     ctx->n_band_columns = 0;
@@ -549,6 +577,7 @@ static FaultArgs fault_args(dfd_ctx* ctx, int pattern, int irk) {
     fa.slip = pl(P_SLIP); fa.mslip = pl(P_MSLIP); fa.tslip = pl(P_TSLIP); fa.hslip = pl(P_HSLIP);
     fa.State = pl(P_STATE); fa.mState = pl(P_MSTATE); fa.tState = pl(P_TSTATE);
     fa.cslip = pl(P_CSLIP); fa.cState = pl(P_CSTATE);
+    fa.tpP = ctx->tp_P ? pl(P_TPP0) : nullptr;  // null unless Friction_type 3
     fa.Vs1 = pl(P_VS1); fa.Vs2 = pl(P_VS2); fa.Tn = pl(P_TN); fa.Ts1 = pl(P_TS1); fa.Ts2 = pl(P_TS2);
     fa.tTn = pl(P_TTN); fa.tTs1 = pl(P_TTS1); fa.tTs2 = pl(P_TTS2);
     fa.sx = pl(P_SX); fa.sy = pl(P_SY); fa.sz = pl(P_SZ);
@@ -625,6 +654,17 @@ static long long interior_nodes(dfd_ctx* ctx, const VolPlan& pl) {
   return n;
 }
 
+static TpArgs tp_args(dfd_ctx* ctx) {
+  const int nf = ctx->d.nj * ctx->d.nk;
+  auto pl = [&](int k) { return ctx->pl + (size_t)k * nf; };
+  TpArgs t;
+  t.nf = nf; t.n = ctx->p.TP_n; t.DT = (float)ctx->p.DT;
+  t.united = ctx->ipl + I_UNITED * nf;
+  t.Vs1 = pl(P_VS1); t.Vs2 = pl(P_VS2); t.Tn = pl(P_TN); t.friction = pl(P_FRIC); t.hy = ctx->tp_hy;
+  t.T = ctx->tp_T; t.P = ctx->tp_P; t.T0 = pl(P_TPT0); t.P0 = pl(P_TPP0);
+  return t;
+}
+
 static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr,
                          cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr, cudaEvent_t* nb = nullptr,
                          cudaEvent_t* ne = nullptr) {
@@ -633,6 +673,8 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   int FX = kFlags[pattern][0] * sg, FY = kFlags[pattern][1] * sg, FZ = kFlags[pattern][2] * sg;
   static const int bin[4] = {0, 1, 2, 1};
   FaultArgs fa;
+  // thermal pressurisation once per step, before the stages (main.cu:444-447)
+  if (p.rupture && irk == 0 && ctx->tp_T) launch_thermpress(tp_args(ctx), ctx->s0);
   if (p.rupture) {
     fa = fault_args(ctx, pattern, irk);
     if (nb) cudaEventRecord(*nb, ctx->s0);
@@ -818,9 +860,26 @@ int dfd_get_fault(dfd_ctx* ctx, int field, float* host) {
     CK(cudaMemcpy(host, ctx->FW[0], sizeof(float) * 18 * ctx->d.nyz, cudaMemcpyDeviceToHost));
   } else if (field == DFD_F_T1) {
     CK(cudaMemcpy(host, ctx->T1, sizeof(float) * 21 * ctx->d.nyz, cudaMemcpyDeviceToHost));
-  } else {
+  } else if (field == DFD_F_HT1) {
     CK(cudaMemcpy(host, ctx->hT1, sizeof(float) * 3 * ctx->d.nyz, cudaMemcpyDeviceToHost));
+  } else {
+    if (!ctx->tp_T) return fail(ctx, DFD_ERR_STATE, "thermal pressurisation is off (Friction_type != 3)");
+    CK(cudaMemcpy(host, ctx->pl + (field == DFD_F_TP_T ? P_TPT0 : P_TPP0) * nf, sizeof(float) * nf,
+                  cudaMemcpyDeviceToHost));
   }
+  return DFD_OK;
+}
+
+int dfd_get_tp_columns(dfd_ctx* ctx, int which, float* host) {
+  if (!ctx || !host || which < 0 || which > 1) return DFD_ERR_PARAM;
+  if (!ctx->tp_T) return fail(ctx, DFD_ERR_STATE, "thermal pressurisation is off (Friction_type != 3)");
+  CK(cudaStreamSynchronize(ctx->s0));
+  const size_t n = ctx->p.TP_n, nf = (size_t)ctx->d.nj * ctx->d.nk;
+  std::vector<float> col(n * nf);
+  CK(cudaMemcpy(col.data(), which ? ctx->tp_P : ctx->tp_T, sizeof(float) * n * nf, cudaMemcpyDeviceToHost));
+  // node-major on the device, plane-major (the reference's layout) for the caller
+  for (size_t q = 0; q < nf; q++)
+    for (size_t i = 0; i < n; i++) host[i * nf + q] = col[q * n + i];
   return DFD_OK;
 }
 
@@ -1060,7 +1119,10 @@ static void out_writer(dfd_ctx* ctx) {
       ok = ok && ctx->ncf.put_fixed(ctx->vf[3], h + 7 * nf);
       ok = ok && ctx->ncf.put_record(17, rec, h + 8 * nf);
       ok = ok && ctx->ncf.put_record(18, rec, h + 9 * nf);
-      for (int v = 19; v < 22; v++) ok = ok && ctx->ncf.put_record(v, rec, zero.data());
+      ok = ok && ctx->ncf.put_record(19, rec, zero.data());  // rup_sensor: not computed
+      // TP_T, TP_P at the fault (io_fault.cu:263-265), zero without thermal pressurisation
+      ok = ok && ctx->ncf.put_record(20, rec, ctx->tp_T ? h + 10 * nf : zero.data());
+      ok = ok && ctx->ncf.put_record(21, rec, ctx->tp_T ? h + 11 * nf : zero.data());
       ok = ok && ctx->ncf.sync();
     }
     for (int a = 0; a < 3 && !e; a++) {
@@ -1172,7 +1234,9 @@ int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
   OutState* o = new OutState();
   ctx->out = o;
   o->nf = (size_t)d.nj * d.nk;
-  size_t off = p.rupture ? 10 * o->nf : 0;
+  // record planes: the seven outputs, init_t0, rup_index_y/z, then TP_T and TP_P at the
+  // fault when thermal pressurisation is on
+  size_t off = p.rupture ? (ctx->tp_T ? 12 : 10) * o->nf : 0;
   for (int a = 0; a < 3; a++) {
     if (idx[a] < 0 || idx[a] >= lim[a]) continue;
     const int na = a == 0 ? d.nk : d.ni, nb = a == 1 ? d.nk : d.nj;
@@ -1219,6 +1283,10 @@ int dfd_output_write(dfd_ctx* ctx, int it_skip) {
     CK(cudaMemcpyAsync(dst + 7 * nf, ctx->pl + P_T0 * nf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
     CK(cudaMemcpyAsync(dst + 8 * nf, ctx->ipl + I_RUPY * nf, sizeof(int) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
     CK(cudaMemcpyAsync(dst + 9 * nf, ctx->ipl + I_RUPZ * nf, sizeof(int) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
+    if (ctx->tp_T) {
+      CK(cudaMemcpyAsync(dst + 10 * nf, ctx->pl + P_TPT0 * nf, sizeof(float) * 2 * nf, cudaMemcpyDeviceToDevice,
+                         ctx->s0));
+    }
   }
   const int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y, ctx->p.EXPORT_WAVE_SLICE_Z};
   for (int a = 0; a < 3; a++)
@@ -1426,6 +1494,9 @@ static int ens_build(dfd_ens* e) {
 static int ens_enqueue(dfd_ens* e, int pat, int irk) {
   const EnsStage& S = e->st[pat][irk];
   const int nr = (int)e->rup.size(), n = (int)e->sc.size();
+  if (irk == 0)
+    for (int r : e->rup)
+      if (e->sc[r]->tp_T) launch_thermpress(tp_args(e->sc[r]), e->s0);
   if (nr) launch_fault_node_batch(S.fault, S.fstart, nr, S.fblocks, S.FY, S.FZ, e->s0);
   if (e->sc[0]->serial) {
     launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);

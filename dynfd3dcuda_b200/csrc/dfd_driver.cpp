@@ -51,6 +51,15 @@ int main(int argc, char** argv) {
       }
     }
     dfd_load_fault_init(ctx, s.data());
+    if (p.Friction_type == 3) {
+      // hydraulic diffusivity of the thermal pressurisation (init.cu:999-1003)
+      std::vector<float> hy(nf);
+      if (!dfd::nc_read_plane(p.Fault_init_stress, "TP_hy", p.NZ, p.NY, hy.data(), &err)) {
+        fprintf(stderr, "%s\n", err.c_str());
+        return 1;
+      }
+      dfd_load_tp_hy(ctx, hy.data());
+    }
   }
   if (p.Media1D[0]) {
     FILE* f = fopen(p.Media1D, "r");

@@ -441,6 +441,10 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int 
     for (int c = 0; c < 3; c++) Tl[c] = T0l[c] - 2.0 * (M0 * M1 * Rl[c] / dt1 + M0 * Rr[c][1] - M1 * Rr[c][0]) / den;
     double cc = -((double)DFD_A0P - (double)DFD_A0M) * dt1 * jacvec / ((double)jac_last * rho_last * dDH);
     double tn = Tl[0] >= -1e-1 ? -1e-1 : Tl[0];
+    // thermal pressurisation: the friction law sees the effective normal stress tn + P at
+    // the fault; the traction put back keeps (tn + P) - P (trial_ratestate.cu:636-643, 787-790)
+    const float Pf = a.tpP ? a.tpP[q2] : 0.0f;
+    tn += Pf;
     double Vt1 = cc * Tl[1], Vt2 = cc * Tl[2];
     double ra = a.a[q2], st = a.State[q2];
     double coef = cc * ra * fabs(tn);
@@ -500,6 +504,7 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int 
     double ts1 = Tl[1] / Ttn * T, ts2 = Tl[2] / Ttn * T;
     float Vf = fmaxf((float)V, 1e-30f);
 #pragma unroll
+    tn -= Pf;
     for (int c = 0; c < 3; c++) Tau[c] = (float)(tn * nv[c] + ts1 * s1[c] + ts2 * s2[c]);
     Tau[0] = a.sx[q2];  // the normal-traction perturbation is forced to zero (:797)
     Tau_n = Tau[0] * nv[0] + Tau[1] * nv[1] + Tau[2] * nv[2];
@@ -912,6 +917,159 @@ __global__ void __launch_bounds__(128, 4) fault_band_batch(const FaultArgs* __re
   const int gx = (a.d.nj + 31) / 32, gxy = gx * ((a.d.nk + 3) / 4);
   // the scenario's blocks: seven parts of its (32, 4)-block grid
   fault_band_body<FX, FY, FZ>(a, (loc % gxy) % gx, (loc % gxy) / gx, loc / gxy);
+}
+
+// Thermal pressurisation (thermpress.cu:22-236), once per step before the stages.  Each
+// fault node carries a column of n points normal to the fault with temperature T and pore
+// pressure P; nsub explicit sub-steps of
+//   dT = alpha_th T'' + omega(x),  dP = alpha_hy P'' + Lambda dT,
+// with mirrored ends, the frictional work tau V = -friction (Tn + P0) V spread as a Gaussian
+// of half-width h = 20 mm, column width sqrt(100 alpha_max), spacing width / (n - 1) and
+// sub-step 0.1 dh^2 / alpha_max, so nsub grows as (n - 1)^2.  The second differences and the
+// Gaussian are evaluated in double as the reference's double literals make them; stored
+// values are FP32.  Columns are node-major ([q][i]); point 0 of T and P is also written to
+// two (NZ, NY) planes, which the friction law and the outputs read.
+
+// per-node scalars of the scheme (thermpress.cu:150-175), as the reference rounds them
+struct TpNode {
+  float rate, Tau_n, fr, ahy, dh, dh2, dt;
+  int nsub;
+  double fden;
+};
+__device__ __forceinline__ TpNode tp_node(const TpArgs& a, int q) {
+  const float rho_c = 2.7e6f, h = 20e-3f, alpha_th = 1.0e-6f;
+  TpNode t;
+  const float vs1 = a.Vs1[q], vs2 = a.Vs2[q];
+  t.rate = sqrtf(vs1 * vs1 + vs2 * vs2);
+  t.Tau_n = a.Tn[q];
+  t.fr = a.friction[q];
+  t.ahy = a.hy[q];
+  const float amax = fmaxf(alpha_th, t.ahy);
+  const float w = (float)sqrt(4.0 * (double)amax * 25.0);
+  t.dh = (float)((double)w / (double)(a.n - 1));
+  t.dh2 = t.dh * t.dh;
+  const float dt0 = (float)(0.1 * (double)t.dh2 / (double)amax);
+  t.nsub = (int)(a.DT / dt0) + 1;
+  t.dt = (float)((double)a.DT / (double)t.nsub);
+  t.fden = (double)(rho_c * h) * 2.506628274631000;
+  return t;
+}
+
+// one point: new T and P from the old values of the point (c) and its plus (r) and minus
+// (l) neighbours; g = exp(-x^2 / 2h^2) in double, fac = tau V / (rho_c h sqrt(2 pi))
+__device__ __forceinline__ void tp_point(const TpNode& t, double g, double fac, float Tc, float Tr, float Tl, float Pc,
+                                         float Pr, float Pl, float* To, float* Po) {
+  const float Lamb = 0.1e6f, alpha_th = 1.0e-6f;
+  const float omega = (float)(g * fac);
+  const float dT = (float)((double)alpha_th * ((double)Tr - 2.0 * (double)Tc + (double)Tl) / (double)t.dh2 +
+                           (double)omega);
+  const float dP = (float)((double)t.ahy * ((double)Pr - 2.0 * (double)Pc + (double)Pl) / (double)t.dh2 +
+                           (double)(Lamb * dT));
+  *To = fmaf(t.dt, dT, Tc);
+  *Po = fmaf(t.dt, dP, Pc);
+}
+
+__device__ __forceinline__ double tp_gauss(const TpNode& t, int i) {
+  const float h = 20e-3f, h2 = h * h;
+  const float x = (float)i * t.dh;
+  const float x2 = x * x;
+  return exp(-0.5 * (double)x2 / (double)h2);
+}
+
+// One warp per node for n <= 32 K: lane l holds points l + 32 m (m < K) in registers, so a
+// column is read and written once per step (coalesced: the points of a column are
+// contiguous) and every sub-step runs in registers, the neighbours exchanged by shuffles.
+template <int K>
+__global__ void __launch_bounds__(256) thermpress_warp_kernel(const TpArgs a) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int q = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);  // uniform in the warp
+  if (q >= a.nf || a.united[q]) return;
+  const TpNode t = tp_node(a, q);
+  const int n = a.n;
+  float* Tq = a.T + (long long)q * n;
+  float* Pq = a.P + (long long)q * n;
+  float T[K], P[K];
+  double g[K];
+#pragma unroll
+  for (int m = 0; m < K; m++) {
+    const int i = lane + 32 * m;
+    T[m] = i < n ? Tq[i] : 0.0f;
+    P[m] = i < n ? Pq[i] : 0.0f;
+    g[m] = tp_gauss(t, i);
+  }
+  for (int sub = 0; sub < t.nsub; sub++) {
+    const float P0 = __shfl_sync(FULL, P[0], 0);
+    const float tau = -t.fr * (t.Tau_n + P0);
+    const double fac = (double)(tau * t.rate) / t.fden;
+    float Tn[K], Pn[K];
+#pragma unroll
+    for (int m = 0; m < K; m++) {
+      const int i = lane + 32 * m;
+      // plus neighbour: lane + 1 of the same m, lane 0 of m + 1 for lane 31
+      float Tr = __shfl_down_sync(FULL, T[m], 1), Pr = __shfl_down_sync(FULL, P[m], 1);
+      const float Tr2 = __shfl_sync(FULL, m + 1 < K ? T[m + 1 < K ? m + 1 : m] : 0.0f, 0);
+      const float Pr2 = __shfl_sync(FULL, m + 1 < K ? P[m + 1 < K ? m + 1 : m] : 0.0f, 0);
+      // minus neighbour: lane - 1 of the same m, lane 31 of m - 1 for lane 0
+      float Tl = __shfl_up_sync(FULL, T[m], 1), Pl = __shfl_up_sync(FULL, P[m], 1);
+      const float Tl2 = __shfl_sync(FULL, m > 0 ? T[m > 0 ? m - 1 : 0] : 0.0f, 31);
+      const float Pl2 = __shfl_sync(FULL, m > 0 ? P[m > 0 ? m - 1 : 0] : 0.0f, 31);
+      if (lane == 31) { Tr = Tr2; Pr = Pr2; }
+      if (lane == 0) { Tl = Tl2; Pl = Pl2; }
+      // the ends mirror their one neighbour (thermpress.cu:201-207)
+      if (i == 0) { Tl = Tr; Pl = Pr; }
+      if (i == n - 1) { Tr = Tl; Pr = Pl; }
+      tp_point(t, g[m], fac, T[m], Tr, Tl, P[m], Pr, Pl, &Tn[m], &Pn[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < K; m++)
+      if (lane + 32 * m < n) { T[m] = Tn[m]; P[m] = Pn[m]; }
+  }
+#pragma unroll
+  for (int m = 0; m < K; m++) {
+    const int i = lane + 32 * m;
+    if (i < n) { Tq[i] = T[m]; Pq[i] = P[m]; }
+  }
+  if (lane == 0) { a.T0[q] = T[0]; a.P0[q] = P[0]; }
+}
+
+// Longer columns: one thread per node walking its column in place each sub-step, the old
+// value of the point below kept in a register.
+__global__ void __launch_bounds__(128) thermpress_column_kernel(const TpArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.nf || a.united[q]) return;
+  const TpNode t = tp_node(a, q);
+  const int n = a.n;
+  float* T = a.T + (long long)q * n;
+  float* P = a.P + (long long)q * n;
+  for (int sub = 0; sub < t.nsub; sub++) {
+    const float tau = -t.fr * (t.Tau_n + P[0]);
+    const double fac = (double)(tau * t.rate) / t.fden;
+    float Tb = 0.0f, Pb = 0.0f;  // old values of point i - 1
+    float Tc = T[0], Pc = P[0];  // old values of point i
+    for (int i = 0; i < n; i++) {
+      float Ta = 0.0f, Pa = 0.0f;  // old values of point i + 1
+      if (i + 1 < n) { Ta = T[i + 1]; Pa = P[i + 1]; }
+      const float Tr = i == n - 1 ? Tb : Ta, Pr = i == n - 1 ? Pb : Pa;
+      const float Tl = i == 0 ? Ta : Tb, Pl = i == 0 ? Pa : Pb;
+      tp_point(t, tp_gauss(t, i), fac, Tc, Tr, Tl, Pc, Pr, Pl, &T[i], &P[i]);
+      Tb = Tc; Pb = Pc;
+      Tc = Ta; Pc = Pa;
+    }
+  }
+  a.T0[q] = T[0];
+  a.P0[q] = P[0];
+}
+
+void launch_thermpress(const TpArgs& a, cudaStream_t s) {
+  const int K = (a.n + 31) / 32;
+  const unsigned wblocks = (unsigned)(((long long)a.nf * 32 + 255) / 256);
+  if (K <= 1) thermpress_warp_kernel<1><<<wblocks, 256, 0, s>>>(a);
+  else if (K <= 2) thermpress_warp_kernel<2><<<wblocks, 256, 0, s>>>(a);
+  else if (K <= 4) thermpress_warp_kernel<4><<<wblocks, 256, 0, s>>>(a);
+  else if (K <= 8) thermpress_warp_kernel<8><<<wblocks, 256, 0, s>>>(a);
+  else if (K <= 16) thermpress_warp_kernel<16><<<wblocks, 256, 0, s>>>(a);
+  else thermpress_column_kernel<<<(a.nf + 127) / 128, 128, 0, s>>>(a);
 }
 
 void launch_fault_node(const FaultArgs& a, cudaStream_t s) {

@@ -113,6 +113,7 @@ void params_default(dfd_params* p) {
   // reference Makefile default switches (Makefile:57-161)
   p->rupture = 1; p->free_surface = 1; p->use_pml = 1; p->use_cerjan = 0; p->normal_refine = 1;
   p->rs_guess = 0;
+  p->TP_n = 1;  // set_params.cu:103
   finalize_params(p);
 }
 
@@ -189,7 +190,8 @@ int params_from_json(const char* text, dfd_params* p, std::string* err) {
     else if (k == "useCerjan") inum(p->use_cerjan);
     else if (k == "NormalRefine") inum(p->normal_refine);
     else if (k == "RS_guess") inum(p->rs_guess);
-    // PX/PY/PZ, igpu, vp1/vs1, TP_n, RupThres, smoothing keys: accepted, not used on one GPU
+    else if (k == "TP_n") inum(p->TP_n);  // set_params.cu:281-282
+    // PX/PY/PZ, igpu, vp1/vs1, RupThres, smoothing keys: accepted, not used on one GPU
   }
   finalize_params(p);
   return DFD_OK;
@@ -199,8 +201,14 @@ int check_params(const dfd_params* p, std::string* err) {
   auto fail = [&](const char* m) { if (err) *err = m; return DFD_ERR_PARAM; };
   if (p->NX < 8 || p->NY < 8 || p->NZ < 8) return fail("NX, NY, NZ must be >= 8");
   if (!(p->DT > 0) || !(p->DH > 0)) return fail("DT and DH must be positive");
-  if (p->Friction_type < 0 || p->Friction_type > 2)
-    return fail("Friction_type must be 0 (slip weakening), 1 (aging law) or 2 (slip law)");
+  if (p->Friction_type < 0 || p->Friction_type > 3)
+    return fail("Friction_type must be 0 (slip weakening), 1 (aging law), 2 (slip law) or 3 (slip law with "
+                "thermal pressurisation)");
+  // the column spacing is width / (TP_n - 1): at the reference's default TP_n = 1 it is
+  // infinite and the heat source at the fault, exp(-(0 * inf)^2 ...), is NaN
+  // (thermpress.cu:167-196)
+  if (p->rupture && p->Friction_type == 3 && (p->TP_n < 2 || p->TP_n > 4096))
+    return fail("Friction_type 3 needs 2 <= TP_n <= 4096 points per thermal-pressurisation column");
   if (p->use_pml && (p->PML_N < 2 || 2 * p->PML_N > p->NX || 2 * p->PML_N > p->NY || p->PML_N > p->NZ))
     return fail("PML_N out of range for the grid");
   if (p->use_pml && p->PML_N > 30)

@@ -152,6 +152,7 @@ struct FaultArgs {
   // (NZ, NY) planes
   float *slip, *mslip, *tslip, *hslip, *State, *mState, *tState;
   float *cslip, *cState;           // compensation terms of the step-to-step sums of slip and state
+  const float* tpP;                // thermal pressurisation: pore pressure at the fault (plane 0), or null
   float *Vs1, *Vs2, *Tn, *Ts1, *Ts2, *tTn, *tTs1, *tTs2;
   float *sx, *sy, *sz;             // str_init
   const float *T0x, *T0y, *T0z, *dT0x, *dT0y, *dT0z;
@@ -283,6 +284,17 @@ void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start
                         int FZ, bool top, cudaStream_t s);
 void launch_fault_node_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FY, int FZ,
                              cudaStream_t s);
+// thermal pressurisation (Friction_type 3): node-major columns of n points across the
+// fault (point i of node q at [q * n + i]), updated once per step before the stages; T0
+// and P0 receive point 0 of every column (dfd_fault.cu)
+struct TpArgs {
+  int nf, n;
+  float DT;
+  const int* united;
+  const float *Vs1, *Vs2, *Tn, *friction, *hy;
+  float *T, *P, *T0, *P0;
+};
+void launch_thermpress(const TpArgs& a, cudaStream_t s);
 void launch_fault_band_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FX, int FY, int FZ,
                              cudaStream_t s);
 

@@ -57,6 +57,9 @@ typedef struct dfd_params {
   char Fault_geometry[1024];
   char Fault_init_stress[1024];
   char Media1D[1024];
+  /* points across the fault of each thermal-pressurisation column (Friction_type 3);
+   * the reference's default is 1, which Friction_type 3 rejects (see dfd_load_tp_hy) */
+  int TP_n;
 } dfd_params;
 
 typedef struct dfd_ctx dfd_ctx;
@@ -69,6 +72,9 @@ enum {
   DFD_F_SPLIT,                               /* (9, 2, nz, ny) split-node state   */
   DFD_F_T1,                                  /* (3, 7, nz, ny) T11 T12 T13 layers */
   DFD_F_HT1,                                 /* (3, nz, ny) hT11 hT12 hT13        */
+  DFD_F_TP_T, DFD_F_TP_P,                    /* thermal pressurisation: temperature and pore
+                                                pressure at the fault (point 0 of each column,
+                                                as io_fault.cu:263-265 writes them) */
   DFD_F_COUNT
 };
 
@@ -92,6 +98,10 @@ int dfd_load_fault_geometry(dfd_ctx *ctx, const float *fxyz);
 int dfd_load_media1d(dfd_ctx *ctx, int n, const float *layers);
 /* 15 planes of (NZ, NY): Tx Ty Tz dTx dTy dTz mu_s mu_d Dc C0 a b L Vw State */
 int dfd_load_fault_init(dfd_ctx *ctx, const float *planes);
+/* Friction_type 3 only: hydraulic diffusivity TP_hy (m^2/s), one plane of (NZ, NY), the
+ * TP_hy variable of the Fault_init_stress file (init.cu:999-1003); zero if never loaded.
+ * DFD_ERR_STATE for any other friction type. */
+int dfd_load_tp_hy(dfd_ctx *ctx, const float *tp_hy);
 
 /* ---- setup: grid, metric and media on the GPU in FP64 (no 3-D coordinate array), PML
  *      and Cerjan profiles on the host, fault and free-surface coefficient tables on the
@@ -118,6 +128,9 @@ int dfd_set_wave(dfd_ctx *ctx, const float *host);  /* 9*nx*ny*nz */
 int dfd_get_metric(dfd_ctx *ctx, float *host);      /* 13*nx*ny*nz: xix..ztz jac lam mu rho */
 int dfd_get_fault(dfd_ctx *ctx, int field, float *host);
 int dfd_get_slice(dfd_ctx *ctx, int axis, int index, float *host);  /* Vx,Vy,Vz on one slice */
+/* thermal pressurisation columns (Friction_type 3): which 0 = temperature TP_T, 1 = pore
+ * pressure TP_P, (TP_n, NZ, NY) float32, point 0 on the fault (alloc.cu:111-116 layout) */
+int dfd_get_tp_columns(dfd_ctx *ctx, int which, float *host);
 /* enqueue (asynchronously, after the work already issued) a copy of the eight per-step
  * on-fault output planes Vs1 Vs2 Tn Ts1 Ts2 slip State init_t0, (8, NZ, NY), into host
  * memory (pinned for a true async copy); completes at the next dfd_synchronize */

@@ -45,6 +45,7 @@ typedef struct {
   int Asp_grid[4];
   double bi_vp1, bi_vs1, bi_rho1, bi_vp2, bi_vs2, bi_rho2;
   int free_surface, use_pml, use_cerjan, normal_refine;
+  int TP_n;  // points across the fault of the thermal-pressurisation columns (Friction_type 3)
 } orc_params;
 }
 
@@ -170,6 +171,8 @@ template <typename R> struct Sim {
   std::vector<R> T0x, T0y, T0z, dT0x, dT0y, dT0z, str_peak, mu_d, Dc, C0, a, b, L, Vw;
   std::vector<R> hslip, slip, tslip, mslip, Vs1, Vs2, State, mState, hState, tState;
   std::vector<R> init_t0, friction;
+  // thermal pressurisation: columns of TP_n points, plane i at [i * nf] (alloc.cu:94-118)
+  std::vector<R> TP_T, TP_P, TP_hy;
   std::vector<int> init_t0_flag, rup_index_y, rup_index_z, united, faultgrid, flag_rup;
   // bookkeeping for the learned-guess study: Newton iterations of the last RS trial
   long newton_iters = 0;
@@ -199,6 +202,8 @@ template <typename R> struct Sim {
                     &tslip, &mslip, &Vs1, &Vs2, &State, &mState, &hState, &tState, &init_t0, &friction})
       v->assign(nf, 0);
     for (auto* v : {&init_t0_flag, &rup_index_y, &rup_index_z, &united, &faultgrid, &flag_rup}) v->assign(nf, 0);
+    const int ntp = std::max(p.TP_n, 1);
+    TP_T.assign(ntp * nf, 0); TP_P.assign(ntp * nf, 0); TP_hy.assign(nf, 0);
   }
 
   // PML damping profiles (init_pml.cu:18-133): d ~ x^2, alpha ~ (1-x), beta ~ 1+(bmax-1)x^2,
@@ -1068,8 +1073,10 @@ template <typename R> struct Sim {
         double cc = -(A0P - A0M) * dt1 * jacvec / (t.jac_last * t.rho_last * p.DH);
         double Tau_n = Tl[0] >= -1e-1 ? -1e-1 : Tl[0];
         double Vt[3] = {cc * Tl[0], cc * Tl[1], cc * Tl[2]};
-        double Pf = 0;
-        if (p.Friction_type == 3) { Pf = 0; Tau_n += Pf; }  // thermal pressurisation is out of scope (TP_P == 0)
+        // thermal pressurisation: the pore pressure at the fault makes the normal stress of
+        // the friction law effective (trial_ratestate.cu:636-643)
+        R Pf = 0;
+        if (p.Friction_type == 3) { Pf = TP_P[q2]; Tau_n += Pf; }
         double ra = a[q2], st = State[q2];
         double coef = cc * ra * std::fabs(Tau_n);
         double Vtn = std::sqrt(Vt[1] * Vt[1] + Vt[2] * Vt[2]);
@@ -1371,9 +1378,58 @@ template <typename R> struct Sim {
       }
   }
 
+  // Thermal pressurisation (thermpress.cu:22-236), once per step before the stages
+  // (main.cu:444-447).  Per non-united node: nt_sub explicit sub-steps of 1-D diffusion of
+  // temperature T and pore pressure P over TP_n points normal to the fault (mirror ends),
+  // heated by the frictional work tau*V spread as a Gaussian of half-width h:
+  //   dT = alpha_th T'' + omega(x),  dP = alpha_hy P'' + Lambda dT,
+  // tau = -friction (Tn + P[0]); column width sqrt(100 alpha_max), sub-step 0.1 dh^2/alpha_max.
+  // Types as the reference's: real_t locals, the double literals promote the second
+  // differences and the Gaussian to double.
+  void thermpress() {
+    const R Lamb = (R)0.1e6, rho_c = (R)2.7e6, h = (R)20e-3, alpha_th = (R)1.0e-6;
+    const R h2 = h * h;
+    const double SQRT2PI = 2.506628274631000;
+    const long nf = (long)nj * nk;
+    const int n = p.TP_n;
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < nf; q++) {
+      if (united[q]) continue;
+      R rate = std::sqrt(Vs1[q] * Vs1[q] + Vs2[q] * Vs2[q]);
+      R Tau_n = Tn[q], fr = friction[q], ahy = TP_hy[q];
+      R amax = std::max(alpha_th, ahy);
+      R w = (R)std::sqrt(4.0 * amax * 25.0);
+      R dh = (R)(w / (double)(n - 1));
+      R dh2 = dh * dh;
+      R dt = (R)(0.1 * dh2 / amax);
+      int nsub = (int)((R)p.DT / dt) + 1;
+      dt = (R)((R)p.DT / (double)nsub);
+      std::vector<R> dT(n), dP(n);
+      for (int sub = 0; sub < nsub; sub++) {
+        R tau = -fr * (Tau_n + TP_P[q]);
+        R tauV = tau * rate;
+        for (int i = 0; i < n; i++) {
+          R x = i * dh;
+          R x2 = x * x;
+          R omega = (R)(std::exp(-0.5 * x2 / h2) * (tauV / (rho_c * h * SQRT2PI)));
+          long c = q + i * nf;
+          long pl = i == n - 1 ? c - nf : c + nf;  // the ends mirror their one neighbour
+          long mi = i == 0 ? c + nf : c - nf;
+          dT[i] = (R)(alpha_th * (TP_T[pl] - 2.0 * TP_T[c] + TP_T[mi]) / dh2 + omega);
+          dP[i] = (R)(ahy * (TP_P[pl] - 2.0 * TP_P[c] + TP_P[mi]) / dh2 + Lamb * dT[i]);
+        }
+        for (int i = 0; i < n; i++) {
+          TP_T[q + i * nf] += dt * dT[i];
+          TP_P[q + i * nf] += dt * dP[i];
+        }
+      }
+    }
+  }
+
   // One time step: four RK stages with the reference's launch order (main.cu:420-535).
   void step(int it) {
     int FX = FD_FLAGS[it % 8][0], FY = FD_FLAGS[it % 8][1], FZ = FD_FLAGS[it % 8][2];
+    if (p.Friction_type == 3) thermpress();
     for (int irk = 0; irk < 4; irk++) {
       state_rk(irk);
       if (p.Friction_type == 0) trial_sw(it, irk, FX, FY, FZ);
@@ -1434,6 +1490,7 @@ template <typename R> struct Sim {
         {"tTs1", &tTs1}, {"tTs2", &tTs2}, {"str_init_x", &str_init_x}, {"str_init_y", &str_init_y},
         {"str_init_z", &str_init_z}, {"slip", &slip}, {"hslip", &hslip}, {"Vs1", &Vs1}, {"Vs2", &Vs2},
         {"State", &State}, {"init_t0", &init_t0}, {"friction", &friction}, {"str_peak", &str_peak},
+        {"TP_T", &TP_T}, {"TP_P", &TP_P}, {"TP_hy", &TP_hy},
         {"matVx2Vz", &matVx2Vz}, {"matVy2Vz", &matVy2Vz}, {"damp", &damp}, {"Bx", &Bx}, {"By", &By},
         {"Bz", &Bz}, {"Dx", &Dx}, {"Dy", &Dy}, {"Dz", &Dz}, {"Ax", &Ax}, {"Ay", &Ay}, {"Az", &Az},
         {"aux_x1", &aux[0][0]}, {"aux_x2", &aux[1][0]}, {"aux_y1", &aux[2][0]}, {"aux_y2", &aux[3][0]},

@@ -24,7 +24,7 @@ DEFAULTS = dict(
     Fault_grid=[0, 0, 0, 0], Asp_grid=[0, 0, 0, 0],
     bi_vp1=6000.0, bi_vs1=3464.0, bi_rho1=2670.0,
     bi_vp2=6000.0, bi_vs2=3464.0, bi_rho2=2670.0,
-    FreeSurface=1, usePML=1, useCerjan=0, NormalRefine=1,
+    FreeSurface=1, usePML=1, useCerjan=0, NormalRefine=1, TP_n=1,
 )
 
 
@@ -44,7 +44,7 @@ class OrcParams(ctypes.Structure):
         ("bi_vp1", ctypes.c_double), ("bi_vs1", ctypes.c_double), ("bi_rho1", ctypes.c_double),
         ("bi_vp2", ctypes.c_double), ("bi_vs2", ctypes.c_double), ("bi_rho2", ctypes.c_double),
         ("free_surface", ctypes.c_int), ("use_pml", ctypes.c_int), ("use_cerjan", ctypes.c_int),
-        ("normal_refine", ctypes.c_int),
+        ("normal_refine", ctypes.c_int), ("TP_n", ctypes.c_int),
     ]
 
 
@@ -85,7 +85,8 @@ def resolve(params):
 def to_struct(params):
     p = resolve(params)
     s = OrcParams()
-    for name in ("NX", "NY", "NZ", "INPORT_GRID_TYPE", "INPORT_STRESS_TYPE", "Friction_type", "PML_N", "DAMP_N"):
+    for name in ("NX", "NY", "NZ", "INPORT_GRID_TYPE", "INPORT_STRESS_TYPE", "Friction_type", "PML_N", "DAMP_N",
+                 "TP_n"):
         setattr(s, name, int(p[name]))
     for name in ("TMAX", "DT", "DH", "PML_velocity", "PML_bmax", "PML_fc", "mu_s", "mu_d", "mu_0", "Dc", "C0",
                  "smooth_load_T", "viscosity", "bi_vp1", "bi_vs1", "bi_rho1", "bi_vp2", "bi_vs2", "bi_rho2"):
@@ -104,7 +105,8 @@ class Oracle:
     """One simulation held by the CPU oracle.
 
     fxyz:   (3, NZ, NY) float32 fault-surface coordinates (the Fault_geometry file), or None
-    stress: (15, NZ, NY) float32 planes Tx,Ty,Tz,dTx,dTy,dTz,mu_s,mu_d,Dc,C0,a,b,L,Vw,State, or None
+    stress: (15, NZ, NY) float32 planes Tx,Ty,Tz,dTx,dTy,dTz,mu_s,mu_d,Dc,C0,a,b,L,Vw,State, or None;
+            a 16th plane TP_hy (hydraulic diffusivity, m^2/s) for thermal pressurisation
     layers: (n, 4) float32 rows depth,rho,vp,vs of a 1-D medium (Media1D file), or None
     """
 
@@ -126,6 +128,8 @@ class Oracle:
         p = self.params
         self.nx, self.ny, self.nz = p["NX"] + 6, p["NY"] + 6, p["NZ"] + 6
         self.nj, self.nk = p["NY"], p["NZ"]
+        if stress is not None and np.asarray(stress).shape[0] > 15:
+            self.set("TP_hy", np.asarray(stress)[15])
 
     def __del__(self):
         if getattr(self, "h", None):

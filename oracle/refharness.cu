@@ -47,6 +47,7 @@ extern void fault_dstrs_b(Wave, Fault, realptr_t M, int, int, int);
 extern void wave_rk(Wave, PML, int irk);
 extern void fault_rk(Fault, int irk);
 extern void state_rk(Fault, int irk);
+extern void thermpress(Wave, Fault, realptr_t M, int it, int irk, int, int, int);
 extern void init_fault_coef(realptr_t M, Fault);
 extern void init_wave_free(realptr_t M, PML, Wave);
 extern void nc_read_init_stress(Fault F);
@@ -97,6 +98,10 @@ static void dump_state(Wave &W, Fault &F, PML &P, int step) {
   DUMP("tTn", step, F.tTn, nf);
   DUMP("tTs1", step, F.tTs1, nf);
   DUMP("tTs2", step, F.tTs2, nf);
+  if (hostParams.Friction_type == 3) {
+    DUMP("TP_T", step, F.TP_T, (size_t)hostParams.TP_n * nf);
+    DUMP("TP_P", step, F.TP_P, (size_t)hostParams.TP_n * nf);
+  }
   if (P.isx1) DUMP("aux_x1", step, P.Wx1, 9 * (size_t)N * nj * nk);
   if (P.isy1) DUMP("aux_y1", step, P.Wy1, 9 * (size_t)N * nk * ni);
   if (P.isz1) DUMP("aux_z1", step, P.Wz1, 9 * (size_t)N * ni * nj);
@@ -255,6 +260,8 @@ int main(int argc, char **argv) {
 
   for (int it = 0; it < nsteps; it++) {
     int FlagX = kFlags[it % 8][0], FlagY = kFlags[it % 8][1], FlagZ = kFlags[it % 8][2];
+    // thermal pressurisation once per step, before the stages (main.cu:444-447)
+    if (!volume && hostParams.Friction_type == 3) thermpress(W, F, M, it, 0, FlagX, FlagY, FlagZ);
     for (int irk = 0; irk < 4; irk++) {
       if (!volume) {
         state_rk(F, irk);

@@ -243,6 +243,14 @@ def get_case(name):
         st = sw_stress(fx, fg, tn=-120e6, ts=-40e6)
         st = rs_fields(st, fx, seed=7, L=0.02, patch=(0.0, -500.0, 600.0), patch_dtau=45e6)
         return p, fx, st, None, None, dict(steps=40, every=20, volume=False)
+    if name == "tp_flat":
+        # rs_flat with thermal pressurisation: 64 points per column, so that the diffusion
+        # sub-cycles (sub-step 10/63^2 s < DT), hydraulic diffusivity log-uniform per node
+        p, fx, st, layers, w0, meta = get_case("rs_flat")
+        p.update(Friction_type=3, TP_n=64)
+        rng = np.random.default_rng(11)
+        hy = np.exp(rng.uniform(np.log(2e-5), np.log(4e-4), size=st.shape[1:])).astype(np.float32)
+        return p, fx, np.concatenate([st, hy[None]]), layers, w0, meta
     if name == "rs_rough":
         return rs_rough_case(76, 24, 40, seed=31, L=0.02, steps=60)
     raise KeyError(name)
@@ -294,7 +302,7 @@ def ensemble_case(i, seed=2025, size=(100, 300), DH=100.0, DT=0.008, steps=1000)
     return p, fx, st
 
 
-CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan"]
+CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan", "tp_flat"]
 
 
 def write_inputs(name, outdir):
@@ -318,7 +326,8 @@ def write_inputs(name, outdir):
         job["Fault_geometry"] = fn
     if st is not None:
         fn = os.path.join(outdir, "init_stress.nc")
-        names = ["Tx", "Ty", "Tz", "dTx", "dTy", "dTz", "mu_s", "mu_d", "Dc", "C0", "a", "b", "L", "Vw", "State"]
+        names = ["Tx", "Ty", "Tz", "dTx", "dTy", "dTz", "mu_s", "mu_d", "Dc", "C0", "a", "b", "L", "Vw", "State",
+                 "TP_hy"][:st.shape[0]]
         with netcdf_file(fn, "w") as f:
             f.createDimension("nz", st.shape[1])
             f.createDimension("ny", st.shape[2])

@@ -5,10 +5,12 @@ by oracle/Makefile, driven in the order of the reference driver) on every case o
 cases.py and stores a compact subset of the dumped state as tests/golden/<case>_<var>.npz:
 
   every dump step : all on-fault 2-D arrays, per-field checksums of the wavefield and of
-                    the PML auxiliary arrays
+                    the PML auxiliary arrays; with thermal pressurisation (Friction_type
+                    3) temperature and pore pressure at the fault
   final step      : the wavefield (full for the volume cases, the seven x-planes around
                     the fault over the rupture block otherwise), split-node state and the
-                    traction layers over the same block
+                    traction layers over the same block; thermal-pressurisation columns
+                    over the non-united block
   setup (dp only) : metric planes around the fault and the fault coefficient tables
 
 Needs a GPU (the reference is CUDA-only).  usage:
@@ -83,6 +85,9 @@ def run_case(name, variant, outdir):
         if not meta["volume"]:
             for nm in ("slip", "hslip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State", "init_t0", "tTn", "tTs1", "tTs2"):
                 save[f"{nm}_s{s}"] = dumps[(nm, s)].astype(np.float32).reshape(NZ, NY)
+            for nm in ("TP_T", "TP_P"):
+                if (nm, s) in dumps:  # thermal pressurisation: the on-fault point of each column
+                    save[f"{nm}_s{s}"] = dumps[(nm, s)].astype(np.float32).reshape(-1, NZ, NY)[0]
     W = dumps[("W", last)].reshape(9, nx, nz, ny)
     if meta["volume"]:
         save["W_final"] = W.astype(np.float32)
@@ -93,6 +98,11 @@ def run_case(name, variant, outdir):
             save[f"{nm}_block"] = dumps[(nm, last)].reshape(7, nz, ny)[..., J0:J1].astype(np.float32)
         for nm in ("hT11", "hT12", "hT13"):
             save[f"{nm}_block"] = dumps[(nm, last)].reshape(nz, ny)[:, J0:J1].astype(np.float32)
+        fg = p["Fault_grid"]
+        for nm in ("TP_T", "TP_P"):
+            if (nm, last) in dumps:  # whole columns over the non-united block
+                col = dumps[(nm, last)].reshape(-1, NZ, NY)
+                save[f"{nm}_cols"] = col[:, fg[2] - 1:fg[3], fg[0] - 1:fg[1]].astype(np.float32)
     if variant.startswith("dp"):
         M = dumps[("M", -1)].reshape(13, nx, nz, ny)
         save["M_planes"] = M[:, i0 - 1:i0 + 2].astype(np.float32)

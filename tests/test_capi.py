@@ -52,6 +52,7 @@ def test_defaults_follow_reference():
     assert (s.rupture, s.free_surface, s.use_pml, s.use_cerjan, s.normal_refine) == (1, 1, 1, 0, 1)
     assert s.OUT == b"output" and s.Fault_geometry == b"Fault_geometry.nc"
     assert s.NT == 100
+    assert s.TP_n == 1  # set_params.cu:103
 
 
 def load_json(tmp_path, job):
@@ -67,7 +68,7 @@ def test_json_keys_and_quirks(tmp_path):
            "Friction_type": 1, "RS_V0": 1e-6, "RS_Vini": 1e-12, "RS_f0": 0.6, "RS_fw": 0.2, "RS_L": 0.02,
            "rho1": 2500.0, "bi_vs2": 3000.0, "PML_N": 12, "PML_velocity": 6000.0, "Fault_grid": [51, 350, 51, 200],
            "Asp_grid": [1, 2, 3, 4], "OUT": "out_dir", "EXPORT_TIME_SKIP": 5, "useCerjan": 1, "FreeSurface": 0,
-           "PX": 2, "igpu": 3}
+           "PX": 2, "igpu": 3, "TP_n": 64}
     r, s = load_json(tmp_path, job)
     assert r == 0
     assert (s.NX, s.NY, s.NZ, s.Friction_type, s.PML_N, s.EXPORT_TIME_SKIP) == (300, 400, 200, 1, 12, 5)
@@ -75,6 +76,7 @@ def test_json_keys_and_quirks(tmp_path):
     assert (s.V0, s.Vini, s.f0, s.fw, s.L) == (1e-6, 1e-12, 0.6, 0.2, 0.02)
     assert list(s.Fault_grid) == [51, 350, 51, 200] and list(s.Asp_grid) == [1, 2, 3, 4]
     assert s.OUT == b"out_dir" and s.use_cerjan == 1 and s.free_surface == 0
+    assert s.TP_n == 64
     # NT = (int)(TMAX / DT) in single precision (set_params.cu:286-295)
     assert s.NT == int(np.float32(5.0031) / np.float32(0.006))
     # unknown and multi-rank keys are accepted and leave the defaults alone
@@ -102,7 +104,10 @@ def test_malformed_and_missing_json(tmp_path):
     assert dfd.lib().dfd_params_load_json(str(tmp_path / "nope.json").encode(), ctypes.byref(s)) == 3
 
 
-@pytest.mark.parametrize("bad", [{"PML_N": 31}, {"Friction_type": 3}, {"NX": 4}, {"DT": 0.0},
+# Friction_type 3 at the reference's default TP_n = 1: the column spacing width / (TP_n - 1)
+# is infinite and the reference's heat source is NaN
+@pytest.mark.parametrize("bad", [{"PML_N": 31}, {"Friction_type": 3}, {"Friction_type": 3, "TP_n": 5000},
+                                 {"Friction_type": 4}, {"NX": 4}, {"DT": 0.0},
                                  {"EXPORT_TIME_SKIP": 0}, {"PML_N": 60, "NY": 100}])
 def test_bad_jobs_rejected_before_device_work(bad):
     """dfd_create validates the job on the host and returns DFD_ERR_PARAM without touching a GPU."""

@@ -127,3 +127,35 @@ def test_fetch_outputs_matches_state():
             np.testing.assert_array_equal(bufs[it][r], b.fault(k).ravel(), err_msg=f"step {it} {k}")
         b.run(it, 1)
     b.close()
+
+
+def test_driver_thermal_pressurisation_records(tmp_path):
+    """Friction_type 3 through the driver: TP_hy comes from the init file's TP_hy variable
+    (init.cu:999-1003) and every record holds temperature and pore pressure at the fault
+    (io_fault.cu:263-265), equal to what the C ABI reads before the same steps."""
+    from scipy.io import netcdf_file
+
+    import dynfd3dcuda_b200 as dfd
+
+    job, meta = cases.write_inputs("tp_flat", str(tmp_path))
+    job.update(EXPORT_TIME_SKIP=4, TMAX=0.16 + 0.004)
+    with open(tmp_path / "params.json", "w") as f:
+        json.dump(job, f)
+    r = subprocess.run([EXE, str(tmp_path / "params.json")], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    NT = int(np.float32(job["TMAX"]) / np.float32(job["DT"]))
+    assert NT == 20
+
+    p, fx, st, _, _, _ = cases.get_case("tp_flat")
+    sim = dfd.Simulation(dict(job), fx, st, None)
+    want = {k: [] for k in ("TP_T", "TP_P", "slip")}
+    for it in range(NT):
+        if it % 4 == 0:
+            for k in want:
+                want[k].append(sim.fault(k))
+        sim.step(it)
+    sim.close()
+    assert np.stack(want["TP_P"]).max() > 1e3  # the pore pressure has started to rise by the last record
+    with netcdf_file(tmp_path / "fault_mpi000000.nc", "r", mmap=False) as f:
+        for nc, k in (("TP_T", "TP_T"), ("TP_P", "TP_P"), ("Us0", "slip")):
+            np.testing.assert_array_equal(np.asarray(f.variables[nc][:]), np.stack(want[k]), err_msg=nc)

@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 
 J0, J1 = 24, 52
 TOL = {"vol_small": 2e-5, "vol_curved": 2e-5, "sw_flat": 2e-4, "sw_flat_nr": 2e-4, "sw_curved": 5e-4,
-       "rs_flat": 2e-3, "sw_cerjan": 2e-4}
+       "rs_flat": 2e-3, "sw_cerjan": 2e-4, "tp_flat": 2e-3}
 
 
 def rel(a, b):
@@ -82,6 +82,11 @@ def test_cuda_matches_oracle(oracle_lib, name, mode):
                 assert rel(a, g[f"{nm}_s{s}"]) < tol, (s, nm, "vs reference FP32 build")
             t0 = sim.fault("init_t0")
             assert np.abs(t0 - o.get("init_t0").reshape(NZ, NY)).max() <= 1.01 * p["DT"]
+            if p.get("Friction_type") == 3:  # thermal pressurisation at the fault
+                for nm in ("TP_T", "TP_P"):
+                    a = sim.fault(nm)
+                    assert rel(a, o.get(nm).reshape(-1, NZ, NY)[0]) < tol, (s, nm)
+                    assert rel(a, g[f"{nm}_s{s}"]) < tol, (s, nm, "vs reference FP32 build")
     sim.check_finite()
     W = sim.wave()
     if meta["volume"]:
@@ -89,6 +94,13 @@ def test_cuda_matches_oracle(oracle_lib, name, mode):
     else:
         assert rel(W[:, i0 - 3:i0 + 4, :, J0:J1], g["W_block"]) < tol
         assert rel(sim.fault("split")[..., J0:J1], g["FW_block"]) < tol
+        if p.get("Friction_type") == 3:  # whole columns across the fault
+            fg = p["Fault_grid"]
+            blk = (slice(None), slice(fg[2] - 1, fg[3]), slice(fg[0] - 1, fg[1]))
+            for nm in ("TP_T", "TP_P"):
+                c = sim.tp_columns(nm)
+                assert rel(c[blk], o.get(nm).reshape(c.shape)[blk]) < tol, nm
+                assert rel(c[blk], g[f"{nm}_cols"]) < tol, (nm, "vs reference FP32 build")
     sim.close()
 
 
@@ -201,3 +213,31 @@ def test_three_streams_equal_one_stream(monkeypatch):
     assert np.array_equal(a.fault("slip"), b.fault("slip"))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("tp_n", [20, 100, 520])
+def test_thermal_pressurisation_column_lengths(oracle_lib, tp_n):
+    """The thermal-pressurisation kernel keeps columns of up to 512 points in registers (one
+    warp per fault node, 1-16 points per lane) and walks longer ones point by point; every
+    variant matches the FP64 oracle (20: one point per lane, 100: four, 520: the column
+    walk, 216 sub-steps per step)."""
+    import dynfd3dcuda_b200 as dfd
+
+    p, fx, st, layers, w0, meta = cases.get_case("tp_flat")
+    p = dict(p, TP_n=tp_n)
+    NZ, NY = p["NZ"], p["NY"]
+    sim = dfd.Simulation(dict(p), fx, st, layers)
+    o = oracle_lib.Oracle(p, fx, st, layers, double=True)
+    steps = 24
+    sim.run(0, steps)
+    for it in range(steps):
+        o.step(it)
+    tol = TOL["tp_flat"]
+    for nm in ("TP_T", "TP_P"):
+        ref = o.get(nm).reshape(tp_n, NZ, NY)
+        assert ref[0].max() > 0  # heated and pressurised by this step
+        assert rel(sim.fault(nm), ref[0]) < tol, nm
+        assert rel(sim.tp_columns(nm), ref) < tol, nm
+    for nm in ("slip", "State"):
+        assert rel(sim.fault(nm), o.get(nm).reshape(NZ, NY)) < tol, nm
+    sim.close()

@@ -25,6 +25,7 @@ TOL = {
     ("sw_curved", "dp"): 3e-5, ("sw_curved", "sp"): 1e-4,
     ("rs_flat", "dp"): 3e-5, ("rs_flat", "sp"): 3e-4,
     ("sw_cerjan", "dp"): 1e-6, ("sw_cerjan", "sp"): 1e-5,
+    ("tp_flat", "dp"): 1e-5, ("tp_flat", "sp"): 3e-4,
 }
 
 
@@ -71,6 +72,9 @@ def test_oracle_matches_reference(oracle_lib, name, var):
             # rupture times are identical to the step
             t0 = o.get("init_t0").reshape(NZ, NY)
             assert np.abs(t0 - g[f"init_t0_s{s}"]).max() < 0.5 * p["DT"]
+            for nm in ("TP_T", "TP_P"):  # thermal pressurisation: the point on the fault
+                if f"{nm}_s{s}" in g:
+                    assert rel(o.get(nm).reshape(-1, NZ, NY)[0], g[f"{nm}_s{s}"]) < tol, (nm, s)
     if meta["volume"]:
         assert rel(o.wave(), g["W_final"]) < tol
     else:
@@ -78,3 +82,8 @@ def test_oracle_matches_reference(oracle_lib, name, var):
         assert rel(o.get("FW").reshape(9, 2, nz, ny)[..., J0:J1], g["FW_block"]) < tol
         for nm in ("T11", "T12", "T13"):
             assert rel(o.get(nm).reshape(7, nz, ny)[..., J0:J1], g[f"{nm}_block"]) < tol, nm
+        fg = p["Fault_grid"]
+        for nm in ("TP_T", "TP_P"):  # whole columns over the non-united block
+            if f"{nm}_cols" in g:
+                col = o.get(nm).reshape(-1, NZ, NY)[:, fg[2] - 1:fg[3], fg[0] - 1:fg[1]]
+                assert rel(col, g[f"{nm}_cols"]) < tol, nm
