@@ -94,3 +94,36 @@ def test_autotune_keeps_results():
         for f in range(9):
             close(wx[f], wy[f], f"field {f}")
     ens.close()
+
+
+def test_ensemble_thermal_pressurisation():
+    """A thermal-pressurisation scenario (Friction_type 3) in a batch: its column update
+    runs once per step before the batched stages and its pore pressure enters the batched
+    friction law; it ends where it ends alone."""
+    import dynfd3dcuda_b200 as dfd
+
+    specs = [make(i) for i in range(3)]
+    p, fx, st = specs[1]  # a rate-and-state scenario
+    hy = np.full(st.shape[1:], 1e-4, np.float32)
+    specs[1] = (dict(p, Friction_type=3, TP_n=40), fx, np.concatenate([st, hy[None]]))
+    singles = [dfd.Simulation(p, fx, st, None) for p, fx, st in specs]
+    batch = [dfd.Simulation(p, fx, st, None) for p, fx, st in specs]
+    ens = dfd.Ensemble(batch)
+    steps = 24
+    ens.run(0, steps)
+    ens.synchronize()
+    for s in singles:
+        s.run(0, steps)
+    assert singles[1].fault("TP_P").max() > 0
+    for i, (a, b) in enumerate(zip(singles, batch)):
+        wa, fa = state(a)
+        wb, fb = state(b)
+        for f in range(9):
+            close(wa[f], wb[f], f"scenario {i} field {f}")
+        for k in fa:
+            close(fa[k], fb[k], f"scenario {i} {k}")
+    for nm in ("TP_T", "TP_P"):
+        close(singles[1].tp_columns(nm), batch[1].tp_columns(nm), nm)
+    ens.close()
+    for s in singles + batch:
+        s.close()
