@@ -45,7 +45,7 @@ for _p in (ROOT, os.path.join(ROOT, "tests", "golden"), os.path.join(ROOT, "orac
         sys.path.insert(0, _p)
 
 ALG_BYTES_PER_NODE_STEP = 768  # 192 floats: stages 39 + 57 + 57 + 39 (stencil input, metric, RK registers)
-LAUNCHES_PER_STEP = 21         # 4 x (fault node + interior + PML + free-surface rows + fault band) + step counter
+LAUNCHES_PER_STEP = 22         # rupture sensor + 4 x (fault node + interior + PML + free-surface rows + fault band) + step counter
 
 
 def workload(name):

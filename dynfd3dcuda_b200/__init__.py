@@ -23,7 +23,7 @@ LIBPATH = os.path.join(_HERE, "libdfd_b200.so")
 _lib = None
 
 FIELDS = ["slip", "hslip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State", "init_t0", "tTn", "tTs1", "tTs2",
-          "str_peak", "friction", "united", "faultgrid", "split", "T1", "hT1", "TP_T", "TP_P"]
+          "str_peak", "friction", "united", "faultgrid", "split", "T1", "hT1", "TP_T", "TP_P", "rup_sensor"]
 STATUS = {0: "ok", 1: "bad or unsupported parameter", 2: "CUDA error", 3: "file missing or malformed",
           4: "call out of order", 5: "DT above the stability limit", 6: "non-finite fault state",
           7: "Newton solve hit its iteration cap"}

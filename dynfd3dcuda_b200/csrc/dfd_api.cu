@@ -61,6 +61,7 @@ enum Plane {
   P_TTS2, P_SX, P_SY, P_SZ, P_T0X, P_T0Y, P_T0Z, P_DT0X, P_DT0Y, P_DT0Z, P_PEAK, P_DC, P_C0, P_A, P_B, P_L, P_VW,
   P_FRIC, P_CSLIP, P_CSTATE,  // the two compensation terms of slip and state
   P_TPT0, P_TPP0,              // thermal pressurisation: T and P at the fault
+  P_RUPS,                      // rupture sensor
   NPLANE
 };
 enum IPlane { I_T0FLAG, I_FLAGRUP, I_UNITED, I_FAULTGRID, I_RUPY, I_RUPZ, NIPLANE };
@@ -665,6 +666,17 @@ static TpArgs tp_args(dfd_ctx* ctx) {
   return t;
 }
 
+static SensorArgs sensor_args(dfd_ctx* ctx) {
+  const int nf = ctx->d.nj * ctx->d.nk;
+  SensorArgs a;
+  a.nj = ctx->d.nj; a.nk = ctx->d.nk;
+  for (int i = 0; i < 4; i++) a.fg[i] = ctx->p.Fault_grid[i];
+  a.united = ctx->ipl + I_UNITED * nf;
+  a.Ts1 = ctx->pl + (size_t)P_TS1 * nf;
+  a.out = ctx->pl + (size_t)P_RUPS * nf;
+  return a;
+}
+
 static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = nullptr, cudaEvent_t* ve = nullptr,
                          cudaEvent_t* kb = nullptr, cudaEvent_t* ke = nullptr, cudaEvent_t* nb = nullptr,
                          cudaEvent_t* ne = nullptr) {
@@ -673,7 +685,9 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   int FX = kFlags[pattern][0] * sg, FY = kFlags[pattern][1] * sg, FZ = kFlags[pattern][2] * sg;
   static const int bin[4] = {0, 1, 2, 1};
   FaultArgs fa;
-  // thermal pressurisation once per step, before the stages (main.cu:444-447)
+  // rupture sensor and thermal pressurisation once per step, before the stages
+  // (main.cu:444-447)
+  if (p.rupture && irk == 0) launch_rup_sensor(sensor_args(ctx), ctx->s0);
   if (p.rupture && irk == 0 && ctx->tp_T) launch_thermpress(tp_args(ctx), ctx->s0);
   if (p.rupture) {
     fa = fault_args(ctx, pattern, irk);
@@ -862,6 +876,8 @@ int dfd_get_fault(dfd_ctx* ctx, int field, float* host) {
     CK(cudaMemcpy(host, ctx->T1, sizeof(float) * 21 * ctx->d.nyz, cudaMemcpyDeviceToHost));
   } else if (field == DFD_F_HT1) {
     CK(cudaMemcpy(host, ctx->hT1, sizeof(float) * 3 * ctx->d.nyz, cudaMemcpyDeviceToHost));
+  } else if (field == DFD_F_RUP_SENSOR) {
+    CK(cudaMemcpy(host, ctx->pl + P_RUPS * nf, sizeof(float) * nf, cudaMemcpyDeviceToHost));
   } else {
     if (!ctx->tp_T) return fail(ctx, DFD_ERR_STATE, "thermal pressurisation is off (Friction_type != 3)");
     CK(cudaMemcpy(host, ctx->pl + (field == DFD_F_TP_T ? P_TPT0 : P_TPP0) * nf, sizeof(float) * nf,
@@ -1119,10 +1135,10 @@ static void out_writer(dfd_ctx* ctx) {
       ok = ok && ctx->ncf.put_fixed(ctx->vf[3], h + 7 * nf);
       ok = ok && ctx->ncf.put_record(17, rec, h + 8 * nf);
       ok = ok && ctx->ncf.put_record(18, rec, h + 9 * nf);
-      ok = ok && ctx->ncf.put_record(19, rec, zero.data());  // rup_sensor: not computed
+      ok = ok && ctx->ncf.put_record(19, rec, h + 10 * nf);  // rup_sensor
       // TP_T, TP_P at the fault (io_fault.cu:263-265), zero without thermal pressurisation
-      ok = ok && ctx->ncf.put_record(20, rec, ctx->tp_T ? h + 10 * nf : zero.data());
-      ok = ok && ctx->ncf.put_record(21, rec, ctx->tp_T ? h + 11 * nf : zero.data());
+      ok = ok && ctx->ncf.put_record(20, rec, ctx->tp_T ? h + 11 * nf : zero.data());
+      ok = ok && ctx->ncf.put_record(21, rec, ctx->tp_T ? h + 12 * nf : zero.data());
       ok = ok && ctx->ncf.sync();
     }
     for (int a = 0; a < 3 && !e; a++) {
@@ -1234,9 +1250,9 @@ int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
   OutState* o = new OutState();
   ctx->out = o;
   o->nf = (size_t)d.nj * d.nk;
-  // record planes: the seven outputs, init_t0, rup_index_y/z, then TP_T and TP_P at the
-  // fault when thermal pressurisation is on
-  size_t off = p.rupture ? (ctx->tp_T ? 12 : 10) * o->nf : 0;
+  // record planes: the seven outputs, init_t0, rup_index_y/z, rup_sensor, then TP_T and
+  // TP_P at the fault when thermal pressurisation is on
+  size_t off = p.rupture ? (ctx->tp_T ? 13 : 11) * o->nf : 0;
   for (int a = 0; a < 3; a++) {
     if (idx[a] < 0 || idx[a] >= lim[a]) continue;
     const int na = a == 0 ? d.nk : d.ni, nb = a == 1 ? d.nk : d.nj;
@@ -1283,8 +1299,9 @@ int dfd_output_write(dfd_ctx* ctx, int it_skip) {
     CK(cudaMemcpyAsync(dst + 7 * nf, ctx->pl + P_T0 * nf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
     CK(cudaMemcpyAsync(dst + 8 * nf, ctx->ipl + I_RUPY * nf, sizeof(int) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
     CK(cudaMemcpyAsync(dst + 9 * nf, ctx->ipl + I_RUPZ * nf, sizeof(int) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
+    CK(cudaMemcpyAsync(dst + 10 * nf, ctx->pl + P_RUPS * nf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, ctx->s0));
     if (ctx->tp_T) {
-      CK(cudaMemcpyAsync(dst + 10 * nf, ctx->pl + P_TPT0 * nf, sizeof(float) * 2 * nf, cudaMemcpyDeviceToDevice,
+      CK(cudaMemcpyAsync(dst + 11 * nf, ctx->pl + P_TPT0 * nf, sizeof(float) * 2 * nf, cudaMemcpyDeviceToDevice,
                          ctx->s0));
     }
   }
@@ -1495,8 +1512,10 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
   const EnsStage& S = e->st[pat][irk];
   const int nr = (int)e->rup.size(), n = (int)e->sc.size();
   if (irk == 0)
-    for (int r : e->rup)
+    for (int r : e->rup) {
+      launch_rup_sensor(sensor_args(e->sc[r]), e->s0);
       if (e->sc[r]->tp_T) launch_thermpress(tp_args(e->sc[r]), e->s0);
+    }
   if (nr) launch_fault_node_batch(S.fault, S.fstart, nr, S.fblocks, S.FY, S.FZ, e->s0);
   if (e->sc[0]->serial) {
     launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);

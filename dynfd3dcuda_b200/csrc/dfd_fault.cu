@@ -1072,6 +1072,52 @@ void launch_thermpress(const TpArgs& a, cudaStream_t s) {
   else thermpress_column_kernel<<<(a.nf + 127) / 128, 128, 0, s>>>(a);
 }
 
+// Rupture sensor (rup_sensor.cu:8-95), once per step before the stages.  On the fault
+// grid shrunk by 3 nodes (1-based indices), with p = Ts1 and, for non-united nodes,
+//   Dy = 0.25 (2 p - p[j+1] - p[j-1]),  Dz = 0.25 (2 p - p[k+1] - p[k-1])  (zero elsewhere),
+//   sensor = 0.5 ((Dy - Dy[j+1])^2 + (Dy - Dy[j-1])^2)
+//          + 0.5 ((Dz - Dy[k+1])^2 + (Dz - Dy[k-1])^2),  divided by p^2 + 1e-16, + 1e-16,
+// zero on united nodes; the z term takes Dy at the z neighbours, as the reference does.
+// The reference's two kernels (differences, then magnitude) become one: each thread
+// evaluates the five differences it needs.  Nodes outside the shrunk grid keep their zero.
+struct SensorGrid {
+  const SensorArgs& a;
+  __device__ bool inside(int j, int k) const {
+    return j + 1 >= a.fg[0] + 3 && j + 1 <= a.fg[1] - 3 && k + 1 >= a.fg[2] + 3 && k + 1 <= a.fg[3] - 3;
+  }
+  // second difference of Ts1 along stride s at node (j, k), zero where the reference never
+  // writes it
+  __device__ float diff(int j, int k, int s) const {
+    const int q = j + a.nj * k;
+    if (!inside(j, k) || a.united[q]) return 0.0f;
+    const float* p = a.Ts1;
+    return (float)(0.25 * (-p[q + s] + 2.0 * p[q] - p[q - s]));
+  }
+};
+
+__global__ void __launch_bounds__(128) rup_sensor_kernel(const SensorArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= a.nj || k >= a.nk) return;
+  const SensorGrid g{a};
+  if (!g.inside(j, k)) return;
+  const int q = j + a.nj * k, nj = a.nj;
+  const float dy = g.diff(j, k, 1), dz = g.diff(j, k, nj);
+  float D1 = dy - g.diff(j + 1, k, 1);
+  float D2 = dy - g.diff(j - 1, k, 1);
+  float mag = (float)(0.5 * (D1 * D1 + D2 * D2));
+  D1 = dz - g.diff(j, k + 1, 1);
+  D2 = dz - g.diff(j, k - 1, 1);
+  mag = (float)(mag + 0.5 * (D1 * D1 + D2 * D2));
+  const float p0 = a.Ts1[q] * a.Ts1[q];
+  a.out[q] = a.united[q] ? 0.0f : (float)(mag / (p0 + 1e-16) + 1e-16);
+}
+
+void launch_rup_sensor(const SensorArgs& a, cudaStream_t s) {
+  dim3 block(32, 4, 1);
+  dim3 grid((a.nj + 31) / 32, (a.nk + 3) / 4, 1);
+  rup_sensor_kernel<<<grid, block, 0, s>>>(a);
+}
+
 void launch_fault_node(const FaultArgs& a, cudaStream_t s) {
   dim3 block(32, 4, 1);
   dim3 grid((a.d.nj + 31) / 32, (a.d.nk + 3) / 4, 1);

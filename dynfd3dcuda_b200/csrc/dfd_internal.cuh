@@ -295,6 +295,14 @@ struct TpArgs {
   float *T, *P, *T0, *P0;
 };
 void launch_thermpress(const TpArgs& a, cudaStream_t s);
+// rupture sensor (rup_sensor.cu), once per step before the stages: from Ts1 into out
+struct SensorArgs {
+  int nj, nk, fg[4];
+  const int* united;
+  const float* Ts1;
+  float* out;
+};
+void launch_rup_sensor(const SensorArgs& a, cudaStream_t s);
 void launch_fault_band_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FX, int FY, int FZ,
                              cudaStream_t s);
 

@@ -75,6 +75,8 @@ enum {
   DFD_F_TP_T, DFD_F_TP_P,                    /* thermal pressurisation: temperature and pore
                                                 pressure at the fault (point 0 of each column,
                                                 as io_fault.cu:263-265 writes them) */
+  DFD_F_RUP_SENSOR,                          /* rupture sensor of the step start
+                                                (rup_sensor.cu:8-95) */
   DFD_F_COUNT
 };
 

@@ -173,6 +173,7 @@ template <typename R> struct Sim {
   std::vector<R> init_t0, friction;
   // thermal pressurisation: columns of TP_n points, plane i at [i * nf] (alloc.cu:94-118)
   std::vector<R> TP_T, TP_P, TP_hy;
+  std::vector<R> rup_sensor, rup_Dy, rup_Dz;  // rupture sensor (rup_sensor.cu)
   std::vector<int> init_t0_flag, rup_index_y, rup_index_z, united, faultgrid, flag_rup;
   // bookkeeping for the learned-guess study: Newton iterations of the last RS trial
   long newton_iters = 0;
@@ -204,6 +205,7 @@ template <typename R> struct Sim {
     for (auto* v : {&init_t0_flag, &rup_index_y, &rup_index_z, &united, &faultgrid, &flag_rup}) v->assign(nf, 0);
     const int ntp = std::max(p.TP_n, 1);
     TP_T.assign(ntp * nf, 0); TP_P.assign(ntp * nf, 0); TP_hy.assign(nf, 0);
+    rup_sensor.assign(nf, 0); rup_Dy.assign(nf, 0); rup_Dz.assign(nf, 0);
   }
 
   // PML damping profiles (init_pml.cu:18-133): d ~ x^2, alpha ~ (1-x), beta ~ 1+(bmax-1)x^2,
@@ -1426,9 +1428,45 @@ template <typename R> struct Sim {
     }
   }
 
+  // Rupture sensor (rup_sensor.cu:8-95), once per step before the stages: on the fault
+  // grid shrunk by 3 nodes (1-based global indices), second differences of Ts1 along y and
+  // z for the non-united nodes, then
+  //   sensor = (0.5 (D1^2 + D2^2)_y + 0.5 (D1^2 + D2^2)_z) / (Ts1^2 + 1e-16) + 1e-16,
+  // zero on united nodes.  The z term differences Dz at the node with Dy (not Dz) at its z
+  // neighbours, as the reference's second kernel does.  Untouched entries keep their zero.
+  void rup_sensor_step() {
+    const int* fg = p.Fault_grid;
+    auto inside = [&](int j, int k) {
+      return j + 1 >= fg[0] + 3 && j + 1 <= fg[1] - 3 && k + 1 >= fg[2] + 3 && k + 1 <= fg[3] - 3;
+    };
+    for (int k = 0; k < nk; k++)
+      for (int j = 0; j < nj; j++) {
+        long q = j + (long)nj * k;
+        if (!inside(j, k) || united[q]) continue;
+        const R* t = Ts1.data();
+        rup_Dy[q] = (R)(0.25 * (-t[q + 1] + 2.0 * t[q] - t[q - 1]));
+        rup_Dz[q] = (R)(0.25 * (-t[q + nj] + 2.0 * t[q] - t[q - nj]));
+      }
+    for (int k = 0; k < nk; k++)
+      for (int j = 0; j < nj; j++) {
+        long q = j + (long)nj * k;
+        if (!inside(j, k)) continue;
+        R D1 = rup_Dy[q] - rup_Dy[q + 1];
+        R D2 = rup_Dy[q] - rup_Dy[q - 1];
+        R mag = (R)(0.5 * (D1 * D1 + D2 * D2));
+        D1 = rup_Dz[q] - rup_Dy[q + nj];
+        D2 = rup_Dz[q] - rup_Dy[q - nj];
+        mag = (R)(mag + 0.5 * (D1 * D1 + D2 * D2));
+        R p0 = Ts1[q] * Ts1[q];
+        rup_sensor[q] = (R)(mag / (p0 + 1e-16) + 1e-16);
+        if (united[q]) rup_sensor[q] = 0;
+      }
+  }
+
   // One time step: four RK stages with the reference's launch order (main.cu:420-535).
   void step(int it) {
     int FX = FD_FLAGS[it % 8][0], FY = FD_FLAGS[it % 8][1], FZ = FD_FLAGS[it % 8][2];
+    rup_sensor_step();
     if (p.Friction_type == 3) thermpress();
     for (int irk = 0; irk < 4; irk++) {
       state_rk(irk);
@@ -1490,7 +1528,7 @@ template <typename R> struct Sim {
         {"tTs1", &tTs1}, {"tTs2", &tTs2}, {"str_init_x", &str_init_x}, {"str_init_y", &str_init_y},
         {"str_init_z", &str_init_z}, {"slip", &slip}, {"hslip", &hslip}, {"Vs1", &Vs1}, {"Vs2", &Vs2},
         {"State", &State}, {"init_t0", &init_t0}, {"friction", &friction}, {"str_peak", &str_peak},
-        {"TP_T", &TP_T}, {"TP_P", &TP_P}, {"TP_hy", &TP_hy},
+        {"TP_T", &TP_T}, {"TP_P", &TP_P}, {"TP_hy", &TP_hy}, {"rup_sensor", &rup_sensor},
         {"matVx2Vz", &matVx2Vz}, {"matVy2Vz", &matVy2Vz}, {"damp", &damp}, {"Bx", &Bx}, {"By", &By},
         {"Bz", &Bz}, {"Dx", &Dx}, {"Dy", &Dy}, {"Dz", &Dz}, {"Ax", &Ax}, {"Ay", &Ay}, {"Az", &Az},
         {"aux_x1", &aux[0][0]}, {"aux_x2", &aux[1][0]}, {"aux_y1", &aux[2][0]}, {"aux_y2", &aux[3][0]},

@@ -48,6 +48,7 @@ extern void wave_rk(Wave, PML, int irk);
 extern void fault_rk(Fault, int irk);
 extern void state_rk(Fault, int irk);
 extern void thermpress(Wave, Fault, realptr_t M, int it, int irk, int, int, int);
+extern void cal_rup_sensor(Fault F);
 extern void init_fault_coef(realptr_t M, Fault);
 extern void init_wave_free(realptr_t M, PML, Wave);
 extern void nc_read_init_stress(Fault F);
@@ -98,6 +99,7 @@ static void dump_state(Wave &W, Fault &F, PML &P, int step) {
   DUMP("tTn", step, F.tTn, nf);
   DUMP("tTs1", step, F.tTs1, nf);
   DUMP("tTs2", step, F.tTs2, nf);
+  DUMP("rup_sensor", step, F.rup_sensor, nf);
   if (hostParams.Friction_type == 3) {
     DUMP("TP_T", step, F.TP_T, (size_t)hostParams.TP_n * nf);
     DUMP("TP_P", step, F.TP_P, (size_t)hostParams.TP_n * nf);
@@ -260,7 +262,9 @@ int main(int argc, char **argv) {
 
   for (int it = 0; it < nsteps; it++) {
     int FlagX = kFlags[it % 8][0], FlagY = kFlags[it % 8][1], FlagZ = kFlags[it % 8][2];
-    // thermal pressurisation once per step, before the stages (main.cu:444-447)
+    // rupture sensor and thermal pressurisation once per step, before the stages
+    // (main.cu:444-447)
+    if (!volume) cal_rup_sensor(F);
     if (!volume && hostParams.Friction_type == 3) thermpress(W, F, M, it, 0, FlagX, FlagY, FlagZ);
     for (int irk = 0; irk < 4; irk++) {
       if (!volume) {

@@ -4,8 +4,9 @@ Runs oracle/_ref/refharness_{sp,dp}[_nr] (the reference sources compiled for sm_
 by oracle/Makefile, driven in the order of the reference driver) on every case of
 cases.py and stores a compact subset of the dumped state as tests/golden/<case>_<var>.npz:
 
-  every dump step : all on-fault 2-D arrays, per-field checksums of the wavefield and of
-                    the PML auxiliary arrays; with thermal pressurisation (Friction_type
+  every dump step : all on-fault 2-D arrays (the rupture sensor included), per-field
+                    checksums of the wavefield and of the PML auxiliary arrays; with
+                    thermal pressurisation (Friction_type
                     3) temperature and pore pressure at the fault
   final step      : the wavefield (full for the volume cases, the seven x-planes around
                     the fault over the rupture block otherwise), split-node state and the
@@ -85,6 +86,8 @@ def run_case(name, variant, outdir):
         if not meta["volume"]:
             for nm in ("slip", "hslip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State", "init_t0", "tTn", "tTs1", "tTs2"):
                 save[f"{nm}_s{s}"] = dumps[(nm, s)].astype(np.float32).reshape(NZ, NY)
+            if ("rup_sensor", s) in dumps:
+                save[f"rup_sensor_s{s}"] = dumps[("rup_sensor", s)].astype(np.float32).reshape(NZ, NY)
             for nm in ("TP_T", "TP_P"):
                 if (nm, s) in dumps:  # thermal pressurisation: the on-fault point of each column
                     save[f"{nm}_s{s}"] = dumps[(nm, s)].astype(np.float32).reshape(-1, NZ, NY)[0]

@@ -38,7 +38,7 @@ def test_driver_writes_reference_outputs(tmp_path):
 
     p, fx, st, _, _, _ = cases.get_case("sw_flat")
     sim = dfd.Simulation(dict(job), fx, st, None)
-    recs = {k: [] for k in ("Vs1", "Vs2", "Tn", "Ts1", "Ts2", "slip", "State")}
+    recs = {k: [] for k in ("Vs1", "Vs2", "Tn", "Ts1", "Ts2", "slip", "State", "rup_sensor")}
     slices = []
     for it in range(NT):
         if it % 5 == 0:
@@ -53,7 +53,7 @@ def test_driver_writes_reference_outputs(tmp_path):
         v = f.variables
         assert v["Vs1"].shape == (NT // 5, job["NZ"], job["NY"])
         for nc, k in (("Vs1", "Vs1"), ("Vs2", "Vs2"), ("tn", "Tn"), ("ts1", "Ts1"), ("ts2", "Ts2"), ("Us0", "slip"),
-                      ("State", "State")):
+                      ("State", "State"), ("rup_sensor", "rup_sensor")):
             np.testing.assert_array_equal(np.asarray(v[nc][:]), np.stack(recs[k]), err_msg=nc)
         assert np.asarray(v["y"][:]).shape == (job["NZ"], job["NY"])
         # rupture times as of the last record (written before step 20)

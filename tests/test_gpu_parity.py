@@ -82,6 +82,9 @@ def test_cuda_matches_oracle(oracle_lib, name, mode):
                 assert rel(a, g[f"{nm}_s{s}"]) < tol, (s, nm, "vs reference FP32 build")
             t0 = sim.fault("init_t0")
             assert np.abs(t0 - o.get("init_t0").reshape(NZ, NY)).max() <= 1.01 * p["DT"]
+            a = sim.fault("rup_sensor")  # rupture sensor of the step start
+            assert rel(a, o.get("rup_sensor").reshape(NZ, NY)) < tol, (s, "rup_sensor")
+            assert rel(a, g[f"rup_sensor_s{s}"]) < tol, (s, "rup_sensor", "vs reference FP32 build")
             if p.get("Friction_type") == 3:  # thermal pressurisation at the fault
                 for nm in ("TP_T", "TP_P"):
                     a = sim.fault(nm)

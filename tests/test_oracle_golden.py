@@ -72,6 +72,8 @@ def test_oracle_matches_reference(oracle_lib, name, var):
             # rupture times are identical to the step
             t0 = o.get("init_t0").reshape(NZ, NY)
             assert np.abs(t0 - g[f"init_t0_s{s}"]).max() < 0.5 * p["DT"]
+            if f"rup_sensor_s{s}" in g:  # rupture sensor of the step start
+                assert rel(o.get("rup_sensor").reshape(NZ, NY), g[f"rup_sensor_s{s}"]) < tol, ("rup_sensor", s)
             for nm in ("TP_T", "TP_P"):  # thermal pressurisation: the point on the fault
                 if f"{nm}_s{s}" in g:
                     assert rel(o.get(nm).reshape(-1, NZ, NY)[0], g[f"{nm}_s{s}"]) < tol, (nm, s)
