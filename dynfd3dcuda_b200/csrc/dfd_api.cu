@@ -313,7 +313,7 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->guess_net, DFD_MLP_PARAMS);
   if (!rc) rc = dalloc(ctx, &ctx->rec_n, 1);
   if (!rc) rc = dalloc(ctx, &ctx->tile_err, 1);
-  if (!rc) rc = dalloc(ctx, &ctx->tile_sched, 2);
+  if (!rc) rc = dalloc(ctx, &ctx->tile_sched, 4);  // unit and finished-CTA counters: interior, PML
   if (rc) { dfd_destroy(ctx); return rc; }
   // volume kernels: DFD_TILE=0 plain interior kernel + general kernel on the PML slabs
   // and free-surface rows; otherwise (default) the TMA-staged interior and PML kernels
@@ -1519,7 +1519,8 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
   if (nr) launch_fault_node_batch(S.fault, S.fstart, nr, S.fblocks, S.FY, S.FZ, e->s0);
   if (e->sc[0]->serial) {
     launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
-    launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
+    launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, S.nunits > 0,
+                     e->s0);
     // the general kernel beside the fault band kernel
     cudaEventRecord(e->ev_fork, e->s0);
     cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
@@ -1542,7 +1543,8 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
   launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s2);
   cudaEventRecord(e->ev_join2, e->s2);
   launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
-  launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
+  launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, S.nunits > 0,
+                     e->s0);
   if (nr) cudaStreamWaitEvent(e->s0, e->ev_join, 0);
   cudaStreamWaitEvent(e->s0, e->ev_join2, 0);
   cudaError_t ce = cudaGetLastError();
@@ -1599,11 +1601,11 @@ int dfd_ens_create(dfd_ctx* const* scenarios, int n, dfd_ens** out) {
   cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&e->ev_join2, cudaEventDisableTiming);
   void* p = nullptr;
-  if (cudaMalloc(&p, 4 * sizeof(int)) != cudaSuccess) return done(DFD_ERR_CUDA);
-  cudaMemset(p, 0, 4 * sizeof(int));
+  if (cudaMalloc(&p, 6 * sizeof(int)) != cudaSuccess) return done(DFD_ERR_CUDA);
+  cudaMemset(p, 0, 6 * sizeof(int));
   e->it_dev = (int*)p;
-  e->sched = e->it_dev + 1;  // unit counter, finished-CTA counter
-  e->err = e->it_dev + 3;
+  e->sched = e->it_dev + 1;  // unit and finished-CTA counters of the interior, then the PML kernel
+  e->err = e->it_dev + 5;
   for (dfd_ctx* c : e->sc) cudaStreamSynchronize(c->s0);
   int r = ens_build(e);
   if (r) return done(r);

@@ -272,10 +272,12 @@ TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid);
 // units of the PML kernel around the interior box (dfd_pml.cu)
 TileSched pml_plan(const VolArgs& a, int ya, int yb, int za, int zb, int ktop, int nsm, int* grid);
 bool pml_setup();
+// pdl: launch behind the interior kernel on the same stream with programmatic
+// serialisation; sched: a 4-int counter block (the interior kernel uses the first pair)
 void launch_pml(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, const TileSched& ps, int grid,
-                cudaStream_t s);
+                bool pdl, cudaStream_t s);
 void launch_pml_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY, int FZ,
-                      int* err, int* sched, cudaStream_t s);
+                      int* err, int* sched, bool pdl, cudaStream_t s);
 // batched launches (dfd_volume.cu, dfd_tile.cu, dfd_fault.cu)
 void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,
                        int FZ, int* err, int* sched, cudaStream_t s);

@@ -389,6 +389,9 @@ __global__ void __maxnreg__(168)
       atomicExch(sched, 0);
       atomicExch(sched + 1, 0);
     }
+    // launched behind the interior kernel (programmatic serialisation), this grid must not
+    // complete before that one: what follows on the stream relies on both
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     return;
   }
 
@@ -564,47 +567,66 @@ TileSched pml_plan(const VolArgs& a, int ya, int yb, int za, int zb, int ktop, i
   return s;
 }
 
+// pdl: launched with programmatic stream serialisation right behind the interior kernel,
+// whose CTAs allow it at their start; the two grids update disjoint nodes of the stage.
+// The PML kernel takes the second pair of the 4-int counter block sched.
+template <int FX, int FY, int FZ, bool BATCH>
+static void pml_launch(const TileMaps& mp, const VolArgs& a, const TileSched& sc, const TileScen* tab, int n,
+                       int nunits, int grid, int* err, int* sched, bool pdl, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(PTOT);
+  cfg.dynamicSmemBytes = PML_SMEM;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, volume_pml_kernel<FX, FY, FZ, BATCH>, mp, a, sc, tab, n, nunits, err, sched + 2);
+}
+
 template <int FX, int FY, int FZ>
-static void launch_p(const TileCtx& tc, const VolArgs& a, int bin, const TileSched& ps, int grid, cudaStream_t s) {
+static void launch_p(const TileCtx& tc, const VolArgs& a, int bin, const TileSched& ps, int grid, bool pdl,
+                     cudaStream_t s) {
   const TileMaps mp = tile_maps(tc, bin);
-  volume_pml_kernel<FX, FY, FZ, false>
-      <<<grid, PTOT, PML_SMEM, s>>>(mp, a, ps, nullptr, 1, ps.nunits, tc.err, tc.sched);
+  pml_launch<FX, FY, FZ, false>(mp, a, ps, nullptr, 1, ps.nunits, grid, tc.err, tc.sched, pdl, s);
 }
 
 void launch_pml(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int bin, const TileSched& ps, int grid,
-                cudaStream_t s) {
+                bool pdl, cudaStream_t s) {
   if (ps.nunits <= 0 || grid <= 0) return;
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: launch_p<-1, -1, -1>(*tc, a, bin, ps, grid, s); break;
-    case 1: launch_p<-1, -1, 1>(*tc, a, bin, ps, grid, s); break;
-    case 2: launch_p<-1, 1, -1>(*tc, a, bin, ps, grid, s); break;
-    case 3: launch_p<-1, 1, 1>(*tc, a, bin, ps, grid, s); break;
-    case 4: launch_p<1, -1, -1>(*tc, a, bin, ps, grid, s); break;
-    case 5: launch_p<1, -1, 1>(*tc, a, bin, ps, grid, s); break;
-    case 6: launch_p<1, 1, -1>(*tc, a, bin, ps, grid, s); break;
-    default: launch_p<1, 1, 1>(*tc, a, bin, ps, grid, s); break;
+    case 0: launch_p<-1, -1, -1>(*tc, a, bin, ps, grid, pdl, s); break;
+    case 1: launch_p<-1, -1, 1>(*tc, a, bin, ps, grid, pdl, s); break;
+    case 2: launch_p<-1, 1, -1>(*tc, a, bin, ps, grid, pdl, s); break;
+    case 3: launch_p<-1, 1, 1>(*tc, a, bin, ps, grid, pdl, s); break;
+    case 4: launch_p<1, -1, -1>(*tc, a, bin, ps, grid, pdl, s); break;
+    case 5: launch_p<1, -1, 1>(*tc, a, bin, ps, grid, pdl, s); break;
+    case 6: launch_p<1, 1, -1>(*tc, a, bin, ps, grid, pdl, s); break;
+    default: launch_p<1, 1, 1>(*tc, a, bin, ps, grid, pdl, s); break;
   }
 }
 
 template <int FX, int FY, int FZ>
 static void launch_pb(const TileScen& f, const TileScen* tab, int n, int nunits, int grid, int* err, int* sched,
-                      cudaStream_t s) {
-  volume_pml_kernel<FX, FY, FZ, true><<<grid, PTOT, PML_SMEM, s>>>(f.mp, f.u.a, f.u.sc, tab, n, nunits, err, sched);
+                      bool pdl, cudaStream_t s) {
+  pml_launch<FX, FY, FZ, true>(f.mp, f.u.a, f.u.sc, tab, n, nunits, grid, err, sched, pdl, s);
 }
 void launch_pml_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY, int FZ,
-                      int* err, int* sched, cudaStream_t s) {
+                      int* err, int* sched, bool pdl, cudaStream_t s) {
   if (nunits <= 0 || grid <= 0) return;
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: launch_pb<-1, -1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 1: launch_pb<-1, -1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 2: launch_pb<-1, 1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 3: launch_pb<-1, 1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 4: launch_pb<1, -1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 5: launch_pb<1, -1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 6: launch_pb<1, 1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    default: launch_pb<1, 1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 0: launch_pb<-1, -1, -1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
+    case 1: launch_pb<-1, -1, 1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
+    case 2: launch_pb<-1, 1, -1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
+    case 3: launch_pb<-1, 1, 1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
+    case 4: launch_pb<1, -1, -1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
+    case 5: launch_pb<1, -1, 1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
+    case 6: launch_pb<1, 1, -1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
+    default: launch_pb<1, 1, 1>(first, tab, n, nunits, grid, err, sched, pdl, s); break;
   }
 }
 

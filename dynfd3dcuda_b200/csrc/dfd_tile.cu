@@ -68,6 +68,9 @@ __global__ void __maxnreg__(96)
   const int irk = a0.irk;
   const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1, usep = needW0 || needT;
   const int G = gridDim.x;
+  // the PML kernel that follows on the stream touches other nodes only: it may take the
+  // SMs that this persistent grid's CTAs leave as they finish
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; s++) { mbar_init(full_w + s, 1); mbar_init(empty_w + s, NCW); }

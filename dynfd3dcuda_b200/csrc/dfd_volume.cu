@@ -412,7 +412,8 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     volume_interior_kernel<FX, FY, FZ><<<grid, block, 0, s>>>(a, pl.lo, pl.hi, chunk);
   }
   if (ke) cudaEventRecord(*ke, s);
-  if (pl.ps.nunits > 0) launch_pml(tc, a, FX, FY, FZ, bin, pl.ps, pl.pgrid, s);
+  // directly behind the interior kernel unless timing events separate them
+  if (pl.ps.nunits > 0) launch_pml(tc, a, FX, FY, FZ, bin, pl.ps, pl.pgrid, pl.tiled && !ke, s);
   if (fork && s_shell != s) {
     // the general kernel on s_shell once the tiled kernels are done
     cudaEventRecord(*fork, s);

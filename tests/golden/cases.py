@@ -243,6 +243,11 @@ def get_case(name):
         st = sw_stress(fx, fg, tn=-120e6, ts=-40e6)
         st = rs_fields(st, fx, seed=7, L=0.02, patch=(0.0, -500.0, 600.0), patch_dtau=45e6)
         return p, fx, st, None, None, dict(steps=40, every=20, volume=False)
+    if name == "rs_aging":
+        # rs_flat with the aging law (Friction_type 1, rk4.cu:899-901)
+        p, fx, st, layers, w0, meta = get_case("rs_flat")
+        p["Friction_type"] = 1
+        return p, fx, st, layers, w0, meta
     if name == "tp_flat":
         # rs_flat with thermal pressurisation: 64 points per column, so that the diffusion
         # sub-cycles (sub-step 10/63^2 s < DT), hydraulic diffusivity log-uniform per node
@@ -302,7 +307,7 @@ def ensemble_case(i, seed=2025, size=(100, 300), DH=100.0, DT=0.008, steps=1000)
     return p, fx, st
 
 
-CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan", "tp_flat"]
+CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan", "tp_flat", "rs_aging"]
 
 
 def write_inputs(name, outdir):

@@ -26,6 +26,7 @@ TOL = {
     ("rs_flat", "dp"): 3e-5, ("rs_flat", "sp"): 3e-4,
     ("sw_cerjan", "dp"): 1e-6, ("sw_cerjan", "sp"): 1e-5,
     ("tp_flat", "dp"): 1e-5, ("tp_flat", "sp"): 3e-4,
+    ("rs_aging", "dp"): 1e-6, ("rs_aging", "sp"): 1e-3,
 }
 
 
