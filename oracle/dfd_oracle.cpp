@@ -66,6 +66,13 @@ static const double A3 = 0.0416862855405999;
 static const double C24_1 = 7.0 / 6.0, C24_2 = 4.0 / 3.0, C24_3 = 1.0 / 6.0;
 static const double PI_ = 3.141592653589793238463;
 
+// The reference's vector norm (device.cu:84-89): squares summed in real_t, then sqrtf,
+// so its FP64 build too rounds every norm3 to single precision.
+static inline double ref_norm3(double a, double b, double c) {
+  double s = a * a + b * b + c * c;
+  return (double)sqrtf((float)s);
+}
+
 template <typename R> static inline R opF(const R* v, long p, long s) {
   return R(-C1 * v[p - s] - C2 * v[p] + C3 * v[p + s] - C4 * v[p + 2 * s] + C5 * v[p + 3 * s]);
 }
@@ -410,9 +417,9 @@ template <typename R> struct Sim {
         double xzt[3] = {inv[0][2], inv[1][2], inv[2][2]};
         // base vectors n = xi_grad/|.|, s1 = x_eta/|.|, s2 = n x s1 (fault_coef.cu:206-248)
         double s1[3], nn[3], s2[3];
-        double ns1 = std::sqrt(xet[0] * xet[0] + xet[1] * xet[1] + xet[2] * xet[2]);
+        double ns1 = ref_norm3(xet[0], xet[1], xet[2]);
         for (int c = 0; c < 3; c++) s1[c] = xet[c] / ns1;
-        double nnn = std::sqrt(e[0][0] * e[0][0] + e[0][1] * e[0][1] + e[0][2] * e[0][2]);
+        double nnn = ref_norm3(e[0][0], e[0][1], e[0][2]);
         for (int c = 0; c < 3; c++) nn[c] = e[0][c] / nnn;
         cross3(nn, s1, s2);
         for (int c = 0; c < 3; c++) {
@@ -494,7 +501,7 @@ template <typename R> struct Sim {
           put9("matVx2Vz1", j, vx[0]); put9("matVy2Vz1", j, vy[0]);
           put9("matVx2Vz2", j, vx[1]); put9("matVy2Vz2", j, vy[1]);
           double v1[3] = {e[0][0], e[0][1], e[0][2]};
-          double v1n = std::sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+          double v1n = ref_norm3(v1[0], v1[1], v1[2]);
           double v3[3];
           cross3(v1, xet, v3);
           double h[3];
@@ -970,7 +977,7 @@ template <typename R> struct Sim {
           Trial[c] = -(t.Mrho[0] * t.Mrho[1] * dV[c] / p.DT + t.Mrho[0] * Rm[c][1] - t.Mrho[1] * Rm[c][0]) / den * 2.0;
         long qm = P3(i0, j + 3, k + 3);
         double nv[3] = {Mf(0)[qm], Mf(1)[qm], Mf(2)[qm]};
-        double n0 = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+        double n0 = ref_norm3(nv[0], nv[1], nv[2]);
         double jacvec = (double)Mf(9)[qm] * n0;
         for (int c = 0; c < 3; c++) nv[c] /= n0;
         double si[3] = {str_init_x[q2], str_init_y[q2], str_init_z[q2]};
@@ -978,7 +985,7 @@ template <typename R> struct Sim {
         for (int c = 0; c < 3; c++) TL[c] = Trial[c] / jacvec + si[c];
         double Trn = TL[0] * nv[0] + TL[1] * nv[1] + TL[2] * nv[2];
         for (int c = 0; c < 3; c++) Ts[c] = TL[c] - nv[c] * Trn;
-        double Ts0 = std::sqrt(Ts[0] * Ts[0] + Ts[1] * Ts[1] + Ts[2] * Ts[2]);
+        double Ts0 = ref_norm3(Ts[0], Ts[1], Ts[2]);
         bool change = false;
         double Tau_n, Tau_s;
         if (Trn >= 0.0) { Tau_n = 0.0; change = true; } else Tau_n = Trn;
@@ -1031,7 +1038,7 @@ template <typename R> struct Sim {
         for (int c = 0; c < 3; c++) { s1[c] = vecn("vec_s1", pf, c); s2[c] = vecn("vec_s2", pf, c); }
         long qm = P3(i0, j + 3, k + 3);
         for (int c = 0; c < 3; c++) nv[c] = Mf(c)[qm];
-        double n0 = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+        double n0 = ref_norm3(nv[0], nv[1], nv[2]);
         double jacvec = (double)Mf(9)[qm] * n0;
         for (int c = 0; c < 3; c++) nv[c] /= n0;
         TrialPre t;

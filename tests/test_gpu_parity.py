@@ -19,7 +19,10 @@ pytestmark = pytest.mark.gpu
 
 J0, J1 = 24, 52
 TOL = {"vol_small": 2e-5, "vol_curved": 2e-5, "sw_flat": 2e-4, "sw_flat_nr": 2e-4, "sw_curved": 5e-4,
-       "rs_flat": 2e-3, "sw_cerjan": 2e-4, "tp_flat": 2e-3, "rs_aging": 2e-3}
+       "rs_flat": 2e-3, "sw_cerjan": 2e-4, "tp_flat": 2e-3, "rs_aging": 2e-3,
+       # the reference's own FP32 build lies 1.6e-3 from FP64 here (rate and state on a rough
+       # fault): the FP32 product is held to the sum of both roundings against that build
+       "rs_curved": 3e-3}
 
 
 def rel(a, b):

@@ -14,9 +14,10 @@ import cases
 J0, J1 = 24, 52
 
 # relative max-error tolerances (of the field's max magnitude).  FP64-vs-FP64 is limited by
-# the fixtures' FP32 storage and by the reference's single-precision sqrtf in its vector
-# norm (device.cu:84-89), which the rupture amplifies mildly; FP32 reference adds its own
-# rounding, most for rate-and-state (exp/sinh of state over a=0.01).
+# the fixtures' FP32 storage (the oracle reproduces the reference's single-precision sqrtf
+# in its vector norm, device.cu:84-89, which on a rough fault moves rate-and-state results
+# by 1e-3); the FP32 reference adds its own rounding, most for rate and state (exp/sinh of
+# state over a = 0.01) and most of all on the rough fault.
 TOL = {
     ("vol_small", "dp"): 1e-6, ("vol_small", "sp"): 2e-6,
     ("vol_curved", "dp"): 1e-6, ("vol_curved", "sp"): 2e-6,
@@ -27,6 +28,7 @@ TOL = {
     ("sw_cerjan", "dp"): 1e-6, ("sw_cerjan", "sp"): 1e-5,
     ("tp_flat", "dp"): 1e-5, ("tp_flat", "sp"): 3e-4,
     ("rs_aging", "dp"): 1e-6, ("rs_aging", "sp"): 1e-3,
+    ("rs_curved", "dp"): 1e-5, ("rs_curved", "sp"): 3e-3,
 }
 
 
