@@ -206,7 +206,8 @@ def lib():
             "dfd_create": [P(DfdParams), I, P(V)], "dfd_destroy": [V], "dfd_dims": [V, P(I), P(I), P(I)],
             "dfd_load_fault_geometry": [V, V], "dfd_load_media1d": [V, I, V], "dfd_load_fault_init": [V, V],
             "dfd_load_tp_hy": [V, V], "dfd_get_tp_columns": [V, I, V],
-            "dfd_precompute": [V], "dfd_stage": [V, I, I], "dfd_step": [V, I], "dfd_run": [V, I, I],
+            "dfd_precompute": [V], "dfd_stage": [V, I, I], "dfd_stage_part": [V, I, I, I], "dfd_step": [V, I],
+            "dfd_run": [V, I, I],
             "dfd_synchronize": [V], "dfd_get_wave": [V, V], "dfd_set_wave": [V, V], "dfd_get_metric": [V, V],
             "dfd_get_fault": [V, I, V], "dfd_get_slice": [V, I, I, V], "dfd_get_slice_noalloc": [V, I, I, V], "dfd_check_finite": [V],
             "dfd_newton_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong)],
@@ -309,6 +310,10 @@ class Simulation:
 
     def stage(self, it, irk):
         self._check(lib().dfd_stage(self.h, it, irk))
+
+    def stage_part(self, it, irk, part):
+        """Part 0 (fault trial), 1 (volume) or 2 (fault band) of stage irk of step it."""
+        self._check(lib().dfd_stage_part(self.h, it, irk, part))
 
     def step(self, it):
         self._check(lib().dfd_step(self.h, it))

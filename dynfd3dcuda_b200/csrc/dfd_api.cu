@@ -140,6 +140,7 @@ struct dfd_ctx {
   std::vector<double> xl, fx, fy, fz;
   bool ready = false;
   int next_stage = 0;
+  int next_part = 0;  // dfd_stage_part: the next part (0..2) of stage next_stage
   std::string err;
   int sticky = DFD_OK;
   cudaGraphExec_t graph[8] = {};
@@ -156,6 +157,9 @@ struct dfd_ctx {
   int fetch_k = 0;
   bool fetch_used[2] = {false, false};
 };
+
+// a step or a stage issued only in part (dfd_stage, dfd_stage_part)
+static inline bool mid_step(const dfd_ctx* c) { return c->next_stage != 0 || c->next_part != 0; }
 
 static int fail(dfd_ctx* c, int code, const std::string& m) {
   if (c) { c->err = m; if (code == DFD_ERR_CUDA) c->sticky = code; }
@@ -540,6 +544,7 @@ int dfd_precompute(dfd_ctx* ctx) {
     if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
   ctx->ready = true;
   ctx->next_stage = 0;
+  ctx->next_part = 0;
   return DFD_OK;
 }
 
@@ -731,18 +736,61 @@ static int enqueue_stage(dfd_ctx* ctx, int pattern, int irk, cudaEvent_t* vb = n
   return cuda_check(ctx, cudaGetLastError(), "stage launch");
 }
 
+// One part of a stage, the kernels of enqueue_stage in three groups on the stepping
+// stream: 0 = (stage 0: rupture sensor, thermal pressurisation) fault node kernel;
+// 1 = the volume kernels, the free-surface rows joined back before the part ends;
+// 2 = the fault band kernel.  Parts 0, 1, 2 compute what enqueue_stage computes.
+static int enqueue_part(dfd_ctx* ctx, int pattern, int irk, int part) {
+  const dfd_params& p = ctx->p;
+  const int sg = (irk % 2) ? -1 : 1;
+  const int FX = kFlags[pattern][0] * sg, FY = kFlags[pattern][1] * sg, FZ = kFlags[pattern][2] * sg;
+  static const int bin[4] = {0, 1, 2, 1};
+  if (part == 0 && p.rupture) {
+    if (irk == 0) launch_rup_sensor(sensor_args(ctx), ctx->s0);
+    if (irk == 0 && ctx->tp_T) launch_thermpress(tp_args(ctx), ctx->s0);
+    launch_fault_node(fault_args(ctx, pattern, irk), ctx->s0);
+  } else if (part == 1) {
+    VolArgs va = vol_args(ctx, pattern, irk);
+    VolPlan pl;
+    launch_volume_stage(va, FX, FY, FZ, ctx->s0, ctx->s2, ctx->use_tile ? &ctx->tile : nullptr, bin[irk], nullptr,
+                        nullptr, &pl, &ctx->ev_fork);
+    ctx->interior_nodes = interior_nodes(ctx, pl);
+    cudaEventRecord(ctx->ev_join2, ctx->s2);
+    cudaStreamWaitEvent(ctx->s0, ctx->ev_join2, 0);
+  } else if (part == 2 && p.rupture) {
+    launch_fault_band(fault_args(ctx, pattern, irk), ctx->s0);
+  }
+  return cuda_check(ctx, cudaGetLastError(), "stage part launch");
+}
+
 extern "C" {
 
 int dfd_stage(dfd_ctx* ctx, int it, int irk) {
   if (!ctx) return DFD_ERR_PARAM;
   if (ctx->sticky) return ctx->sticky;
   if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
-  if (irk != ctx->next_stage) return fail(ctx, DFD_ERR_STATE, "stages must be issued in order 0..3");
+  if (irk != ctx->next_stage || ctx->next_part != 0)
+    return fail(ctx, DFD_ERR_STATE, "stages must be issued in order 0..3");
   cudaSetDevice(ctx->device);
   if (irk == 0) dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it);
   int r = enqueue_stage(ctx, ((it % 8) + 8) % 8, irk);
   if (r) return r;
   ctx->next_stage = (irk + 1) % 4;
+  return DFD_OK;
+}
+
+int dfd_stage_part(dfd_ctx* ctx, int it, int irk, int part) {
+  if (!ctx || irk < 0 || irk > 3 || part < 0 || part > 2) return DFD_ERR_PARAM;
+  if (ctx->sticky) return ctx->sticky;
+  if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
+  if (irk != ctx->next_stage || part != ctx->next_part)
+    return fail(ctx, DFD_ERR_STATE, "stage parts must be issued in order 0..2 within stages 0..3");
+  cudaSetDevice(ctx->device);
+  if (irk == 0 && part == 0) dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it);
+  int r = enqueue_part(ctx, ((it % 8) + 8) % 8, irk, part);
+  if (r) return r;
+  ctx->next_part = (part + 1) % 3;
+  if (part == 2) ctx->next_stage = (irk + 1) % 4;
   return DFD_OK;
 }
 
@@ -765,7 +813,7 @@ int dfd_run(dfd_ctx* ctx, int it0, int nsteps) {
   if (!ctx) return DFD_ERR_PARAM;
   if (ctx->sticky) return ctx->sticky;
   if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
-  if (ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "a step is half done (dfd_stage)");
+  if (mid_step(ctx)) return fail(ctx, DFD_ERR_STATE, "a step is half done (dfd_stage)");
   cudaSetDevice(ctx->device);
   dfd::set_it_kernel<<<1, 1, 0, ctx->s0>>>(ctx->it_dev, it0);
   for (int s = 0; s < nsteps; s++) {
@@ -787,7 +835,7 @@ int dfd_run_graph_timed(dfd_ctx* ctx, int it0, int nsteps, float* ms) {
   if (!ctx || !ms || nsteps < 1) return DFD_ERR_PARAM;
   if (ctx->sticky) return ctx->sticky;
   if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
-  if (ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "a step is half done (dfd_stage)");
+  if (mid_step(ctx)) return fail(ctx, DFD_ERR_STATE, "a step is half done (dfd_stage)");
   cudaSetDevice(ctx->device);
   for (int pat = 0; pat < 8; pat++)
     if (!ctx->graph[pat]) {
@@ -840,7 +888,7 @@ static int volume_copy(dfd_ctx* ctx, float* host, float* dev, int nf, bool to_ho
 
 int dfd_get_wave(dfd_ctx* ctx, float* host) {
   if (!ctx || !host) return DFD_ERR_PARAM;
-  if (ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "wavefield is mid-step");
+  if (mid_step(ctx)) return fail(ctx, DFD_ERR_STATE, "wavefield is mid-step");
   CK(cudaStreamSynchronize(ctx->s0));
   return volume_copy(ctx, host, ctx->W[0], 9, true);
 }
@@ -1005,7 +1053,7 @@ int dfd_fetch_outputs(dfd_ctx* ctx, float* host) {
 int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* volume_ms, float* fault_ms) {
   if (!ctx) return DFD_ERR_PARAM;
   if (ctx->sticky) return ctx->sticky;
-  if (!ctx->ready || ctx->next_stage != 0) return fail(ctx, DFD_ERR_STATE, "not ready for a step");
+  if (!ctx->ready || mid_step(ctx)) return fail(ctx, DFD_ERR_STATE, "not ready for a step");
   cudaSetDevice(ctx->device);
   int nev = 8 * nsteps + 2;
   std::vector<cudaEvent_t> ev(nev), kev(8 * nsteps), fev(8 * nsteps);
@@ -1579,7 +1627,7 @@ int dfd_ens_create(dfd_ctx* const* scenarios, int n, dfd_ens** out) {
   e->device = scenarios[0]->device;
   for (int i = 0; i < n; i++) {
     dfd_ctx* c = scenarios[i];
-    if (!c || !c->ready || c->device != e->device || c->next_stage != 0 || !c->use_tile) {
+    if (!c || !c->ready || c->device != e->device || mid_step(c) || !c->use_tile) {
       delete e;
       return DFD_ERR_PARAM;
     }

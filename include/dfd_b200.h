@@ -118,6 +118,19 @@ int dfd_precompute(dfd_ctx *ctx);
  * trial_rs, fault2wave, wave_deriv, abs_deriv_{x,y,z}, fault_dvelo, fault_dstrs_{f,b},
  * wave_rk, fault_rk, apply_cerjan (main.cu:448-516).  Stages must be issued in order. */
 int dfd_stage(dfd_ctx *ctx, int it, int irk);
+/* One part of stage irk, for part-by-part parity with the reference's launchers; parts
+ * 0, 1, 2 issued in order are dfd_stage(ctx, it, irk).  The product fuses the reference's
+ * launchers into three kernel groups, so a part stands for several of them:
+ *   DFD_PART_FAULT_TRIAL  state_rk, trial_sw / trial_rs, fault2wave (main.cu:458-467);
+ *                         at stage 0 first cal_rup_sensor and thermpress (main.cu:444-446)
+ *   DFD_PART_VOLUME       wave_deriv, abs_deriv_{x,y,z}, and for every node outside the
+ *                         fault band wave_rk and apply_cerjan (main.cu:469-481,495,508)
+ *   DFD_PART_FAULT_BAND   fault_dvelo, fault_dstrs_{f,b}, wave_rk, fault_rk and fault2wave
+ *                         for the fault band and split nodes (main.cu:486-504)
+ * DFD_ERR_STATE when a part comes out of order; dfd_step / dfd_run refuse a stage left
+ * half done. */
+enum { DFD_PART_FAULT_TRIAL = 0, DFD_PART_VOLUME = 1, DFD_PART_FAULT_BAND = 2 };
+int dfd_stage_part(dfd_ctx *ctx, int it, int irk, int part);
 /* one full step (four stages, replayed from a CUDA graph per flag pattern) */
 int dfd_step(dfd_ctx *ctx, int it);
 /* nsteps steps starting at it0, without host synchronisation in between */

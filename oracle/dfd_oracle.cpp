@@ -1496,6 +1496,39 @@ template <typename R> struct Sim {
       FX = -FX; FY = -FY; FZ = -FZ;
     }
   }
+  // One part of stage irk of step it, the stage split as the product's dfd_stage_part
+  // splits it: 0 = (stage 0: rupture sensor, thermal pressurisation) state_rk, trial,
+  // fault2wave; 1 = wave_deriv, abs_deriv of the PML faces; 2 = fault_dvelo, fault_dstrs,
+  // wave_rk, fault_rk, fault2wave, apply_cerjan.  Parts 0, 1, 2 of stages 0..3 are step().
+  void stage_part(int it, int irk, int part) {
+    const int sg = (irk % 2) ? -1 : 1;
+    const int FX = FD_FLAGS[it % 8][0] * sg, FY = FD_FLAGS[it % 8][1] * sg, FZ = FD_FLAGS[it % 8][2] * sg;
+    if (part == 0) {
+      if (irk == 0) {
+        rup_sensor_step();
+        if (p.Friction_type == 3) thermpress();
+      }
+      state_rk(irk);
+      if (p.Friction_type == 0) trial_sw(it, irk, FX, FY, FZ);
+      else trial_rs(it, irk, FX, FY, FZ);
+      fault2wave();
+    } else if (part == 1) {
+      wave_deriv(FX, FY, FZ);
+      if (isx1) abs_deriv(0, FX);
+      if (isx2) abs_deriv(1, FX);
+      if (isy1) abs_deriv(2, FY);
+      if (isy2) abs_deriv(3, FY);
+      if (isz1) abs_deriv(4, FZ);
+      if (isz2) abs_deriv(5, FZ);
+    } else {
+      fault_dvelo(FX, FY, FZ);
+      fault_dstrs(FX, FY, FZ);
+      wave_rk(irk);
+      fault_rk(irk);
+      fault2wave();
+      apply_cerjan();
+    }
+  }
   // Volume-only stage sequence (no rupture kernels) used by the pure-stencil checks.
   void step_volume(int it) {
     int FX = FD_FLAGS[it % 8][0], FY = FD_FLAGS[it % 8][1], FZ = FD_FLAGS[it % 8][2];
@@ -1579,6 +1612,12 @@ void orc_destroy(void* hv) {
 int orc_step(void* hv, int it) {
   orc_handle* h = (orc_handle*)hv;
   if (h->dp) h->d->step(it); else h->f->step(it);
+  return 0;
+}
+int orc_stage_part(void* hv, int it, int irk, int part) {
+  orc_handle* h = (orc_handle*)hv;
+  if (irk < 0 || irk > 3 || part < 0 || part > 2) return 1;
+  if (h->dp) h->d->stage_part(it, irk, part); else h->f->stage_part(it, irk, part);
   return 0;
 }
 int orc_step_volume(void* hv, int it) {

@@ -61,6 +61,7 @@ def lib():
         _LIB.orc_destroy.argtypes = [ctypes.c_void_p]
         _LIB.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         _LIB.orc_step_volume.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        _LIB.orc_stage_part.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         _LIB.orc_get.restype = ctypes.c_long
         _LIB.orc_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
         _LIB.orc_set.restype = ctypes.c_long
@@ -138,6 +139,11 @@ class Oracle:
 
     def step(self, it):
         lib().orc_step(self.h, it)
+
+    def stage_part(self, it, irk, part):
+        """Part 0 (fault trial), 1 (volume derivatives and PML) or 2 (fault band, RK,
+        sponge) of stage irk of step it."""
+        lib().orc_stage_part(self.h, it, irk, part)
 
     def step_volume(self, it):
         lib().orc_step_volume(self.h, it)

@@ -247,3 +247,57 @@ def test_thermal_pressurisation_column_lengths(oracle_lib, tp_n):
     for nm in ("slip", "State"):
         assert rel(sim.fault(nm), o.get(nm).reshape(NZ, NY)) < tol, nm
     sim.close()
+
+
+@pytest.mark.parametrize("name", ["sw_flat", "rs_flat", "tp_flat"])
+def test_stage_parts_match_fused_stage_and_oracle(oracle_lib, name):
+    """dfd_stage_part splits a stage as the reference's launchers group: the fault trial
+    (state_rk, trial, fault2wave), the volume (wave_deriv, abs_deriv, RK and sponge off the
+    band) and the fault band (fault_dvelo, fault_dstrs, RK, fault2wave).  Issued part by
+    part, a run equals the fused stages bit for bit; after the trial part of each stage the
+    trial tractions match the oracle's state_rk + trial + fault2wave of that stage."""
+    a, p, fx, st, layers, w0, meta = make_sim(name)
+    b, *_ = make_sim(name)
+    o = oracle_lib.Oracle(p, fx, st, layers, double=True)
+    NZ, NY = p["NZ"], p["NY"]
+    tol = TOL[name]
+    steps = 24
+    a.run(0, steps)
+    for it in range(steps):
+        for irk in range(4):
+            b.stage_part(it, irk, 0)
+            o.stage_part(it, irk, 0)
+            if it >= steps - 2:
+                for nm in ("tTn", "tTs1", "tTs2"):
+                    assert rel(b.fault(nm), o.get(nm).reshape(NZ, NY)) < tol, (it, irk, nm)
+            for part in (1, 2):
+                b.stage_part(it, irk, part)
+                o.stage_part(it, irk, part)
+    assert np.array_equal(a.wave(), b.wave())
+    for nm in ("slip", "State", "Ts1"):
+        assert np.array_equal(a.fault(nm), b.fault(nm)), nm
+    W, Wo = b.wave(), o.wave()
+    for f in range(9):
+        assert rel(W[f], Wo[f]) < tol, f
+    a.close()
+    b.close()
+
+
+def test_stage_parts_in_order_only():
+    """Parts come in order 0, 1, 2 within stages 0..3; a step refuses a stage left half done."""
+    import dynfd3dcuda_b200 as dfd
+
+    a, *_ = make_sim("sw_flat")
+    with pytest.raises(dfd.DfdError):
+        a.stage_part(0, 0, 1)
+    a.stage_part(0, 0, 0)
+    with pytest.raises(dfd.DfdError):
+        a.run(0, 1)
+    with pytest.raises(dfd.DfdError):
+        a.stage(0, 0)
+    a.stage_part(0, 0, 1)
+    a.stage_part(0, 0, 2)
+    for irk in range(1, 4):
+        a.stage(0, irk)
+    a.run(1, 1)
+    a.close()
