@@ -1,6 +1,7 @@
 // C ABI of the B200 dynamic-rupture time step: context (device memory owner), setup,
 // stage sequencing with a side stream for the fault band, CUDA-graph replay of whole
 // steps, state access and NetCDF output.
+#include <atomic>
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -971,9 +972,11 @@ int dfd_get_slice(dfd_ctx* ctx, int axis, int index, float* host) {
 // rejected with DFD_ERR_PARAM.  The gather kernel writes every element that is copied
 // back, so nothing in the array has to start at zero.  The array is shared by every
 // context on a device: two calls that overlap in time on the same device (from two host
-// threads) race on it.
+// threads) race on it.  It occupies 16 MiB of device memory on every device where this
+// library's module is loaded, whether or not the entry is ever called.  The host-side
+// cache of its address is atomic, so first calls from several threads are safe.
 static __device__ __align__(256) float g_slice_scratch[DFD_SLICE_SCRATCH_FLOATS];
-static float* g_slice_scratch_ptr[64] = {};
+static std::atomic<float*> g_slice_scratch_ptr[64] = {};
 
 int dfd_get_slice_noalloc(dfd_ctx* ctx, int axis, int index, float* host) {
   if (!ctx || !host || axis < 0 || axis > 2) return DFD_ERR_PARAM;
@@ -988,12 +991,11 @@ int dfd_get_slice_noalloc(dfd_ctx* ctx, int axis, int index, float* host) {
   if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, DFD_ERR_PARAM, "device ordinal out of range");
   CK(cudaSetDevice(ctx->device));
   // first call on this device: look up the array's device address (setup, done once)
-  if (!g_slice_scratch_ptr[ctx->device]) {
-    float* ptr = nullptr;
-    CK(cudaGetSymbolAddress((void**)&ptr, g_slice_scratch));
-    g_slice_scratch_ptr[ctx->device] = ptr;
+  float* dv = g_slice_scratch_ptr[ctx->device].load(std::memory_order_acquire);
+  if (!dv) {
+    CK(cudaGetSymbolAddress((void**)&dv, g_slice_scratch));
+    g_slice_scratch_ptr[ctx->device].store(dv, std::memory_order_release);
   }
-  float* dv = g_slice_scratch_ptr[ctx->device];
   dfd::slice_kernel<<<(na * nb + 255) / 256, 256, 0, ctx->s0>>>(d, ctx->W[0], axis, index, dv);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(host, dv, sizeof(float) * nfloat, cudaMemcpyDeviceToHost, ctx->s0));
@@ -1051,12 +1053,21 @@ int dfd_fetch_outputs(dfd_ctx* ctx, float* host) {
 }
 
 int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* volume_ms, float* fault_ms) {
-  if (!ctx) return DFD_ERR_PARAM;
+  if (!ctx || nsteps < 0) return DFD_ERR_PARAM;
   if (ctx->sticky) return ctx->sticky;
   if (!ctx->ready || mid_step(ctx)) return fail(ctx, DFD_ERR_STATE, "not ready for a step");
   cudaSetDevice(ctx->device);
   int nev = 8 * nsteps + 2;
-  std::vector<cudaEvent_t> ev(nev), kev(8 * nsteps), fev(8 * nsteps);
+  std::vector<cudaEvent_t> ev(nev, nullptr), kev(8 * nsteps, nullptr), fev(8 * nsteps, nullptr);
+  // the events are destroyed on every return path, the early error returns included
+  struct EventSet {
+    std::vector<cudaEvent_t>* v[3];
+    ~EventSet() {
+      for (auto* l : v)
+        for (auto e : *l)
+          if (e) cudaEventDestroy(e);
+    }
+  } guard{{&ev, &kev, &fev}};
   for (auto& e : ev) CK(cudaEventCreate(&e));
   for (auto& e : kev) CK(cudaEventCreate(&e));
   for (auto& e : fev) CK(cudaEventCreate(&e));
@@ -1087,9 +1098,6 @@ int dfd_run_timed(dfd_ctx* ctx, int it0, int nsteps, float* total_ms, float* vol
       node += m;
     }
   }
-  for (auto& e : ev) cudaEventDestroy(e);
-  for (auto& e : kev) cudaEventDestroy(e);
-  for (auto& e : fev) cudaEventDestroy(e);
   ctx->interior_ms = inner;
   ctx->node_ms = node;
   if (total_ms) *total_ms = tot;

@@ -173,7 +173,8 @@ int dfd_fault_node_ms(dfd_ctx *ctx, float *ms);
  * DFD_SLICE_SCRATCH_FLOATS floats (3 x the slice's nodes), else DFD_ERR_PARAM; the first
  * call on a device looks up the array's address (setup), so make it before any stream
  * capture; the array is shared per device, so calls that overlap in time on one device
- * race. */
+ * race.  Cost: the array holds 16 MiB of device memory on every device where the library's
+ * module is loaded, whether or not this entry is called. */
 #define DFD_SLICE_SCRATCH_FLOATS (1 << 22)
 int dfd_get_slice_noalloc(dfd_ctx *ctx, int axis, int index, float *host);
 /* host-side health check: 0 ok, DFD_ERR_NONFINITE if the fault state holds NaN/Inf */

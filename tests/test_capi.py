@@ -2,8 +2,9 @@
 struct matches its ctypes mirror, job parsing follows the reference's set_params.cu, and
 bad jobs are rejected on the host before any device work.
 
-The reference's job files are read from the reference checkout when it is present (this
-only adds cases; the hand-written jobs below always run).
+The reference's job files are read from the reference checkout named by the environment
+variable DFD_REFERENCE when it is set (this only adds cases; the hand-written jobs below
+always run).
 """
 import ctypes
 import glob
@@ -18,7 +19,8 @@ import dynfd3dcuda_b200 as dfd
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "dfd_b200.h")
-REF_JOBS = sorted(glob.glob("/root/reference/jobs/*/params.json"))
+REF_ROOT = os.environ.get("DFD_REFERENCE", "")
+REF_JOBS = sorted(glob.glob(os.path.join(REF_ROOT, "jobs", "*", "params.json"))) if REF_ROOT else []
 
 
 def declared_functions():
