@@ -1,13 +1,16 @@
 #!/usr/bin/env python
 """Benchmark: grid-point-steps per second of the curved-grid rupture time step on B200.
 
-Workload (default): the curved-grid slip-weakening job -- 400 (strike) x 300 (normal) x
-200 (depth) nodes at DH = 100 m, a 60-degree dipping planar fault meshed by a curvilinear
-grid, free-surface topography of seeded Gaussian hills (amplitude 500 m, width 5 km),
-normal stress 7378 Pa/m of depth and shear 0.55 x normal, TPV10 friction, 12-node PML,
-DT = 6 ms.  Inputs are seeded synthetic data in the reference's file layouts
-(tests/golden/cases.py); each of the four 24.5 M-node volume buffers (0.88 GB) is far
-larger than the 126 MB L2, so no explicit flush is needed between steps.
+Workload (default, --config large): the large single domain the HBM roofline is quoted
+on -- 1000 (strike) x 600 (normal) x 300 (depth) nodes = 180 M at DH = 50 m, a 1-D
+layered medium (vs 2000 to 3600 m/s over depth, Media1D table), a curved non-planar
+vertical fault 50 km x 15 km (seeded along-strike bumps), normal stress 7378 Pa/m of
+depth and shear 0.55 x normal, slip-weakening friction, a 20-node PML plus a 20-node
+Cerjan sponge, free surface, DT = 4 ms.  --config curved: the curved-grid job, 400 x 300 x
+200 nodes at DH = 100 m with a 60-degree dipping fault and Gaussian-hill topography.
+Inputs are seeded synthetic data in the reference's file layouts (tests/golden/cases.py);
+each of the four volume buffers (6.7 GB for the large domain) is far larger than the
+126 MB L2, so no explicit flush is needed between steps.
 
   value      Gpt-steps/s of the stepping loop on the device: K steps replayed from the
              CUDA graphs, timed with CUDA events on the stepping stream, max over ranks
@@ -25,7 +28,7 @@ larger than the 126 MB L2, so no explicit flush is needed between steps.
              (oracle/), the reference having no CPU path, on a bounded sample of steps
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-       [--config curved|flat|profile|large|ensemble] [--scenarios S]
+       [--config large|curved|flat|profile|ensemble] [--scenarios S]
 """
 import argparse
 import json
@@ -87,9 +90,15 @@ def workload(name):
         st = cases.sw_stress(fx, fg, patch=(0.0, -6.0e3, 1.5e3), patch_ts=-81.6e6)
         label = "profiling case: Cartesian SW rupture 256x160x160, dh=100 m, PML 12"
         return job, fx, st, None, label
-    if name == "large":
-        NX, NY, NZ, DH = 600, 1000, 300, 50.0
-        fg = [101, 900, 61, 300]
+    if name in ("large", "large_profile"):
+        # large_profile: the same configuration on 320 x 160 x 160 nodes (8.2 M, about 3 GB
+        # on the device) for ncu captures, whose per-node traffic scales to the full domain
+        if name == "large":
+            NX, NY, NZ, DH = 600, 1000, 300, 50.0
+            fg, pz = [101, 900, 61, 300], -7.5e3
+        else:
+            NX, NY, NZ, DH = 160, 320, 160, 50.0
+            fg, pz = [41, 280, 41, 160], -4.0e3
         depth = np.linspace(0, 15e3, 16)
         vs = np.linspace(2000.0, 3600.0, 16)
         layers = np.stack([depth, 2670.0 + 0 * depth, np.sqrt(3.0) * vs, vs], 1).astype(np.float32)
@@ -102,8 +111,9 @@ def workload(name):
         fx[0] = (200.0 * np.sin(2 * np.pi * jj / NY * rng.uniform(1, 3)) + 0 * fx[0]).astype(np.float32)
         n = cases.surface_normal(fx, DH)
         st = cases.depth_stress(fx, fg, grad=7378.0, ratio=0.55, normal=n, mu_s=0.677, mu_d=0.525, Dc=0.4, C0=0.0,
-                                patch=(0.0, -7.5e3, 1.5e3))
-        label = "large curved-fault SW rupture 1000x600x300 (180 M nodes), dh=50 m, 1-D layered, PML 20 + Cerjan"
+                                patch=(0.0, pz, 1.5e3))
+        label = (f"large curved-fault SW rupture {NY}x{NX}x{NZ} ({NX * NY * NZ / 1e6:.0f} M nodes), dh=50 m, "
+                 "1-D layered, PML 20 + Cerjan")
         return job, fx, st, layers, label
     raise SystemExit(f"unknown config {name}")
 
@@ -363,10 +373,10 @@ def run_ensemble(args, dfd, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="curved", choices=["curved", "flat", "profile", "large", "ensemble"])
+    ap.add_argument("--config", default="large", choices=["curved", "flat", "profile", "large", "large_profile", "ensemble"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--scenarios", type=int, default=64, help="scenarios of the ensemble configuration")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned Newton-guess comparison")
@@ -445,6 +455,7 @@ def main():
     d2h = 8 * nf * 4
 
     peak, peak_kind = peaks()
+    buf_gb = 9 * (job["NX"] + 6) * (job["NY"] + 8) * (job["NZ"] + 6) * 4 / 1e9
     # dominant kernel: the interior (TMA-tiled) volume kernel, timed live with CUDA events on
     # its stream; its algorithmic bytes are 768 per node per step over the nodes it updates
     launches = 4 * ksteps
@@ -456,7 +467,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": label, "nodes": npts, "fault_nodes": nf, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (each 9-field buffer 0.88 GB); no flush"},
+                   "l2": f"inputs larger than L2 (each 9-field buffer {buf_gb:.2f} GB); no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": tpn * int_nodes / 4 if tpn else None,
                      "kernel": "volume_tile_kernel (interior box, TMA-tiled)", "peak_source": peak_kind,

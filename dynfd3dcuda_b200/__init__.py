@@ -24,6 +24,13 @@ _lib = None
 
 FIELDS = ["slip", "hslip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State", "init_t0", "tTn", "tTs1", "tTs2",
           "str_peak", "friction", "united", "faultgrid", "split", "T1", "hT1", "TP_T", "TP_P", "rup_sensor"]
+# coefficient tables of dfd_get_fault_table, in the order of the DFD_TAB_* names
+TABLES = ["D21_1", "D22_1", "D23_1", "D31_1", "D32_1", "D33_1", "D21_2", "D22_2", "D23_2", "D31_2", "D32_2", "D33_2",
+          "matMin2Plus1", "matMin2Plus2", "matMin2Plus3", "matMin2Plus4", "matMin2Plus5",
+          "matPlus2Min1", "matPlus2Min2", "matPlus2Min3", "matPlus2Min4", "matPlus2Min5",
+          "matT1toVxm", "matVytoVxm", "matVztoVxm", "matT1toVxp", "matVytoVxp", "matVztoVxp",
+          "matVx2Vz1", "matVy2Vz1", "matVx2Vz2", "matVy2Vz2", "matPlus2Min1f", "matPlus2Min2f", "matPlus2Min3f",
+          "matMin2Plus1f", "matMin2Plus2f", "matMin2Plus3f", "vec_n", "vec_s1", "vec_s2"]
 STATUS = {0: "ok", 1: "bad or unsupported parameter", 2: "CUDA error", 3: "file missing or malformed",
           4: "call out of order", 5: "DT above the stability limit", 6: "non-finite fault state",
           7: "Newton solve hit its iteration cap"}
@@ -205,7 +212,7 @@ def lib():
             "dfd_params_default": [P(DfdParams)], "dfd_params_load_json": [ctypes.c_char_p, P(DfdParams)],
             "dfd_create": [P(DfdParams), I, P(V)], "dfd_destroy": [V], "dfd_dims": [V, P(I), P(I), P(I)],
             "dfd_load_fault_geometry": [V, V], "dfd_load_media1d": [V, I, V], "dfd_load_fault_init": [V, V],
-            "dfd_load_tp_hy": [V, V], "dfd_get_tp_columns": [V, I, V],
+            "dfd_load_tp_hy": [V, V], "dfd_get_tp_columns": [V, I, V], "dfd_get_fault_table": [V, I, V],
             "dfd_precompute": [V], "dfd_stage": [V, I, I], "dfd_stage_part": [V, I, I, I], "dfd_step": [V, I],
             "dfd_run": [V, I, I],
             "dfd_synchronize": [V], "dfd_get_wave": [V, V], "dfd_set_wave": [V, V], "dfd_get_metric": [V, V],
@@ -350,6 +357,19 @@ class Simulation:
         else:
             out = np.empty((self.NZ, self.NY), np.float32)
         self._check(lib().dfd_get_fault(self.h, f, out.ctypes.data))
+        return out
+
+    def fault_table(self, name):
+        """A split-node coefficient table by its reference name (TABLES): (nz, ny, 9) per
+        fault node, (ny, 9) on the free-surface row, (nz, ny, 3) for vec_n/vec_s1/vec_s2."""
+        t = TABLES.index(name)
+        if name.startswith("vec_"):
+            out = np.empty((self.nz, self.ny, 3), np.float32)
+        elif t >= TABLES.index("matVx2Vz1"):
+            out = np.empty((self.ny, 9), np.float32)
+        else:
+            out = np.empty((self.nz, self.ny, 9), np.float32)
+        self._check(lib().dfd_get_fault_table(self.h, t, out.ctypes.data))
         return out
 
     def tp_columns(self, name):

@@ -935,6 +935,34 @@ int dfd_get_fault(dfd_ctx* ctx, int field, float* host) {
   return DFD_OK;
 }
 
+// The device keeps each table as 9 planes of (nz, ny) (element-major, so neighbouring
+// threads read neighbouring addresses); the caller gets the reference's node-major
+// [node][9] layout (fault_coef.cu:26-1312).
+static_assert(DFD_TAB_MATVZTOVXP + 1 == dfd::NTAB9, "public table names follow the device table order");
+static_assert(DFD_TAB_MATMIN2PLUS3F - DFD_TAB_MATVX2VZ1 + 1 == dfd::NTABF, "free-surface tables");
+int dfd_get_fault_table(dfd_ctx* ctx, int table, float* host) {
+  if (!ctx || !host || table < 0 || table >= DFD_TAB_COUNT) return DFD_ERR_PARAM;
+  if (!ctx->p.rupture || !ctx->tab) return fail(ctx, DFD_ERR_STATE, "rupture is off or setup has not run");
+  CK(cudaStreamSynchronize(ctx->s0));
+  const Dims& d = ctx->d;
+  const float* src;
+  size_t nodes;
+  int ne;
+  if (table <= DFD_TAB_MATVZTOVXP) {
+    src = ctx->tab + (size_t)table * 9 * d.nyz; nodes = d.nyz; ne = 9;
+  } else if (table <= DFD_TAB_MATMIN2PLUS3F) {
+    src = ctx->tabf + (size_t)(table - DFD_TAB_MATVX2VZ1) * 9 * d.ny; nodes = d.ny; ne = 9;
+  } else {
+    src = table == DFD_TAB_VEC_N ? ctx->vecn : table == DFD_TAB_VEC_S1 ? ctx->vecs1 : ctx->vecs2;
+    nodes = d.nyz; ne = 3;
+  }
+  std::vector<float> t(nodes * ne);
+  CK(cudaMemcpy(t.data(), src, sizeof(float) * t.size(), cudaMemcpyDeviceToHost));
+  for (size_t q = 0; q < nodes; q++)
+    for (int e = 0; e < ne; e++) host[q * ne + e] = t[e * nodes + q];
+  return DFD_OK;
+}
+
 int dfd_get_tp_columns(dfd_ctx* ctx, int which, float* host) {
   if (!ctx || !host || which < 0 || which > 1) return DFD_ERR_PARAM;
   if (!ctx->tp_T) return fail(ctx, DFD_ERR_STATE, "thermal pressurisation is off (Friction_type != 3)");

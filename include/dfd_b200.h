@@ -143,6 +143,26 @@ int dfd_set_wave(dfd_ctx *ctx, const float *host);  /* 9*nx*ny*nz */
 int dfd_get_metric(dfd_ctx *ctx, float *host);      /* 13*nx*ny*nz: xix..ztz jac lam mu rho */
 int dfd_get_fault(dfd_ctx *ctx, int field, float *host);
 int dfd_get_slice(dfd_ctx *ctx, int axis, int index, float *host);  /* Vx,Vy,Vz on one slice */
+/* Split-node coefficient tables of the FP64 precompute, rounded to FP32, in the layout
+ * init_fault_coef leaves them on the device (fault_coef.cu:26-1312, alloc.cu:170-260):
+ *   DFD_TAB_D21_1 .. DFD_TAB_MATVZTOVXP   (NZ+6, NY+6, 9)  per fault node, row-major 3x3
+ *   DFD_TAB_MATVX2VZ1 .. DFD_TAB_MATMIN2PLUS3F  (NY+6, 9)  free-surface row
+ *   DFD_TAB_VEC_N, _VEC_S1, _VEC_S2        (NZ+6, NY+6, 3)  fault normal and strike/dip vectors
+ * The names and their order are the reference's. */
+enum {
+  DFD_TAB_D21_1 = 0, DFD_TAB_D22_1, DFD_TAB_D23_1, DFD_TAB_D31_1, DFD_TAB_D32_1, DFD_TAB_D33_1,
+  DFD_TAB_D21_2, DFD_TAB_D22_2, DFD_TAB_D23_2, DFD_TAB_D31_2, DFD_TAB_D32_2, DFD_TAB_D33_2,
+  DFD_TAB_MATMIN2PLUS1, DFD_TAB_MATMIN2PLUS2, DFD_TAB_MATMIN2PLUS3, DFD_TAB_MATMIN2PLUS4, DFD_TAB_MATMIN2PLUS5,
+  DFD_TAB_MATPLUS2MIN1, DFD_TAB_MATPLUS2MIN2, DFD_TAB_MATPLUS2MIN3, DFD_TAB_MATPLUS2MIN4, DFD_TAB_MATPLUS2MIN5,
+  DFD_TAB_MATT1TOVXM, DFD_TAB_MATVYTOVXM, DFD_TAB_MATVZTOVXM, DFD_TAB_MATT1TOVXP, DFD_TAB_MATVYTOVXP,
+  DFD_TAB_MATVZTOVXP,
+  DFD_TAB_MATVX2VZ1, DFD_TAB_MATVY2VZ1, DFD_TAB_MATVX2VZ2, DFD_TAB_MATVY2VZ2, DFD_TAB_MATPLUS2MIN1F,
+  DFD_TAB_MATPLUS2MIN2F, DFD_TAB_MATPLUS2MIN3F, DFD_TAB_MATMIN2PLUS1F, DFD_TAB_MATMIN2PLUS2F,
+  DFD_TAB_MATMIN2PLUS3F,
+  DFD_TAB_VEC_N, DFD_TAB_VEC_S1, DFD_TAB_VEC_S2,
+  DFD_TAB_COUNT
+};
+int dfd_get_fault_table(dfd_ctx *ctx, int table, float *host);
 /* thermal pressurisation columns (Friction_type 3): which 0 = temperature TP_T, 1 = pore
  * pressure TP_P, (TP_n, NZ, NY) float32, point 0 on the fault (alloc.cu:111-116 layout) */
 int dfd_get_tp_columns(dfd_ctx *ctx, int which, float *host);

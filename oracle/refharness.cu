@@ -7,9 +7,12 @@
 // be pinned against the reference's real output.  It skips only output I/O
 // (NetCDF slices, receivers) and the unused rupture sensor.
 //
-// usage: refharness <params.json> <outdir> <nsteps> <dump_every> [--volume] [--init-wave file.f64]
+// usage: refharness <params.json> <outdir> <nsteps> <dump_every> [--volume] [--init-wave file.f64] [--time]
 //   --volume      run only the volume kernels (no rupture kernels), for stencil checks
 //   --init-wave   float64 file of 9*nx*ny*nz values copied into the wavefield at t=0
+//   --time        dump nothing; print the wall time of the stepping loop (the reference's
+//                 own per-stage cudaDeviceSynchronize included, as main.cu:511 has it)
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -160,10 +163,11 @@ int main(int argc, char **argv) {
   }
   g_out = argv[2];
   int nsteps = atoi(argv[3]), every = atoi(argv[4]);
-  bool volume = false;
+  bool volume = false, timing = false;
   const char *init_wave = nullptr;
   for (int a = 5; a < argc; a++) {
     if (!strcmp(argv[a], "--volume")) volume = true;
+    if (!strcmp(argv[a], "--time")) timing = true;
     if (!strcmp(argv[a], "--init-wave") && a + 1 < argc) init_wave = argv[++a];
   }
   g_manifest = fopen((g_out + "/manifest.txt").c_str(), "w");
@@ -257,9 +261,12 @@ int main(int argc, char **argv) {
     cudaMemcpy(W.W, wr.data(), sizeof(real_t) * wr.size(), cudaMemcpyHostToDevice);
   }
   cudaDeviceSynchronize();
-  dump_setup(M, W, F);
-  dump_state(W, F, P, 0);
+  if (!timing) {
+    dump_setup(M, W, F);
+    dump_state(W, F, P, 0);
+  }
 
+  auto t_start = std::chrono::steady_clock::now();
   for (int it = 0; it < nsteps; it++) {
     int FlagX = kFlags[it % 8][0], FlagY = kFlags[it % 8][1], FlagZ = kFlags[it % 8][2];
     // rupture sensor and thermal pressurisation once per step, before the stages
@@ -300,8 +307,13 @@ int main(int argc, char **argv) {
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { fprintf(stderr, "CUDA error at step %d: %s\n", it, cudaGetErrorString(e)); return 3; }
-    if (every > 0 && (it + 1) % every == 0) dump_state(W, F, P, it + 1);
+    if (!timing && every > 0 && (it + 1) % every == 0) dump_state(W, F, P, it + 1);
   }
+  cudaDeviceSynchronize();
+  double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  if (timing)
+    printf("refharness timing: %d steps in %.4f s, %.4f s per step, %.5f Gpt-steps/s\n", nsteps, secs,
+           secs / (nsteps > 0 ? nsteps : 1), (double)ni * nj * nk * nsteps / (secs > 0 ? secs : 1) / 1e9);
   fclose(g_manifest);
   printf("refharness done: %d steps, real_t=%zu bytes\n", nsteps, sizeof(real_t));
   return 0;

@@ -265,7 +265,49 @@ def get_case(name):
         p, fx, st, layers, w0, meta = rs_rough_case(76, 24, 40, seed=31, L=0.02, steps=40)
         p["smooth_load_T"] = 0.05
         return p, fx, st, layers, w0, dict(meta, every=20)
+    if name == "media_cj":
+        return media_case()
     raise KeyError(name)
+
+
+def media_case(NX=56, NY=100, NZ=60, DH=50.0, steps=80):
+    """The large-domain configuration in miniature: a 1-D layered medium from a Media1D
+    table (vs 2000 to 3600 m/s and rho 2400 to 2800 kg/m^3 over depth, vp = sqrt(3) vs),
+    a 20-node PML with a 20-node Cerjan sponge beside it, a non-planar fault (smooth
+    along-strike and down-dip bumps of the fault surface x(y, z)) meshed by the curvilinear
+    grid, DH = 50 m, and a slip-weakening rupture (TPV10-style depth-dependent stress and
+    friction) nucleated at 700 m depth.  Layer depths
+    lie between node depths so that the layer each node takes does not hinge on rounding.
+    The reference's FP64 build cannot read a Media1D table (media.cu:84 scans "%g" into
+    double), so this case has an FP32 reference fixture only."""
+    fg = [31, NY - 30, 31, NZ]
+    p = dict(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=0.004, TMAX=steps * 0.004 + 0.002, PML_N=20, PML_velocity=6236.0,
+             INPORT_GRID_TYPE=1, INPORT_STRESS_TYPE=1, Friction_type=0, Fault_grid=fg, mu_s=0.76,
+             mu_d=0.448, Dc=0.01, C0=0.2e6, useCerjan=1, DAMP_N=20)
+    fx = flat_geometry(NY, NZ, DH).astype(np.float64)
+    j = np.arange(NY)[None, :]
+    k = np.arange(NZ)[:, None]
+    fx[0] = 60.0 * np.sin(2 * np.pi * 1.3 * j / NY + 0.4) + 30.0 * np.cos(2 * np.pi * 0.6 * k / NZ)
+    fx = fx.astype(np.float32)
+    n = surface_normal(fx, DH)
+    st = depth_stress(fx, fg, normal=n, Dc=0.01, patch=(0.0, -700.0, 400.0))
+    depth = np.array([0.0, 325.0, 625.0, 925.0, 1225.0, 1525.0, 2025.0])
+    vs = np.linspace(2000.0, 3600.0, depth.size)
+    rho = np.linspace(2400.0, 2800.0, depth.size)
+    layers = np.stack([depth, rho, np.sqrt(3.0) * vs, vs], 1).astype(np.float32)
+    return p, fx, st, layers, None, dict(steps=steps, every=steps // 2, volume=False, variants=("sp",),
+                                         jblock=(36, 72))
+
+
+def write_media1d(fn, layers):
+    """A Media1D text file as init_media1d reads it (media.cu:63-90): a comment line, the
+    layer count, a column header, then one 'depth rho vp vs' row per layer."""
+    with open(fn, "w") as f:
+        f.write("# 1-D layered medium\n")
+        f.write(f"{len(layers)}\n")
+        f.write("depth rho vp vs\n")
+        for row in np.asarray(layers, np.float32):
+            f.write(" ".join(f"{float(v):.9g}" for v in row) + "\n")
 
 
 def rs_rough_case(NY, NX, NZ, seed=0, DH=100.0, steps=40, L=0.4):
@@ -314,15 +356,22 @@ def ensemble_case(i, seed=2025, size=(100, 300), DH=100.0, DT=0.008, steps=1000)
     return p, fx, st
 
 
-CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan", "tp_flat", "rs_aging", "rs_curved"]
+CASES = ["vol_small", "vol_curved", "sw_flat", "sw_flat_nr", "sw_curved", "rs_flat", "sw_cerjan", "tp_flat", "rs_aging",
+         "rs_curved", "media_cj"]
 
 
 def write_inputs(name, outdir):
-    """Write params.json, Fault_geometry / Fault_init_stress NetCDF-classic files and the
-    optional initial wavefield for the reference harness."""
+    """Write params.json, Fault_geometry / Fault_init_stress NetCDF-classic files, the
+    Media1D table and the optional initial wavefield for the reference harness."""
+    p, fx, st, layers, w0, meta = get_case(name)
+    return write_job(outdir, p, fx, st, layers, w0), meta
+
+
+def write_job(outdir, p, fx=None, st=None, layers=None, w0=None):
+    """Write a job (parameters and input arrays) in the reference's file formats; returns
+    the params.json dictionary."""
     from scipy.io import netcdf_file
 
-    p, fx, st, layers, w0, meta = get_case(name)
     os.makedirs(outdir, exist_ok=True)
     job = dict(p)
     job["OUT"] = outdir
@@ -347,8 +396,12 @@ def write_inputs(name, outdir):
                 v = f.createVariable(nm, "f4", ("nz", "ny"))
                 v[:] = st[c]
         job["Fault_init_stress"] = fn
+    if layers is not None:
+        fn = os.path.join(outdir, "media1d.txt")
+        write_media1d(fn, layers)
+        job["Media1D"] = fn
     with open(os.path.join(outdir, "params.json"), "w") as f:
         json.dump(job, f, indent=1)
     if w0 is not None:
         w0.astype(np.float64).tofile(os.path.join(outdir, "wave0.f64"))
-    return job, meta
+    return job

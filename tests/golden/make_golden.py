@@ -31,9 +31,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
 import cases  # noqa: E402
 
-# block of padded (j, k) indices kept for the rupture cases: the non-united nodes plus
-# the stencil halo
-J0, J1 = 24, 52
+# block of padded j indices kept for the rupture cases (the non-united nodes plus the
+# stencil halo on the 76-node grids); a case may name its own block (meta "jblock")
+JBLOCK = (24, 52)
 
 
 def load_dumps(d):
@@ -74,9 +74,11 @@ def run_case(name, variant, outdir):
     NX, NY, NZ = p["NX"], p["NY"], p["NZ"]
     nx, ny, nz = NX + 6, NY + 6, NZ + 6
     i0 = nx // 2
+    J0, J1 = meta.get("jblock", JBLOCK)
     steps = sorted({s for (_, s) in dumps if s >= 0})
     last = steps[-1]
-    save = {"params": np.array(json.dumps(p)), "steps": np.array(steps), "variant": np.array(variant)}
+    save = {"params": np.array(json.dumps(p)), "steps": np.array(steps), "variant": np.array(variant),
+            "jblock": np.array([J0, J1])}
     for s in steps:
         W = dumps[("W", s)].reshape(9, nx, nz, ny)
         save[f"Wsum_s{s}"] = np.stack([checksums(W[f]) for f in range(9)])
@@ -133,7 +135,10 @@ def main():
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     for c in a.cases.split(","):
+        allowed = cases.get_case(c)[5].get("variants", ("sp", "dp"))
         for v in a.variants.split(","):
+            if v not in allowed:
+                continue
             fn = run_case(c, v, a.out)
             print(f"wrote {fn} ({os.path.getsize(fn) / 1e3:.0f} kB)", flush=True)
 

@@ -17,12 +17,13 @@ import cases
 
 pytestmark = pytest.mark.gpu
 
-J0, J1 = 24, 52
 TOL = {"vol_small": 2e-5, "vol_curved": 2e-5, "sw_flat": 2e-4, "sw_flat_nr": 2e-4, "sw_curved": 5e-4,
        "rs_flat": 2e-3, "sw_cerjan": 2e-4, "tp_flat": 2e-3, "rs_aging": 2e-3,
        # the reference's own FP32 build lies 1.6e-3 from FP64 here (rate and state on a rough
        # fault): the FP32 product is held to the sum of both roundings against that build
-       "rs_curved": 3e-3}
+       "rs_curved": 3e-3,
+       # layered medium, PML 20, Cerjan 20, non-planar fault (the large-domain configuration)
+       "media_cj": 5e-4}
 
 
 def rel(a, b):
@@ -30,6 +31,15 @@ def rel(a, b):
     b = np.asarray(b, np.float64)
     s = np.abs(b).max()
     return np.abs(a - b).max() / (s if s > 0 else 1.0)
+
+
+def sensor_mask(ts1):
+    """Nodes where the rupture sensor is well conditioned.  It divides jumps of second
+    differences of Ts1 by Ts1^2 (rup_sensor.cu:8-95), so where Ts1 passes through zero
+    (a fault loaded along dip) FP32 rounding of Ts1 alone changes it by percent; the
+    comparison keeps the nodes with |Ts1| above 5 % of its maximum."""
+    a = np.abs(np.asarray(ts1, np.float64))
+    return a > 5e-2 * a.max()
 
 
 def make_sim(name):
@@ -62,6 +72,7 @@ def test_cuda_matches_oracle(oracle_lib, name, mode):
         assert rel(M[f], Mo[f]) < 2e-6, f
     tol = TOL[name]
     g = np.load(f"{cases.__file__[:-8]}/{name}_sp.npz")
+    J0, J1 = (int(v) for v in g["jblock"]) if "jblock" in g.files else (24, 52)
     steps = [int(s) for s in g["steps"]]
     it = 0
     for s in steps:
@@ -85,9 +96,11 @@ def test_cuda_matches_oracle(oracle_lib, name, mode):
                 assert rel(a, g[f"{nm}_s{s}"]) < tol, (s, nm, "vs reference FP32 build")
             t0 = sim.fault("init_t0")
             assert np.abs(t0 - o.get("init_t0").reshape(NZ, NY)).max() <= 1.01 * p["DT"]
-            a = sim.fault("rup_sensor")  # rupture sensor of the step start
-            assert rel(a, o.get("rup_sensor").reshape(NZ, NY)) < tol, (s, "rup_sensor")
-            assert rel(a, g[f"rup_sensor_s{s}"]) < tol, (s, "rup_sensor", "vs reference FP32 build")
+            # rupture sensor of the step start, where it is well conditioned
+            a = sim.fault("rup_sensor")
+            m = sensor_mask(o.get("Ts1").reshape(NZ, NY))
+            assert rel(a[m], o.get("rup_sensor").reshape(NZ, NY)[m]) < tol, (s, "rup_sensor")
+            assert rel(a[m], g[f"rup_sensor_s{s}"][m]) < tol, (s, "rup_sensor", "vs reference FP32 build")
             if p.get("Friction_type") == 3:  # thermal pressurisation at the fault
                 for nm in ("TP_T", "TP_P"):
                     a = sim.fault(nm)
@@ -301,3 +314,30 @@ def test_stage_parts_in_order_only():
         a.stage(0, irk)
     a.run(1, 1)
     a.close()
+
+
+RUPTURE_DP = [c for c in cases.CASES if not cases.get_case(c)[5]["volume"]
+              and "dp" in cases.get_case(c)[5].get("variants", ("sp", "dp"))]
+
+
+@pytest.mark.parametrize("name", RUPTURE_DP)
+def test_fault_tables_match_reference(oracle_lib, name):
+    """The GPU's FP64 precompute of the split-node coefficient tables, table by table:
+    against the reference's FP64 build (the tables its fixtures hold, over their block)
+    and against the FP64 oracle (every table over the whole plane), to FP32 rounding."""
+    import dynfd3dcuda_b200 as dfd
+
+    sim, p, fx, st, layers, w0, meta = make_sim(name)
+    g = np.load(f"{cases.__file__[:-8]}/{name}_dp.npz")
+    J0, J1 = (int(v) for v in g["jblock"]) if "jblock" in g.files else (24, 52)
+    o = oracle_lib.Oracle(p, fx, st, layers, double=True)
+    for nm in ("D21_1", "D33_2", "matPlus2Min1", "matMin2Plus5", "matT1toVxm", "matVztoVxp", "vec_n", "vec_s1",
+               "vec_s2"):
+        assert rel(sim.fault_table(nm)[:, J0:J1], g[nm]) < 2e-6, (nm, "vs reference FP64 build")
+    for nm in ("matVx2Vz1", "matPlus2Min2f", "matMin2Plus3f"):
+        assert rel(sim.fault_table(nm), g[nm]) < 2e-6, (nm, "vs reference FP64 build")
+    for nm in dfd.TABLES:
+        a = sim.fault_table(nm)
+        b = o.get(nm).reshape(a.shape)
+        assert rel(a, b) < 2e-6, (nm, rel(a, b))
+    sim.close()

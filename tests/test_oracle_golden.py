@@ -11,7 +11,6 @@ import pytest
 
 import cases
 
-J0, J1 = 24, 52
 
 # relative max-error tolerances (of the field's max magnitude).  FP64-vs-FP64 is limited by
 # the fixtures' FP32 storage (the oracle reproduces the reference's single-precision sqrtf
@@ -29,6 +28,7 @@ TOL = {
     ("tp_flat", "dp"): 1e-5, ("tp_flat", "sp"): 3e-4,
     ("rs_aging", "dp"): 1e-6, ("rs_aging", "sp"): 1e-3,
     ("rs_curved", "dp"): 1e-5, ("rs_curved", "sp"): 3e-3,
+    ("media_cj", "sp"): 1e-4,  # no FP64 fixture: the reference's FP64 build misreads Media1D
 }
 
 
@@ -37,6 +37,13 @@ def rel(a, b):
     b = np.asarray(b, np.float64)
     s = np.abs(b).max()
     return np.abs(a - b).max() / (s if s > 0 else 1.0)
+
+
+def sensor_mask(ts1):
+    """Nodes where the rupture sensor (jumps of second differences of Ts1 over Ts1^2,
+    rup_sensor.cu:8-95) is well conditioned: |Ts1| above 5 % of its maximum."""
+    a = np.abs(np.asarray(ts1, np.float64))
+    return a > 5e-2 * a.max()
 
 
 @pytest.mark.parametrize("name,var", sorted(TOL))
@@ -50,6 +57,7 @@ def test_oracle_matches_reference(oracle_lib, name, var):
     nx, ny, nz = NX + 6, NY + 6, NZ + 6
     i0 = nx // 2
     tol = TOL[(name, var)]
+    J0, J1 = (int(v) for v in g["jblock"]) if "jblock" in g.files else (24, 52)
     if var == "dp":
         M = o.get("M").reshape(13, nx, nz, ny)
         assert rel(M[:, i0 - 1:i0 + 2], g["M_planes"]) < 1e-6
@@ -75,8 +83,9 @@ def test_oracle_matches_reference(oracle_lib, name, var):
             # rupture times are identical to the step
             t0 = o.get("init_t0").reshape(NZ, NY)
             assert np.abs(t0 - g[f"init_t0_s{s}"]).max() < 0.5 * p["DT"]
-            if f"rup_sensor_s{s}" in g:  # rupture sensor of the step start
-                assert rel(o.get("rup_sensor").reshape(NZ, NY), g[f"rup_sensor_s{s}"]) < tol, ("rup_sensor", s)
+            if f"rup_sensor_s{s}" in g:  # rupture sensor of the step start, where well conditioned
+                m = sensor_mask(o.get("Ts1").reshape(NZ, NY))
+                assert rel(o.get("rup_sensor").reshape(NZ, NY)[m], g[f"rup_sensor_s{s}"][m]) < tol, ("rup_sensor", s)
             for nm in ("TP_T", "TP_P"):  # thermal pressurisation: the point on the fault
                 if f"{nm}_s{s}" in g:
                     assert rel(o.get(nm).reshape(-1, NZ, NY)[0], g[f"{nm}_s{s}"]) < tol, (nm, s)
