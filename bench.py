@@ -108,7 +108,8 @@ def workload(name):
         fx = cases.curved_geometry(NY, NZ, DH, dip_deg=90.0, hill_amp=0.0, seed=7)
         rng = np.random.default_rng(7)
         jj = np.arange(NY)[None, :]
-        fx[0] = (200.0 * np.sin(2 * np.pi * jj / NY * rng.uniform(1, 3)) + 0 * fx[0]).astype(np.float32)
+        # along-strike bumps of the same wavelengths (in metres) on both grid sizes
+        fx[0] = (200.0 * np.sin(2 * np.pi * jj / 1000 * rng.uniform(1, 3)) + 0 * fx[0]).astype(np.float32)
         n = cases.surface_normal(fx, DH)
         st = cases.depth_stress(fx, fg, grad=7378.0, ratio=0.55, normal=n, mu_s=0.677, mu_d=0.525, Dc=0.4, C0=0.0,
                                 patch=(0.0, pz, 1.5e3))
@@ -276,7 +277,9 @@ def learned_rs(dfd, steps=600, every=7, epochs=4, device=0):
     """The learned Newton guess on the rate-and-state rough-fault configuration
     (300 x 200 x 150, slip law): record plain-solver samples on one seed, train the MLP on
     the GPU, then run another seed with the plain and with the learned guess and compare
-    the fault node kernel time, Newton iterations per solve and the final slip."""
+    the fault node kernel time, the clock cycles of the solve section alone (guess,
+    network, Newton iterations), Newton iterations per solve, the residual test's
+    acceptance and the final slip."""
     import cases
 
     job, fx, st, _, _, _ = cases.rs_rough_case(300, 200, 150, seed=11, steps=steps)
@@ -295,6 +298,7 @@ def learned_rs(dfd, steps=600, every=7, epochs=4, device=0):
            "train_samples": int(len(samples)), "epochs": epochs, "train_s": train_s,
            "loss_per_epoch": [float(v) for v in hist]}
     slips = {}
+    nprof = 40  # steps with the solve section timed (clock64 around guess, network and Newton)
     for name, net in (("plain", None), ("learned", w)):
         sim = dfd.Simulation(job, fx, st, None, device=device)
         if net is not None:
@@ -302,17 +306,28 @@ def learned_rs(dfd, steps=600, every=7, epochs=4, device=0):
         sim.run(0, 5)
         sim.synchronize()
         it0, cap0 = sim.newton_stats()
-        total_ms, vol_ms, _ = sim.run_timed(5, steps - 5)
+        acc0, fb0, _, _ = sim.rs_solve_stats()
+        total_ms, vol_ms, _ = sim.run_timed(5, steps - 5 - nprof)
         node_ms = sim.fault_node_ms()
         it1, cap1 = sim.newton_stats()
-        solves = nact * 4 * (steps - 5)
+        acc1, fb1, _, _ = sim.rs_solve_stats()
+        nst = steps - 5 - nprof
+        solves = nact * 4 * nst
+        sim.rs_profile(timing=True)
+        sim.run(steps - nprof, nprof)
+        _, _, cyc, _ = sim.rs_solve_stats()
         slips[name] = sim.fault("slip").astype(np.float64)
-        out[name] = {"node_kernel_us_per_stage": 1e3 * node_ms / (4 * (steps - 5)),
+        out[name] = {"node_kernel_us_per_stage": 1e3 * node_ms / (4 * nst),
                      "newton_iterations_per_solve": (it1 - it0) / solves,
-                     "unconverged_solves": int(cap1 - cap0), "step_ms": total_ms / (steps - 5)}
+                     "solve_cycles_per_node": cyc,
+                     "unconverged_solves": int(cap1 - cap0), "step_ms": total_ms / nst}
+        if net is not None:
+            out[name]["guesses_accepted"] = int(acc1 - acc0)
+            out[name]["guesses_fell_back"] = int(fb1 - fb0)
         sim.close()
     p, l = out["plain"], out["learned"]
     out["speedup_node_kernel"] = p["node_kernel_us_per_stage"] / l["node_kernel_us_per_stage"]
+    out["speedup_solve_section"] = p["solve_cycles_per_node"] / l["solve_cycles_per_node"]
     out["speedup_newton_iterations"] = p["newton_iterations_per_solve"] / l["newton_iterations_per_solve"]
     s0 = np.abs(slips["plain"]).max()
     out["final_slip_max_m"] = float(s0)

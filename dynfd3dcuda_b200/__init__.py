@@ -129,6 +129,16 @@ def mlp_forward(w, x):
     return y
 
 
+def mlp_forward_node(w, x, tensor_cores=True):
+    """Residuals from the fault node kernel's own inference (per-thread or tensor-core
+    network) for inputs x (n, 4), on the GPU."""
+    w = np.ascontiguousarray(w, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.empty(len(x), np.float32)
+    _check(lib().dfd_mlp_forward_node(w.ctypes.data, x.ctypes.data, len(x), int(tensor_cores), y.ctypes.data))
+    return y
+
+
 def mlp_loss_grad(w, x, y):
     """(mean squared standardised error, gradient over the MLP_TRAINABLE weights), on the GPU."""
     w = np.ascontiguousarray(w, np.float32)
@@ -189,7 +199,7 @@ class DfdParams(ctypes.Structure):
         ("use_cerjan", ctypes.c_int), ("normal_refine", ctypes.c_int), ("rs_guess", ctypes.c_int),
         ("OUT", ctypes.c_char * 1024), ("Fault_geometry", ctypes.c_char * 1024),
         ("Fault_init_stress", ctypes.c_char * 1024), ("Media1D", ctypes.c_char * 1024),
-        ("TP_n", ctypes.c_int),
+        ("TP_n", ctypes.c_int), ("rs_guess_tol", ctypes.c_double),
     ]
 
 
@@ -197,7 +207,7 @@ class DfdParams(ctypes.Structure):
 # reference's compile-time switches as job keys)
 _KEYMAP = {"RS_V0": "V0", "RS_Vini": "Vini", "RS_f0": "f0", "RS_fw": "fw", "RS_L": "L", "rho1": "bi_rho1",
            "Rupture": "rupture", "FreeSurface": "free_surface", "usePML": "use_pml", "useCerjan": "use_cerjan",
-           "NormalRefine": "normal_refine", "RS_guess": "rs_guess"}
+           "NormalRefine": "normal_refine", "RS_guess": "rs_guess", "RS_guess_tol": "rs_guess_tol"}
 
 
 def lib():
@@ -226,9 +236,11 @@ def lib():
             "dfd_ens_create": [V, I, P(ctypes.c_void_p)], "dfd_ens_destroy": [V], "dfd_ens_run": [V, I, I],
             "dfd_ens_synchronize": [V], "dfd_ens_run_timed": [V, I, I, P(ctypes.c_float)],
             "dfd_ens_set_chunk": [V, I], "dfd_ens_nodes": [V, P(ctypes.c_longlong)],
-            "dfd_newton_record": [V, I, I], "dfd_fault_node_ms": [V, P(ctypes.c_float)], "dfd_newton_samples": [V, V, I, P(ctypes.c_int)],
+            "dfd_newton_record": [V, I, I], "dfd_rs_profile": [V, I, I],
+            "dfd_rs_solve_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong), P(ctypes.c_double),
+                                   P(ctypes.c_double)], "dfd_fault_node_ms": [V, P(ctypes.c_float)], "dfd_newton_samples": [V, V, I, P(ctypes.c_int)],
             "dfd_mlp_init": [V, ctypes.c_uint, V, V, ctypes.c_float, ctypes.c_float],
-            "dfd_mlp_forward": [V, V, I, V],
+            "dfd_mlp_forward": [V, V, I, V], "dfd_mlp_forward_node": [V, V, I, I, V],
             "dfd_mlp_loss_grad": [V, V, V, I, P(ctypes.c_double), V],
             "dfd_mlp_train": [V, V, I, I, I, ctypes.c_float, ctypes.c_uint, V, V],
         }
@@ -400,6 +412,19 @@ class Simulation:
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(lib().dfd_newton_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def rs_profile(self, timing=True, judge=False):
+        """Switch the rate-and-state solve measurement aids (solve timing, plain-solve judge)."""
+        self._check(lib().dfd_rs_profile(self.h, int(timing), int(judge)))
+
+    def rs_solve_stats(self):
+        """(accepted learned guesses, fallbacks to the plain solve, mean clock cycles of a timed
+        solve, judge's largest relative difference)."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        c, d = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().dfd_rs_solve_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                             ctypes.byref(d)))
+        return a.value, b.value, c.value, d.value
 
     def fetch_outputs(self, host_ptr):
         """Enqueue the copy of the (8, NZ, NY) per-step outputs into host memory at host_ptr."""

@@ -18,7 +18,7 @@ EXE = os.path.join(HERE, "dfd_b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU = ["dfd_volume.cu", "dfd_tile.cu", "dfd_pml.cu", "dfd_fault.cu", "dfd_mlp.cu", "dfd_precompute.cu", "dfd_setup.cu", "dfd_api.cu"]
 CPP = ["dfd_host.cpp", "dfd_netcdf.cpp"]
-HEADERS = ["dfd_internal.cuh", "dfd_stencil.cuh", "dfd_tma.cuh", "dfd_host.h"]
+HEADERS = ["dfd_internal.cuh", "dfd_stencil.cuh", "dfd_tma.cuh", "dfd_mlp.cuh", "dfd_host.h"]
 
 
 def nvcc():

@@ -122,6 +122,7 @@ struct dfd_ctx {
   unsigned* rec_n = nullptr;
   int rec_cap = 0;
   int rec_every = 1;
+  int rs_prof = 0, rs_judge = 0;   // solve-section timing and judge mode (measurement aids)
   TileCtx tile;                    // tiled interior kernel (TMA maps)
   int* tile_err = nullptr;
   int* tile_sched = nullptr;         // tiled kernel's unit counters
@@ -312,7 +313,7 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
       if (!rc) rc = dalloc(ctx, &ctx->tp_hy, (long long)d.nj * d.nk);
     }
   }
-  if (!rc) rc = dalloc(ctx, &ctx->newton, 2);
+  if (!rc) rc = dalloc(ctx, &ctx->newton, 8);
   if (!rc) rc = dalloc(ctx, &ctx->it_dev, 1);
   if (!rc) rc = dalloc(ctx, &ctx->flag_dev, 1);
   if (!rc) rc = dalloc(ctx, &ctx->guess_net, DFD_MLP_PARAMS);
@@ -538,7 +539,7 @@ int dfd_precompute(dfd_ctx* ctx) {
   for (int b = 0; b < 4; b++) CK(cudaMemsetAsync(ctx->W[b], 0, sizeof(float) * 9 * d.nxyz, s));
   for (int f = 0; f < 6; f++)
     if (ctx->aux[f][0]) CK(cudaMemsetAsync(ctx->aux[f][0], 0, sizeof(float) * 27 * pml_fstride(d, f), s));
-  CK(cudaMemsetAsync(ctx->newton, 0, 2 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(ctx->newton, 0, 8 * sizeof(unsigned long long), s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
   for (auto& gr : ctx->graph)
@@ -606,6 +607,7 @@ static FaultArgs fault_args(dfd_ctx* ctx, int pattern, int irk) {
     fa.irk = irk; fa.FX = FX; fa.FY = FY; fa.FZ = FZ;
     fa.freenode = p.free_surface; fa.friction_type = p.Friction_type; fa.inport_stress = p.INPORT_STRESS_TYPE;
     fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess;
+    fa.prof = ctx->rs_prof; fa.judge = ctx->rs_judge; fa.guess_tol = p.rs_guess_tol;
   }
   (void)FX;
   return fa;
@@ -1159,6 +1161,37 @@ int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {
   return DFD_OK;
 }
 
+int dfd_rs_profile(dfd_ctx* ctx, int timing, int judge) {
+  if (!ctx) return DFD_ERR_PARAM;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  ctx->rs_prof = timing ? 1 : 0;
+  ctx->rs_judge = judge ? 1 : 0;
+  // the switches are baked into the step graphs: rebuild them
+  for (auto& g : ctx->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return DFD_OK;
+}
+
+int dfd_rs_solve_stats(dfd_ctx* ctx, long long* accepted, long long* fallback, double* cycles_per_solve,
+                       double* judge_max_rel) {
+  if (!ctx) return DFD_ERR_PARAM;
+  unsigned long long v[8] = {};
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  CK(cudaMemcpy(v, ctx->newton, sizeof v, cudaMemcpyDeviceToHost));
+  if (accepted) *accepted = (long long)v[2];
+  if (fallback) *fallback = (long long)v[3];
+  if (cycles_per_solve) *cycles_per_solve = v[5] ? (double)v[4] / (double)v[5] : 0.0;
+  if (judge_max_rel) {
+    float f;
+    unsigned u = (unsigned)v[6];
+    memcpy(&f, &u, sizeof f);
+    *judge_max_rel = f;
+  }
+  return DFD_OK;
+}
+
 int dfd_newton_record(dfd_ctx* ctx, int capacity, int every) {
   if (!ctx || capacity < 0 || every < 1) return DFD_ERR_PARAM;
   ctx->rec_every = every;
@@ -1525,7 +1558,7 @@ static int ens_build(dfd_ens* e) {
         a.it_dev = e->it_dev;  // one step counter for the whole ensemble
         fa.push_back(a);
         const int g = ((a.d.nj + 31) / 32) * ((a.d.nk + 3) / 4);
-        fs.push_back(fs.back() + g);
+        fs.push_back(fs.back() + node_blocks(a.NY, a.NZ, a.freenode));
         bs.push_back(bs.back() + 7 * g);  // the band kernel: seven parts per column block
       }
       S.fblocks = fs.back();

@@ -1,6 +1,7 @@
 // Split-node fault kernels of one RK stage.
 //
-// fault_node_kernel (one thread per non-united fault node), first in the stage:
+// fault_node_kernel (one thread per non-united fault node, numbered row by row over their
+//   rectangle), first in the stage:
 //   state and slip RK4 with the rate-and-state evolution law in FP64 (rk4.cu:791-938),
 //   trial traction + slip-weakening (trial_slipweakening.cu:23-732) or rate-and-state
 //   FP64 Newton solve (trial_ratestate.cu:20-893), then the split-node -> volume transfer
@@ -12,6 +13,7 @@
 //   update of those band nodes and of the split nodes (rk4.cu:573-789), the RK-weighted
 //   on-fault outputs (rk4.cu:466-571), the end-of-stage transfer and the sponge.
 #include "dfd_internal.cuh"
+#include "dfd_mlp.cuh"
 #include "../../include/dfd_b200.h"
 
 namespace dfd {
@@ -160,51 +162,13 @@ __device__ __forceinline__ double gt_func(double t, double T) {  // device.cu:13
   return 1.0;
 }
 
-// Learned initial guess: MLP 4 -> 32 -> 32 -> 1 (tanh) on the standardised inputs; the
-// de-standardised output is the residual x* - asinh(Vhat e^{psi/a} / (2 V0)).  Weight
-// layout (dfd_mlp.cu): W1[32][4] b1[32] W2[32][32] b2[32] W3[32] b3 mu[4] sd[4] ymu ysd.
-// The hidden activations use the hardware tanh approximation (absolute error ~5e-4): the
-// output is scaled by the residual's small standard deviation, and the Newton iteration
-// that follows removes what is left.
-__device__ __forceinline__ float tanh_fast(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ float mlp_residual(const float* w, const float* xin) {
-  const float4* W1 = reinterpret_cast<const float4*>(w);  // rows of 4
-  const float* b1 = w + 128;
-  const float4* W2 = reinterpret_cast<const float4*>(w + 160);
-  const float* b2 = w + 1184;
-  const float* W3 = w + 1216;
-  const float* b3 = w + 1248;
-  const float* mu = b3 + 1;
-  const float* sd = mu + 4;
-  const float* ys = sd + 4;
-  float x[4];
-#pragma unroll
-  for (int c = 0; c < 4; c++) x[c] = (xin[c] - mu[c]) / sd[c];
-  float h1[32];
-#pragma unroll
-  for (int r = 0; r < 32; r++) {
-    const float4 wr = W1[r];
-    float s = b1[r];
-    s = fmaf(wr.x, x[0], s); s = fmaf(wr.y, x[1], s); s = fmaf(wr.z, x[2], s); s = fmaf(wr.w, x[3], s);
-    h1[r] = tanh_fast(s);
-  }
-  float out = *b3;
-#pragma unroll 4
-  for (int r = 0; r < 32; r++) {
-    float s = b2[r];
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const float4 wv = W2[r * 8 + c];
-      s = fmaf(wv.x, h1[4 * c], s); s = fmaf(wv.y, h1[4 * c + 1], s);
-      s = fmaf(wv.z, h1[4 * c + 2], s); s = fmaf(wv.w, h1[4 * c + 3], s);
-    }
-    out = fmaf(W3[r], tanh_fast(s), out);
-  }
-  return out * ys[1] + ys[0];
+// Base of the learned guess: the root asinh(Vhat e^{psi/a} / (2 V0)) of the solve without
+// the radiation-damping term, V0 = 1e-6; from its logarithm where the argument is above
+// e^18 (asinh y = ln 2y + 1/(4 y^2) + ..., the rest below FP64 rounding there), which
+// also keeps e^{psi/a} from overflowing.  Takes ln Vhat and psi/a.
+__device__ __forceinline__ double guess_base(double lnVhat, double psi_over_a) {
+  const double ly = lnVhat + psi_over_a + 13.122363377404328;  // ln(1 / 2e-6)
+  return ly > 18.0 ? ly + 0.6931471805599453 : asinh(exp(ly));
 }
 
 // Bounded Newton on f(x) = 2 V0 e^{-psi/a} sinh x + coef x - Vhat (trial_ratestate.cu:20-57);
@@ -233,7 +197,7 @@ __device__ double newton_rs(double x, double psi, double ra, double Vhat, double
 // Body of the fault node kernel for the block (bx, by) of a (32, 4) grid over (NY, NZ);
 // snet is the block's shared copy of the learned-guess weights.
 template <int FY, int FZ>
-__device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int by, float* snet) {
+__device__ __forceinline__ void fault_node_body(const FaultArgs& a, int blk, float* snet) {
   const Dims& d = a.d;
   // learned-guess weights staged in shared memory (every thread reads the same weight at
   // the same time: a broadcast)
@@ -243,11 +207,18 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int 
     for (int p = tid; p < DFD_MLP_PARAMS; p += nt) snet[p] = __ldg(a.guess_net + p);
     __syncthreads();
   }
-  int j = bx * blockDim.x + threadIdx.x;
-  int k = by * blockDim.y + threadIdx.y;
-  if (j >= d.nj || k >= d.nk) return;
-  int q2 = j + k * d.nj;
-  if (a.united[q2]) return;
+  // node t of the non-united rectangle, numbered row by row
+  const NodeRect rc = node_rect(a.NY, a.NZ, a.freenode);
+  const long long tn = (long long)blk * blockDim.x + threadIdx.x;
+  const bool inr = tn < rc.count();
+  const int j = inr ? rc.j0 + (int)(tn % rc.w) : 0, k = inr ? rc.k0 + (int)(tn / rc.w) : 0;
+  const int q2 = j + k * d.nj;
+  const bool live = inr && !a.united[q2];
+  // the tensor-core network takes a whole warp (32 consecutive nodes of the rectangle):
+  // it runs where every lane's node is live (all warps but the last), the per-thread
+  // network elsewhere
+  const bool warp_full = __all_sync(0xffffffffu, live);
+  if (!live) return;
   const long long n = d.nxyz, nyz = d.nyz;
   const int j1 = j + 3, k1 = k + 3, km = d.nk - k;
   const long long pf = j1 + (long long)k1 * d.ny;
@@ -451,50 +422,105 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int bx, int 
     double Vtn = sqrt(Vt1 * Vt1 + Vt2 * Vt2);
     double Ttn = sqrt(Tl[1] * Tl[1] + Tl[2] * Tl[2]);
     double Rn = sqrt(Rl[1] * Rl[1] + Rl[2] * Rl[2]);
-    const double es = exp(st / ra);
+    const double psi_a = st / ra;
+    const double es = exp(psi_a);
     int its = 0, its2 = 0;
     bool ok = false;
     double xn;
     // network inputs (FP32, as the network computes), needed by the learned guess and by
     // the sample recording only
-    auto features = [&](float* fin) {
-      fin[0] = (float)(st / ra);
-      fin[1] = log10f(fmaxf((float)Vtn, 1e-30f));
+    // network inputs (FP32, as the network computes), from ln Vhat, which the guess's base
+    // needs too
+    auto features = [&](double lnV, float* fin) {
+      fin[0] = (float)psi_a;
+      fin[1] = (float)fmax(lnV * 0.4342944819032518, -30.0);  // log10 max(Vhat, 1e-30)
       fin[2] = log10f(fmaxf((float)coef, 1e-30f));
       fin[3] = (float)ra;
     };
+    long long clk0 = 0;
+    if (a.prof) clk0 = clock64();
+    bool accepted = false;
     if (a.rs_guess && a.guess_net) {
-      // learned guess: the root without radiation damping corrected by the network, then
-      // the same Newton iteration (capped); the plain solve from the reference's guess
-      // takes over whenever it does not converge
+      // learned guess: the root without radiation damping corrected by the network.  Newton
+      // corrections are evaluated from the guess (sinh and cosh from one expm1), and after
+      // each the residual test bounds the error left, |f''| dd^2 / (2 f') with f'' taken at
+      // its largest over the step (the iteration converges quadratically): the corrected
+      // guess is accepted when that bound is at most guess_tol |x|.  After two corrections
+      // without acceptance the plain solve from the reference's guess runs.
+      const double lnV = log(fmax(Vtn, 1e-300));
       float fin[4];
-      features(fin);
-      double xa = asinh(Vtn * es / (2.0 * 1e-6));
-      double xg = xa + (double)mlp_residual(snet, fin);
-      xn = newton_rs(xg, st, ra, Vtn, coef, 12, &its, &ok);
-      if (!ok || !isfinite(xn)) xn = newton_rs(asinh(es * Rn / (2.0 * 1e-6)), st, ra, Vtn, coef, 100, &its2, &ok);
+      features(lnV, fin);
+      float res;
+      if (warp_full) {
+        __syncwarp();
+        res = mlp_residual_warp(snet, fin);
+      } else {
+        res = mlp_residual(snet, fin);
+      }
+      const double e = 2e-6 / es;
+      double x = guess_base(lnV, psi_a) + (double)res;
+      its = 0;
+      for (int c = 0; c < 2 && !accepted; c++) {
+        const double em = expm1(x), r = 1.0 / (1.0 + em);
+        const double sh = 0.5 * (em + em * r), ch = sh + r;
+        const double rfp = 1.0 / (e * ch + coef + 1e-100);
+        const double dd = -(e * sh + coef * x - Vtn) * rfp;
+        const double bound = e * (fabs(sh) + 2.0 * fabs(dd) * ch) * dd * dd * rfp;
+        its++;
+        x += dd;
+        if (!isfinite(x)) break;
+        accepted = fabs(dd) <= 1e-2 * (1.0 + fabs(x)) && bound <= a.guess_tol * fabs(x);
+      }
+      if (accepted) {
+        xn = x;
+        ok = true;
+      } else {
+        xn = newton_rs(asinh(es * Rn / (2.0 * 1e-6)), st, ra, Vtn, coef, 100, &its2, &ok);
+      }
+      if (a.judge) {
+        // the plain solve as the judge of the accepted value (a measurement aid)
+        int itj;
+        bool okj;
+        const double xp = newton_rs(asinh(es * Rn / (2.0 * 1e-6)), st, ra, Vtn, coef, 100, &itj, &okj);
+        const float rel = (float)(fabs(xn - xp) / fmax(fabs(xp), 1e-300));
+        atomicMax(reinterpret_cast<unsigned*>(a.newton + 6), __float_as_uint(rel));
+      }
     } else {
       xn = newton_rs(asinh(es * Rn / (2.0 * 1e-6)), st, ra, Vtn, coef, 100, &its, &ok);
       if (a.rec && ok && ((unsigned)q2 * 7919u + (unsigned)it * 4u + (unsigned)a.irk) % (unsigned)a.rec_every == 0) {
         // training sample: inputs and the residual target of the converged solve
         unsigned slot = atomicAdd(a.rec_n, 1u);
         if (slot < (unsigned)a.rec_cap) {
+          const double lnV = log(fmax(Vtn, 1e-300));
           float fin[4];
-          features(fin);
+          features(lnV, fin);
           float* o = a.rec + 5ull * slot;
           o[0] = fin[0]; o[1] = fin[1]; o[2] = fin[2]; o[3] = fin[3];
-          o[4] = (float)(xn - asinh(Vtn * es / (2.0 * 1e-6)));
+          o[4] = (float)(xn - guess_base(lnV, psi_a));
         }
       }
     }
     {
-      // Newton statistics, one atomic per warp
+      // Newton statistics, one atomic per warp: iterations, capped solves, accepted learned
+      // guesses, learned guesses that fell back, and with solve timing on the clock cycles
+      // of the solve (guess, network, Newton) and the solves timed
       const unsigned m = __activemask();
       const unsigned sum_it = __reduce_add_sync(m, (unsigned)(its + its2));
       const unsigned n_bad = __reduce_add_sync(m, ok ? 0u : 1u);
+      const unsigned n_acc = __reduce_add_sync(m, accepted ? 1u : 0u);
+      const unsigned n_all = __popc(m);
+      const unsigned cyc = a.prof ? __reduce_add_sync(m, (unsigned)(clock64() - clk0)) : 0u;
       if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == __ffs(m) - 1) {
         atomicAdd(a.newton, (unsigned long long)sum_it);
         if (n_bad) atomicAdd(a.newton + 1, (unsigned long long)n_bad);
+        if (a.rs_guess && a.guess_net) {
+          atomicAdd(a.newton + 2, (unsigned long long)n_acc);
+          atomicAdd(a.newton + 3, (unsigned long long)(n_all - n_acc));
+        }
+        if (a.prof) {
+          atomicAdd(a.newton + 4, (unsigned long long)cyc);
+          atomicAdd(a.newton + 5, (unsigned long long)n_all);
+        }
       }
     }
     double V = 2.0 * 1e-6 * exp(-st / ra) * sinh(xn);
@@ -877,7 +903,7 @@ __device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int 
 template <int FY, int FZ>
 __global__ void __launch_bounds__(128) fault_node_kernel(const __grid_constant__ FaultArgs a) {
   __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
-  fault_node_body<FY, FZ>(a, blockIdx.x, blockIdx.y, snet);
+  fault_node_body<FY, FZ>(a, blockIdx.x, snet);
 }
 // grid z: the part (six off-fault layers, then the split nodes), so that the seven
 // independent pieces of a fault column run in parallel.  At most 128 registers (four
@@ -900,9 +926,7 @@ __global__ void __launch_bounds__(128) fault_node_batch(const FaultArgs* __restr
   const int sc = scenario_of(start, n, blockIdx.x, &loc);
   stage_args(sa, tab + sc);
   __syncthreads();
-  const FaultArgs& a = *sa;
-  const int gx = (a.d.nj + 31) / 32;
-  fault_node_body<FY, FZ>(a, loc % gx, loc / gx, snet);
+  fault_node_body<FY, FZ>(*sa, loc, snet);
 }
 template <int FX, int FY, int FZ>
 __global__ void __launch_bounds__(128, 4) fault_band_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
@@ -1119,8 +1143,8 @@ void launch_rup_sensor(const SensorArgs& a, cudaStream_t s) {
 }
 
 void launch_fault_node(const FaultArgs& a, cudaStream_t s) {
-  dim3 block(32, 4, 1);
-  dim3 grid((a.d.nj + 31) / 32, (a.d.nk + 3) / 4, 1);
+  dim3 block(128, 1, 1);
+  dim3 grid(node_blocks(a.NY, a.NZ, a.freenode), 1, 1);
   int code = (a.FY > 0) * 2 + (a.FZ > 0);
   switch (code) {
     case 0: fault_node_kernel<-1, -1><<<grid, block, 0, s>>>(a); break;
@@ -1150,7 +1174,7 @@ void launch_fault_band(const FaultArgs& a, cudaStream_t s) {
 // FX, FY, FZ are the ensemble's (every scenario is at the same step and stage)
 void launch_fault_node_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FY, int FZ,
                              cudaStream_t s) {
-  dim3 block(32, 4, 1);
+  dim3 block(128, 1, 1);
   int code = (FY > 0) * 2 + (FZ > 0);
   switch (code) {
     case 0: fault_node_batch<-1, -1><<<blocks, block, 0, s>>>(tab, start, n); break;

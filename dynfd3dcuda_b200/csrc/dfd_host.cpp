@@ -114,6 +114,7 @@ void params_default(dfd_params* p) {
   p->rupture = 1; p->free_surface = 1; p->use_pml = 1; p->use_cerjan = 0; p->normal_refine = 1;
   p->rs_guess = 0;
   p->TP_n = 1;  // set_params.cu:103
+  p->rs_guess_tol = 1e-10;
   finalize_params(p);
 }
 
@@ -190,6 +191,7 @@ int params_from_json(const char* text, dfd_params* p, std::string* err) {
     else if (k == "useCerjan") inum(p->use_cerjan);
     else if (k == "NormalRefine") inum(p->normal_refine);
     else if (k == "RS_guess") inum(p->rs_guess);
+    else if (k == "RS_guess_tol") num(p->rs_guess_tol);
     else if (k == "TP_n") inum(p->TP_n);  // set_params.cu:281-282
     // PX/PY/PZ, igpu, vp1/vs1, RupThres, smoothing keys: accepted, not used on one GPU
   }
@@ -215,6 +217,7 @@ int check_params(const dfd_params* p, std::string* err) {
     return fail("PML_N > 30 overlaps the fault band (non-united fault nodes start 31 nodes in)");
   if (p->use_cerjan && (2 * p->DAMP_N > p->NX || 2 * p->DAMP_N > p->NY || 2 * p->DAMP_N > p->NZ))
     return fail("DAMP_N too large for the grid");
+  if (!(p->rs_guess_tol >= 0.0 && p->rs_guess_tol < 1.0)) return fail("RS_guess_tol must lie in [0, 1)");
   if (p->EXPORT_TIME_SKIP < 1) return fail("EXPORT_TIME_SKIP must be >= 1");
   return DFD_OK;
 }

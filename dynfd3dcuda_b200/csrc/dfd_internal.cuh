@@ -160,7 +160,14 @@ struct FaultArgs {
   float *init_t0, *friction;
   int *init_t0_flag, *flag_rup;
   const int *united, *faultgrid, *rupy, *rupz;
-  unsigned long long* newton;      // [0] iterations, [1] capped solves
+  // [0] Newton iterations, [1] capped solves, [2] accepted learned guesses, [3] learned
+  // guesses that fell back to the plain solve, [4] clock cycles of timed solves, [5] solves
+  // timed, [6] largest relative difference of an accepted value from the plain solve (float
+  // bits, judge mode), [7] unused
+  unsigned long long* newton;
+  int prof;                        // time the rate-and-state solve section (clock64)
+  int judge;                       // also run the plain solve after a learned one and compare
+  double guess_tol;                // residual test of the learned guess: error bound <= guess_tol |x|
   const int* it_dev;               // current step index (device copy, advanced inside graphs)
   const float* guess_net;          // learned-guess MLP weights or null
   float* rec;                      // Newton sample recording buffer (cap x 5) or null
@@ -172,6 +179,29 @@ struct FaultArgs {
   double dDT, smooth_load_T, f0, V0, fw, Vini;
   int it, irk, FX, FY, FZ, freenode, friction_type, inport_stress, NY, NZ, rs_guess;
 };
+
+// The non-united fault nodes, where the fault node kernel works: the rectangle
+// 30 < j + 1 < NY - 30, k + 1 > 30 (and k + 1 < NZ - 30 without a free surface)
+// (init.cu:806-816).  The kernel numbers its nodes row by row over the rectangle, so that
+// every warp but the last holds 32 live nodes.
+struct NodeRect {
+  int j0, k0, w, h;
+  __host__ __device__ long long count() const { return (long long)w * h; }
+};
+__host__ __device__ inline NodeRect node_rect(int NY, int NZ, int freenode) {
+  NodeRect r;
+  r.j0 = 30;
+  r.k0 = 30;
+  r.w = NY - 61 > 0 ? NY - 61 : 0;
+  const int kh = freenode ? NZ : NZ - 31;
+  r.h = kh - 30 > 0 ? kh - 30 : 0;
+  return r;
+}
+// blocks of the fault node kernel (128 threads, one node each; at least one)
+inline int node_blocks(int NY, int NZ, int freenode) {
+  const long long c = node_rect(NY, NZ, freenode).count();
+  return c > 0 ? (int)((c + 127) / 128) : 1;
+}
 
 // Separable grid description for the FP64 metric kernel (dfd_setup.cu).
 struct GridArgs {

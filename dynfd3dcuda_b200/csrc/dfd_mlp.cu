@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/dfd_b200.h"
+#include "dfd_mlp.cuh"
 
 namespace dfd {
 namespace mlp {
@@ -68,6 +69,19 @@ __global__ void forward_kernel(const float* __restrict__ w, const float* __restr
   float h1[H], h2[H];
   float xin[4] = {X[4 * t], X[4 * t + 1], X[4 * t + 2], X[4 * t + 3]};
   y[t] = forward(sw, xin, h1, h2);  // standardised output
+}
+
+// The node kernel's inference paths on a batch (n a multiple of 32): tc 0 the per-thread
+// network, tc 1 the tensor-core network of a full warp; de-standardised residuals.
+__global__ void __launch_bounds__(128) forward_node_kernel(const float* __restrict__ w, const float* __restrict__ X,
+                                                            int n, int tc, float* y) {
+  __shared__ __align__(16) float sw[NPAR];
+  for (int p = threadIdx.x; p < NPAR; p += blockDim.x) sw[p] = w[p];
+  __syncthreads();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;  // n is a multiple of 32: warps stay whole
+  const float xin[4] = {X[4 * t], X[4 * t + 1], X[4 * t + 2], X[4 * t + 3]};
+  y[t] = tc ? mlp_residual_warp(sw, xin) : mlp_residual(sw, xin);
 }
 
 // Gradient of the mean squared error over n samples (sample s = idx[s0 + b] for b < nb)
@@ -224,6 +238,25 @@ int dfd_mlp_forward(const float* w, const float* x, int n, float* y) {
   MCK(cudaMemcpy(y, dy.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
   // de-standardise
   for (int i = 0; i < n; i++) y[i] = y[i] * w[OYSD] + w[OYMU];
+  return DFD_OK;
+}
+
+int dfd_mlp_forward_node(const float* w, const float* x, int n, int tensor_cores, float* y) {
+  if (!w || !x || !y || n <= 0) return DFD_ERR_PARAM;
+  const int np = (n + 31) / 32 * 32;  // whole warps: the rows past n repeat the last input
+  std::vector<float> xp(4 * (size_t)np);
+  memcpy(xp.data(), x, sizeof(float) * 4 * (size_t)n);
+  for (int i = n; i < np; i++) memcpy(&xp[4 * (size_t)i], x + 4 * (size_t)(n - 1), 4 * sizeof(float));
+  DevBuf dw, dx, dy;
+  MCK(cudaMalloc(&dw.p, sizeof(float) * NPAR));
+  MCK(cudaMalloc(&dx.p, sizeof(float) * 4 * (size_t)np));
+  MCK(cudaMalloc(&dy.p, sizeof(float) * (size_t)np));
+  MCK(cudaMemcpy(dw.p, w, sizeof(float) * NPAR, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(dx.p, xp.data(), sizeof(float) * 4 * (size_t)np, cudaMemcpyHostToDevice));
+  forward_node_kernel<<<(np + 127) / 128, 128>>>(dw.get<float>(), dx.get<float>(), np, tensor_cores ? 1 : 0,
+                                                 dy.get<float>());
+  MCK(cudaGetLastError());
+  MCK(cudaMemcpy(y, dy.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
   return DFD_OK;
 }
 

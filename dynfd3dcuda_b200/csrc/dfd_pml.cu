@@ -91,7 +91,7 @@ __device__ __forceinline__ PmlUnit pml_unit(const TileSched& sc, const VolArgs& 
 }
 
 // ADE update of face `face` for fields F0..F0+2 at this node (pml_update of
-// dfd_stencil.cuh, restricted to three fields): accumulates -aux/beta into p and advances
+// dfd_stencil.cuh, restricted to three fields): adds -aux/beta to the rates p and advances
 // the state in place with the RK4 registers.  The state comes from shared memory (A, the
 // staged own face) or from global memory; every load precedes the stores, which may alias
 // them as far as the compiler knows.
@@ -200,15 +200,20 @@ __device__ __forceinline__ float d5r(const float* p, int S) {
   else return d5v<-1>(p[-3 * S], p[-2 * S], p[-S], p[0], p[S]);
 }
 
+// the y and z PML factors of a node (1/beta, d, alpha): fixed over a unit, loaded once per
+// unit so that no global load waits inside the plane loop
+struct YZFactors {
+  float rby, ddy, aly, rbz, ddz, alz;
+};
+
 template <int FX, int FY, int FZ>
 __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* x0, const float* x1, const float* x2,
                                          const float* x3, const float* x4, const float* cur, const NodeMetric& g,
                                          int i, int j, int k, int fx, int fy, int fz, int own, const float* A,
-                                         long long q, const float* P, float damp, float rbx, float ddx, float alx) {
+                                         long long q, const float* P, float damp, float rbx, float ddx, float alx,
+                                         const YZFactors& yz) {
   const float r = a.rDH;
-  float hv[9], p[9], D[9], dv[9];
-#pragma unroll
-  for (int f = 0; f < 9; f++) p[f] = 0.0f;
+  float hv[9], D[9], dv[9];
   // x
   {
 #pragma unroll
@@ -225,9 +230,9 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
     if (fx >= 0) {
       const bool st = fx == own;
       const float dd = ddx, al = alx;
-      role_face<0, 0>(a, fx, st, A, i, j, k, rb, dd, al, D, p);
-      role_face<3, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 3, p + 3);
-      role_face<6, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 6, p + 6);
+      role_face<0, 0>(a, fx, st, A, i, j, k, rb, dd, al, D, hv + 0);
+      role_face<3, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
+      role_face<6, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
     }
   }
   // y
@@ -237,15 +242,15 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
     role_terms<0, false>(dv + 3, 0.0f, g.ey1, g.ey2, g.lam, g.mu, g.rrho, D);
     role_terms<3, false>(dv, 0.0f, g.ey1, g.ey2, g.lam, g.mu, g.rrho, D + 3);
     role_terms<6, false>(dv, 0.0f, g.ey1, g.ey2, g.lam, g.mu, g.rrho, D + 6);
-    const float rb = __ldg(a.rBy + j);
+    const float rb = yz.rby;
 #pragma unroll
     for (int f = 0; f < 9; f++) hv[f] += D[f] * rb;
     if (fy >= 0) {
       const bool st = fy == own;
-      const float dd = __ldg(a.Dpy + j), al = __ldg(a.Apy + j);
-      role_face<0, 1>(a, fy, st, A, i, j, k, rb, dd, al, D, p);
-      role_face<3, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 3, p + 3);
-      role_face<6, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 6, p + 6);
+      const float dd = yz.ddy, al = yz.aly;
+      role_face<0, 1>(a, fy, st, A, i, j, k, rb, dd, al, D, hv + 0);
+      role_face<3, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
+      role_face<6, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
     }
   }
   // z
@@ -255,19 +260,17 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
     role_terms<0, false>(dv + 3, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D);
     role_terms<3, false>(dv, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D + 3);
     role_terms<6, false>(dv, 0.0f, g.ez1, g.ez2, g.lam, g.mu, g.rrho, D + 6);
-    const float rb = __ldg(a.rBz + k);
+    const float rb = yz.rbz;
 #pragma unroll
     for (int f = 0; f < 9; f++) hv[f] += D[f] * rb;
     if (fz >= 0) {
       const bool st = fz == own;
-      const float dd = __ldg(a.Dpz + k), al = __ldg(a.Apz + k);
-      role_face<0, 2>(a, fz, st, A, i, j, k, rb, dd, al, D, p);
-      role_face<3, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 3, p + 3);
-      role_face<6, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 6, p + 6);
+      const float dd = yz.ddz, al = yz.alz;
+      role_face<0, 2>(a, fz, st, A, i, j, k, rb, dd, al, D, hv + 0);
+      role_face<3, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
+      role_face<6, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
     }
   }
-#pragma unroll
-  for (int f = 0; f < 9; f++) hv[f] += p[f];
   rk_tile_store<0, 9>(a, a.d.nxyz, q, cur, P, hv, damp);
 }
 
@@ -424,6 +427,13 @@ __global__ void __maxnreg__(168)
     const int fz = (a.aux[4] && k < d.N) ? 4 : (a.aux[5] && k >= d.nk - d.N) ? 5 : -1;
     float dyz = 1.0f;
     if (active && a.dampx) dyz = fminf(__ldg(a.dampy + j + 3), __ldg(a.dampz + k + 3));
+    YZFactors yz = {1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f};
+    if (active) {
+      yz.rby = __ldg(a.rBy + j);
+      yz.rbz = __ldg(a.rBz + k);
+      if (fy >= 0) { yz.ddy = __ldg(a.Dpy + j); yz.aly = __ldg(a.Apy + j); }
+      if (fz >= 0) { yz.ddz = __ldg(a.Dpz + k); yz.alz = __ldg(a.Apz + k); }
+    }
     const long long qyz = idx3(d, 0, j + 3, k + 3);
     const int nst = pu.ie - pu.ib;
     const bool usep = needW0 || needT || pu.face >= 0;
@@ -477,7 +487,7 @@ __global__ void __maxnreg__(168)
         if (pu.strip || pml) {
           // (strips hold y-slab nodes and the few interior columns beside them)
           pml_node<FX, FY, FZ>(a, pu.strip ? STRIP + 8 : HW, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face,
-                               P + 18 * PB, q, P, damp, rbx, ddx, alx);
+                               P + 18 * PB, q, P, damp, rbx, ddx, alx, yz);
         } else {
           float hv[9];
           lean_velocity<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);

@@ -60,6 +60,11 @@ typedef struct dfd_params {
   /* points across the fault of each thermal-pressurisation column (Friction_type 3);
    * the reference's default is 1, which Friction_type 3 rejects (see dfd_load_tp_hy) */
   int TP_n;
+  /* residual test of the learned guess (rs_guess 1): after each of at most two Newton
+   * corrections from the guess, the corrected guess is accepted when the bound on its
+   * remaining error (quadratic convergence) is at most rs_guess_tol |x|; default 1e-10,
+   * which keeps the slip rate within FP32 rounding of the plain solve's */
+  double rs_guess_tol;
 } dfd_params;
 
 typedef struct dfd_ctx dfd_ctx;
@@ -230,6 +235,16 @@ int dfd_set_guess_net(dfd_ctx *ctx, const float *weights, int n);
  * Newton solves (chosen by node, step and stage) into a device buffer of `capacity`
  * samples (0 frees it); solves beyond the capacity are dropped */
 int dfd_newton_record(dfd_ctx *ctx, int capacity, int every);
+/* measurement aids of the rate-and-state solve: timing 1 accumulates the clock cycles of
+ * the solve section (guess, network and Newton iterations) per node; judge 1 also runs the
+ * plain solve after every learned one and keeps the largest relative difference of the
+ * accepted values from it.  Both off by default. */
+int dfd_rs_profile(dfd_ctx *ctx, int timing, int judge);
+/* since the last dfd_precompute: learned guesses accepted by the residual test and those
+ * that fell back to the plain solve, mean clock cycles of a timed solve (0 without
+ * timing), and the judge's largest relative difference (0 without judge) */
+int dfd_rs_solve_stats(dfd_ctx *ctx, long long *accepted, long long *fallback, double *cycles_per_solve,
+                       double *judge_max_rel);
 /* copy up to max recorded samples (5 floats each) to host, set *n, and empty the buffer */
 int dfd_newton_samples(dfd_ctx *ctx, float *host, int max, int *n);
 /* stand-alone training and inference on the current device, host arrays in and out:
@@ -238,6 +253,10 @@ int dfd_newton_samples(dfd_ctx *ctx, float *host, int max, int *n);
  * (DFD_MLP_TRAINABLE floats), and minibatch Adam training for `epochs` epochs */
 int dfd_mlp_init(float *w, unsigned seed, const float *x_mean, const float *x_scale, float y_mean, float y_scale);
 int dfd_mlp_forward(const float *w, const float *x, int n, float *y);
+/* the fault node kernel's own inference of the residual on a batch: tensor_cores 0 the
+ * per-thread network (hardware tanh), 1 the warp-wide network whose hidden layer runs on
+ * the tensor cores (mma.sync, FP16 operands, FP32 accumulation) */
+int dfd_mlp_forward_node(const float *w, const float *x, int n, int tensor_cores, float *y);
 int dfd_mlp_loss_grad(const float *w, const float *x, const float *y, int n, double *loss, float *grad);
 int dfd_mlp_train(const float *x, const float *y, int n, int epochs, int batch, float lr, unsigned seed, float *w,
                   float *loss_per_epoch);
