@@ -236,7 +236,7 @@ def lib():
             "dfd_ens_create": [V, I, P(ctypes.c_void_p)], "dfd_ens_destroy": [V], "dfd_ens_run": [V, I, I],
             "dfd_ens_synchronize": [V], "dfd_ens_run_timed": [V, I, I, P(ctypes.c_float)],
             "dfd_ens_set_chunk": [V, I], "dfd_ens_nodes": [V, P(ctypes.c_longlong)],
-            "dfd_newton_record": [V, I, I], "dfd_rs_profile": [V, I, I],
+            "dfd_newton_record": [V, I, I], "dfd_rs_profile": [V, I, I], "dfd_test_wait_drill": [V, I],
             "dfd_rs_solve_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong), P(ctypes.c_double),
                                    P(ctypes.c_double)], "dfd_fault_node_ms": [V, P(ctypes.c_float)], "dfd_newton_samples": [V, V, I, P(ctypes.c_int)],
             "dfd_mlp_init": [V, ctypes.c_uint, V, V, ctypes.c_float, ctypes.c_float],
@@ -412,6 +412,10 @@ class Simulation:
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(lib().dfd_newton_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def test_wait_drill(self, on=True):
+        """Test hook: the interior kernel issues no copies, so its bounded waits run out."""
+        self._check(lib().dfd_test_wait_drill(self.h, int(on)))
 
     def rs_profile(self, timing=True, judge=False):
         """Switch the rate-and-state solve measurement aids (solve timing, plain-solve judge)."""

@@ -1161,6 +1161,17 @@ int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {
   return DFD_OK;
 }
 
+int dfd_test_wait_drill(dfd_ctx* ctx, int on) {
+  if (!ctx) return DFD_ERR_PARAM;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  ctx->tile.drill = on ? 1 : 0;
+  // the switch is baked into the step graphs: rebuild them
+  for (auto& g : ctx->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return DFD_OK;
+}
+
 int dfd_rs_profile(dfd_ctx* ctx, int timing, int judge) {
   if (!ctx) return DFD_ERR_PARAM;
   cudaSetDevice(ctx->device);

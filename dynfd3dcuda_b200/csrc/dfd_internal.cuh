@@ -242,6 +242,7 @@ struct TileCtx {
   int* err = nullptr;
   int* sched = nullptr;  // unit counter and finished-CTA counter (zero between launches)
   int nsm = 0;
+  int drill = 0;         // test drill of the bounded waits (TileSched::drill), off by default
   bool ok = false;
 };
 bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, float* const aux[6], int* err,
@@ -263,6 +264,8 @@ struct TileSched {
   int nx1, nx2, ktop, nedge;              // PML kernel: x slab widths, top row bound, edge tiles
   int ya, yb, za, zb;                     // PML kernel: the interior box in y and z
   int ny1, ny2, nrs, ntz, nz1, nz2;       // PML kernel: edge tile counts
+  int drill;  // interior kernel, test drill: the copy warp issues no copies, so the computing
+              // warps' first wait runs out (after DRILL_LIMIT polls) and sets the error flag
 };
 // Values of one scenario of a batched (ensemble) launch of the tiled kernel that the
 // computing warps read; a CTA copies them into shared memory with each unit's planes.

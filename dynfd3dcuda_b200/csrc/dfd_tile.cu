@@ -89,8 +89,10 @@ __global__ void __maxnreg__(96)
     int wcount = 0, pcount = 0, qcount = 0;
     bool ok = true;
     // units are taken from a global counter, so that CTAs that start late (their SM busy
-    // with a concurrent kernel) simply take fewer
-    while (ok) {
+    // with a concurrent kernel) simply take fewer.  In the test drill of the bounded waits
+    // this warp takes no unit and issues nothing: no copy is ever in flight, and the
+    // computing warps' first wait runs out.
+    while (ok && !sc0.drill) {
       const int u = atomicAdd(sched, 1);
       if (qcount >= NQ && !(ok = mbar_wait(empty_q + qr.slot, qr.phase ^ 1))) break;
       if (u >= nunits) {
@@ -168,7 +170,7 @@ __global__ void __maxnreg__(96)
   Ring wr, pr, qr;  // next stencil plane to wait for; RK-register slot of the step; unit planes
   int sb = 0;       // slot of the step's first stencil plane
   for (;;) {
-    if (!__all_sync(0xffffffffu, mbar_wait(full_q + qr.slot, qr.phase))) {
+    if (!__all_sync(0xffffffffu, mbar_wait_n(full_q + qr.slot, qr.phase, sc0.drill ? DRILL_LIMIT : WAIT_LIMIT))) {
       if (lane == 0) atomicExch(err, 1);
       return;
     }
@@ -404,6 +406,7 @@ static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3
   const TileMaps mp = tile_maps(tc, bin);
   int grid = 0;
   TileSched sc = tile_plan(lo, hi, tc.nsm, &grid);
+  sc.drill = tc.drill;
   volume_tile_kernel<FX, FY, FZ, false>
       <<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, nullptr, 1, sc.nunits, tc.err, tc.sched);
 }

@@ -24,6 +24,7 @@ constexpr int QSLOT = 12 * PB;       // metric / media planes of a unit: U V ety
 constexpr int NCW = 2 * NTHR / 32;   // computing warps: two per 32-node row of the tile
 constexpr int NTOT = NCW * 32 + 32;  // plus one copy-issuing warp
 constexpr long long WAIT_LIMIT = 1LL << 22;  // polls of one mbarrier before giving up
+constexpr long long DRILL_LIMIT = 1LL << 12; // the same in the test drill of the bounded waits
 static_assert((HSLOT * 4) % 128 == 0 && (QSLOT * 4) % 128 == 0 && (PB * 4) % 128 == 0, "slot alignment");
 static_assert(sizeof(TileUnit) % 16 == 0 && offsetof(TileScen, u) % 16 == 0, "bulk copy of the scenario values");
 }  // namespace
@@ -49,11 +50,12 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, unsigned parity) {
   return ok != 0;
 }
 // bounded wait for the completion of phase `parity`; false if it did not complete
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
-  for (long long n = 0; n < WAIT_LIMIT; n++)
+__device__ __forceinline__ bool mbar_wait_n(uint64_t* b, unsigned parity, long long limit) {
+  for (long long n = 0; n < limit; n++)
     if (mbar_try(b, parity)) return true;
   return false;
 }
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) { return mbar_wait_n(b, parity, WAIT_LIMIT); }
 __device__ __forceinline__ void tma_load4(float* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                           uint64_t* b) {
   asm volatile(

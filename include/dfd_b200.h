@@ -202,6 +202,13 @@ int dfd_fault_node_ms(dfd_ctx *ctx, float *ms);
  * module is loaded, whether or not this entry is called. */
 #define DFD_SLICE_SCRATCH_FLOATS (1 << 22)
 int dfd_get_slice_noalloc(dfd_ctx *ctx, int axis, int index, float *host);
+/* Test hook of the bounded waits (no counterpart in the reference; off by default): with
+ * on = 1 the interior (TMA-tiled) kernel's copy-issuing warp issues no copies, so the
+ * computing warps' first wait on a copy runs out after a short bounded poll; they set the
+ * context's error flag and return.  The next dfd_synchronize reports DFD_ERR_CUDA ("a TMA
+ * copy did not complete"), which stays sticky in this context; the device and other
+ * contexts are unaffected.  Exercises the timeout path without faulting the GPU. */
+int dfd_test_wait_drill(dfd_ctx *ctx, int on);
 /* host-side health check: 0 ok, DFD_ERR_NONFINITE if the fault state holds NaN/Inf */
 int dfd_check_finite(dfd_ctx *ctx);
 /* cumulative Newton iterations and non-converged solves of the rate-and-state trial */
