@@ -24,6 +24,8 @@ _lib = None
 
 FIELDS = ["slip", "hslip", "Vs1", "Vs2", "Tn", "Ts1", "Ts2", "State", "init_t0", "tTn", "tTs1", "tTs2",
           "str_peak", "friction", "united", "faultgrid", "split", "T1", "hT1", "TP_T", "TP_P", "rup_sensor"]
+HALO_SETUP = 4  # dfd_halo_pack / dfd_halo_unpack: the metric and media of the ghost columns
+
 # coefficient tables of dfd_get_fault_table, in the order of the DFD_TAB_* names
 TABLES = ["D21_1", "D22_1", "D23_1", "D31_1", "D32_1", "D33_1", "D21_2", "D22_2", "D23_2", "D31_2", "D32_2", "D33_2",
           "matMin2Plus1", "matMin2Plus2", "matMin2Plus3", "matMin2Plus4", "matMin2Plus5",
@@ -199,7 +201,7 @@ class DfdParams(ctypes.Structure):
         ("use_cerjan", ctypes.c_int), ("normal_refine", ctypes.c_int), ("rs_guess", ctypes.c_int),
         ("OUT", ctypes.c_char * 1024), ("Fault_geometry", ctypes.c_char * 1024),
         ("Fault_init_stress", ctypes.c_char * 1024), ("Media1D", ctypes.c_char * 1024),
-        ("TP_n", ctypes.c_int), ("rs_guess_tol", ctypes.c_double),
+        ("TP_n", ctypes.c_int), ("rs_guess_tol", ctypes.c_double), ("PY", ctypes.c_int), ("rank_y", ctypes.c_int),
     ]
 
 
@@ -237,6 +239,7 @@ def lib():
             "dfd_ens_synchronize": [V], "dfd_ens_run_timed": [V, I, I, P(ctypes.c_float)],
             "dfd_ens_set_chunk": [V, I], "dfd_ens_nodes": [V, P(ctypes.c_longlong)],
             "dfd_newton_record": [V, I, I], "dfd_rs_profile": [V, I, I], "dfd_test_wait_drill": [V, I],
+            "dfd_halo_floats": [V, P(ctypes.c_longlong)], "dfd_halo_pack": [V, I, I, V], "dfd_halo_unpack": [V, I, I, V],
             "dfd_rs_solve_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong), P(ctypes.c_double),
                                    P(ctypes.c_double)], "dfd_fault_node_ms": [V, P(ctypes.c_float)], "dfd_newton_samples": [V, V, I, P(ctypes.c_int)],
             "dfd_mlp_init": [V, ctypes.c_uint, V, V, ctypes.c_float, ctypes.c_float],
@@ -293,7 +296,8 @@ class Simulation:
         nx, ny, nz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         L.dfd_dims(self.h, ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz))
         self.nx, self.ny, self.nz = nx.value, ny.value, nz.value
-        self.NX, self.NY, self.NZ = self.p.NX, self.p.NY, self.p.NZ
+        # NY: the columns this context holds (NY / PY for a slab of a decomposed domain)
+        self.NX, self.NY, self.NZ = self.p.NX, self.ny - 6, self.p.NZ
         if fxyz is not None:
             a = np.ascontiguousarray(fxyz, np.float32)
             self._check(L.dfd_load_fault_geometry(self.h, a.ctypes.data))
@@ -412,6 +416,21 @@ class Simulation:
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(lib().dfd_newton_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def halo_floats(self):
+        """Floats of one halo message (dfd_halo_floats)."""
+        n = ctypes.c_longlong()
+        self._check(lib().dfd_halo_floats(self.h, ctypes.byref(n)))
+        return n.value
+
+    def halo_pack(self, what, side, device_ptr):
+        """Gather the leaving columns of side 0 (low y) or 1 (high y) into device memory;
+        what = 0..3 (the input of that RK stage) or HALO_SETUP."""
+        self._check(lib().dfd_halo_pack(self.h, what, side, device_ptr))
+
+    def halo_unpack(self, what, side, device_ptr):
+        """Scatter a neighbour's message into the ghost columns of side 0 or 1."""
+        self._check(lib().dfd_halo_unpack(self.h, what, side, device_ptr))
 
     def test_wait_drill(self, on=True):
         """Test hook: the interior kernel issues no copies, so its bounded waits run out."""

@@ -50,6 +50,31 @@ __global__ void slice_kernel(Dims d, const float* W, int axis, int index, float*
   long long q = idx3(d, i + 3, j + 3, k + 3);
   for (int c = 0; c < 3; c++) out[(long long)c * na * nb + t] = W[c * d.nxyz + q];
 }
+
+// Halo message of a slab (domain decomposed along y): three columns starting at padded
+// column jp of nvf volume fields (layout (f, x, z, y), pitched rows) and of nff fault
+// planes (layout (f, z, y)), in the order ((f, x, z), column) then ((f, z), column).
+// unpack = 0 gathers them into buf, unpack = 1 scatters buf into them.
+__global__ void halo_kernel(Dims d, float* vol, int nvf, float* fw, int nff, int jp, float* buf, int unpack) {
+  const long long nv = (long long)nvf * d.nx * d.nz * 3, nt = nv + (long long)nff * d.nz * 3;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nt; t += (long long)gridDim.x * blockDim.x) {
+    float* p;
+    if (t < nv) {
+      const int c = (int)(t % 3);
+      const long long r = t / 3;  // (f, x, z)
+      const int k = (int)(r % d.nz), i = (int)((r / d.nz) % d.nx), f = (int)(r / ((long long)d.nz * d.nx));
+      p = vol + f * d.nxyz + (jp + c + d.oy) + (long long)k * d.py + (long long)i * d.sx;
+    } else {
+      const long long u = t - nv;
+      const int c = (int)(u % 3);
+      const long long r = u / 3;  // (f, z)
+      const int k = (int)(r % d.nz), f = (int)(r / d.nz);
+      p = fw + f * d.nyz + (jp + c) + (long long)k * d.ny;
+    }
+    if (unpack) *p = buf[t];
+    else buf[t] = *p;
+  }
+}
 }  // namespace dfd
 
 using namespace dfd;
@@ -239,8 +264,9 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return DFD_ERR_CUDA; }
   Dims& d = ctx->d;
-  d.ni = q.NX; d.nj = q.NY; d.nk = q.NZ;
-  d.nx = q.NX + 6; d.ny = q.NY + 6; d.nz = q.NZ + 6;
+  // a slab of a domain decomposed along y holds NY / PY columns (PY 1: the whole domain)
+  d.ni = q.NX; d.nj = q.NY / q.PY; d.nk = q.NZ;
+  d.nx = q.NX + 6; d.ny = d.nj + 6; d.nz = q.NZ + 6;
   d.i0 = d.nx / 2;
   d.N = q.PML_N;
   // row offset 1: the first interior node (after 3 ghost nodes) of every row on a 16-byte
@@ -277,6 +303,8 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
     // one block of 27 fields per face: value, RK accumulator, step-start copy
     for (int f = 0; f < 6 && !rc; f++) {
       if (f == 5 && q.free_surface) continue;
+      // the y faces only on the slabs at the domain's y ends
+      if ((f == 2 && q.rank_y > 0) || (f == 3 && q.rank_y < q.PY - 1)) continue;
       const long long fs = pml_fstride(d, f);
       rc = dalloc(ctx, &ctx->aux[f][0], 27 * fs);
       if (!rc) {
@@ -418,6 +446,17 @@ int dfd_precompute(dfd_ctx* ctx) {
   // ---- grid, metric, media (FP64 on the GPU)
   x_line(&p, ctx->xl);
   surface(&p, ctx->fxyz.empty() ? nullptr : ctx->fxyz.data(), ctx->fx, ctx->fy, ctx->fz);
+  if (p.PY > 1) {
+    // this slab's columns of the domain's extended surface, its ghost columns included:
+    // the neighbours' coordinates inside the domain, the extrapolated ones at its ends
+    const int nyg = p.NY + 6, j0 = p.rank_y * d.nj;
+    for (auto* v : {&ctx->fx, &ctx->fy, &ctx->fz}) {
+      std::vector<double> loc((size_t)d.ny * d.nz);
+      for (int k = 0; k < d.nz; k++)
+        for (int j = 0; j < d.ny; j++) loc[j + (size_t)k * d.ny] = (*v)[j0 + j + (size_t)k * nyg];
+      v->swap(loc);
+    }
+  }
   double *dxl, *dfx, *dfy, *dfz;
   float* dlay = nullptr;
   CK(cudaMalloc(&dxl, sizeof(double) * ctx->xl.size()));
@@ -470,9 +509,10 @@ int dfd_precompute(dfd_ctx* ctx) {
   // ---- PML 1-D profiles
   bool fs = p.free_surface != 0;
   int len[3] = {d.ni, d.nj, d.nk};
+  const bool ylo = p.rank_y == 0, yhi = p.rank_y == p.PY - 1;  // the slab holds a y end
   for (int a = 0; a < 3; a++) {
     std::vector<float> A, B, D, rb;
-    bool lo = p.use_pml != 0, hi = p.use_pml && !(a == 2 && fs);
+    bool lo = p.use_pml && !(a == 1 && !ylo), hi = p.use_pml && !(a == 2 && fs) && !(a == 1 && !yhi);
     pml_profile(&p, len[a], lo, hi, A, B, D);
     rb.resize(B.size());
     for (size_t i = 0; i < B.size(); i++) rb[i] = 1.0f / B[i];
@@ -485,7 +525,7 @@ int dfd_precompute(dfd_ctx* ctx) {
     int np[3] = {d.nx, d.ny, d.nz};
     for (int a = 0; a < 3; a++) {
       std::vector<float> prof;
-      cerjan_profile(&p, np[a], true, !(a == 2 && fs), prof);
+      cerjan_profile(&p, np[a], !(a == 1 && !ylo), !(a == 2 && fs) && !(a == 1 && !yhi), prof);
       CK(cudaMemcpy(ctx->damp[a], prof.data(), sizeof(float) * prof.size(), cudaMemcpyHostToDevice));
     }
   }
@@ -516,8 +556,14 @@ int dfd_precompute(dfd_ctx* ctx) {
       // zero columns (alloc.cu:117-118); the diffusivity from dfd_load_tp_hy, else zero
       CK(cudaMemsetAsync(ctx->tp_T, 0, sizeof(float) * p.TP_n * nf, s));
       CK(cudaMemsetAsync(ctx->tp_P, 0, sizeof(float) * p.TP_n * nf, s));
-      if (ctx->tp_hy_h.size() == nf)
-        CK(cudaMemcpyAsync(ctx->tp_hy, ctx->tp_hy_h.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
+      if (ctx->tp_hy_h.size() == (size_t)p.NY * d.nk) {
+        // this slab's columns of the (NZ, NY) plane
+        std::vector<float> hy(nf);
+        for (int k = 0; k < d.nk; k++)
+          for (int j = 0; j < d.nj; j++) hy[j + (size_t)k * d.nj] = ctx->tp_hy_h[p.rank_y * d.nj + j + (size_t)k * p.NY];
+        CK(cudaMemcpyAsync(ctx->tp_hy, hy.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+      }
       else
         CK(cudaMemsetAsync(ctx->tp_hy, 0, sizeof(float) * nf, s));
     }
@@ -606,7 +652,7 @@ static FaultArgs fault_args(dfd_ctx* ctx, int pattern, int irk) {
     fa.Vini = (double)(float)p.Vini;
     fa.irk = irk; fa.FX = FX; fa.FY = FY; fa.FZ = FZ;
     fa.freenode = p.free_surface; fa.friction_type = p.Friction_type; fa.inport_stress = p.INPORT_STRESS_TYPE;
-    fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess;
+    fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess; fa.jg0 = p.rank_y * d.nj;
     fa.prof = ctx->rs_prof; fa.judge = ctx->rs_judge; fa.guess_tol = p.rs_guess_tol;
   }
   (void)FX;
@@ -678,7 +724,11 @@ static SensorArgs sensor_args(dfd_ctx* ctx) {
   const int nf = ctx->d.nj * ctx->d.nk;
   SensorArgs a;
   a.nj = ctx->d.nj; a.nk = ctx->d.nk;
-  for (int i = 0; i < 4; i++) a.fg[i] = ctx->p.Fault_grid[i];
+  // a slab of a decomposed domain: the fault grid in its local columns, and no sensor where
+  // the second differences would reach past the slab (as the reference's per-rank sensor)
+  const int j0 = ctx->p.rank_y * ctx->d.nj;
+  for (int i = 0; i < 4; i++) a.fg[i] = ctx->p.Fault_grid[i] - (i < 2 ? j0 : 0);
+  a.slab = ctx->p.PY > 1;
   a.united = ctx->ipl + I_UNITED * nf;
   a.Ts1 = ctx->pl + (size_t)P_TS1 * nf;
   a.out = ctx->pl + (size_t)P_RUPS * nf;
@@ -1161,6 +1211,43 @@ int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {
   return DFD_OK;
 }
 
+// ---- halo exchange of a slab of a domain decomposed along y
+static long long halo_count(const dfd_ctx* ctx, int what) {
+  const Dims& d = ctx->d;
+  if (what == DFD_HALO_SETUP) return 13LL * 3 * d.nx * d.nz;
+  return 9LL * 3 * d.nx * d.nz + (ctx->p.rupture ? 18LL * 3 * d.nz : 0);
+}
+
+int dfd_halo_floats(dfd_ctx* ctx, long long* floats) {
+  if (!ctx || !floats) return DFD_ERR_PARAM;
+  *floats = std::max(halo_count(ctx, DFD_HALO_SETUP), halo_count(ctx, 0));
+  return DFD_OK;
+}
+
+static int halo_move(dfd_ctx* ctx, int what, int side, float* buf, int unpack) {
+  if (!ctx || !buf || side < 0 || side > 1 || what < 0 || what > DFD_HALO_SETUP) return DFD_ERR_PARAM;
+  if (ctx->sticky) return ctx->sticky;
+  if (!ctx->ready) return fail(ctx, DFD_ERR_STATE, "dfd_precompute has not run");
+  cudaSetDevice(ctx->device);
+  const Dims& d = ctx->d;
+  // leaving: the slab's first or last three columns; arriving: the ghost columns beside them
+  const int jp = unpack ? (side ? d.nj + 3 : 0) : (side ? d.nj : 3);
+  static const int bin[4] = {0, 1, 2, 1};  // stage inputs (the buffer cycle of the stages)
+  float* vol = what == DFD_HALO_SETUP ? ctx->M : ctx->W[bin[what]];
+  const int nvf = what == DFD_HALO_SETUP ? 13 : 9;
+  float* fw = what < DFD_HALO_SETUP && ctx->p.rupture ? ctx->FW[what % 2] : nullptr;
+  const int nff = fw ? 18 : 0;
+  const long long n = halo_count(ctx, what);
+  const int threads = 256;
+  const int blocks = (int)std::min<long long>((n + threads - 1) / threads, 148LL * 8);
+  dfd::halo_kernel<<<blocks, threads, 0, ctx->s0>>>(d, vol, nvf, fw, nff, jp, buf, unpack);
+  return cuda_check(ctx, cudaGetLastError(), "halo");
+}
+int dfd_halo_pack(dfd_ctx* ctx, int what, int side, float* buf) { return halo_move(ctx, what, side, buf, 0); }
+int dfd_halo_unpack(dfd_ctx* ctx, int what, int side, const float* buf) {
+  return halo_move(ctx, what, side, const_cast<float*>(buf), 1);
+}
+
 int dfd_test_wait_drill(dfd_ctx* ctx, int on) {
   if (!ctx) return DFD_ERR_PARAM;
   cudaSetDevice(ctx->device);
@@ -1294,7 +1381,9 @@ int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
   // fault file (io_fault.cu:16-71)
   if (p.rupture) {
     NcWriter& w = ctx->ncf;
-    if (!w.open(dir + "/fault_mpi000000.nc")) return fail(ctx, DFD_ERR_IO, "cannot create fault output");
+    char fn[64];
+    snprintf(fn, sizeof fn, "/fault_mpi%06d.nc", p.rank_y);
+    if (!w.open(dir + fn)) return fail(ctx, DFD_ERR_IO, "cannot create fault output");
     int nt = w.dim("nt", 0), nzd = w.dim("nz", d.nk), nyd = w.dim("ny", d.nj);
     std::vector<int> d2 = {nzd, nyd}, d3 = {nt, nzd, nyd};
     const char* fixed[] = {"x", "y", "z", "init_t0", "C0", "str_peak"};
@@ -1339,12 +1428,15 @@ int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
   }
   // wave slices (io_wave_xy.cu / io_wave_xz.cu / io_wave_yz.cu)
   const char* names[3] = {"wave_yz", "wave_xz", "wave_xy"};
-  int idx[3] = {p.EXPORT_WAVE_SLICE_X, p.EXPORT_WAVE_SLICE_Y, p.EXPORT_WAVE_SLICE_Z};
+  // the y slice in this slab's columns (written by the slab that holds it)
+  int idx[3] = {p.EXPORT_WAVE_SLICE_X, p.EXPORT_WAVE_SLICE_Y - p.rank_y * d.nj, p.EXPORT_WAVE_SLICE_Z};
   int lim[3] = {d.ni, d.nj, d.nk};
   for (int a = 0; a < 3; a++) {
     if (idx[a] < 0 || idx[a] >= lim[a]) continue;
     NcWriter& w = ctx->ncw[a];
-    if (!w.open(dir + "/" + names[a] + "_mpi000000.nc")) return fail(ctx, DFD_ERR_IO, "cannot create slice output");
+    char fn[64];
+    snprintf(fn, sizeof fn, "/%s_mpi%06d.nc", names[a], p.rank_y);
+    if (!w.open(dir + fn)) return fail(ctx, DFD_ERR_IO, "cannot create slice output");
     int nt = w.dim("nt", 0);
     int da, db;
     if (a == 0) { da = w.dim("nz", d.nk); db = w.dim("ny", d.nj); }
@@ -1433,7 +1525,8 @@ int dfd_output_write(dfd_ctx* ctx, int it_skip) {
                          ctx->s0));
     }
   }
-  const int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y, ctx->p.EXPORT_WAVE_SLICE_Z};
+  const int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y - ctx->p.rank_y * ctx->d.nj,
+                      ctx->p.EXPORT_WAVE_SLICE_Z};
   for (int a = 0; a < 3; a++)
     if (o.slice_n[a])
       dfd::slice_kernel<<<(unsigned)((o.slice_n[a] + 255) / 256), 256, 0, ctx->s0>>>(d, ctx->W[0], a, idx[a],
@@ -1569,7 +1662,7 @@ static int ens_build(dfd_ens* e) {
         a.it_dev = e->it_dev;  // one step counter for the whole ensemble
         fa.push_back(a);
         const int g = ((a.d.nj + 31) / 32) * ((a.d.nk + 3) / 4);
-        fs.push_back(fs.back() + node_blocks(a.NY, a.NZ, a.freenode));
+        fs.push_back(fs.back() + node_blocks(a.NY, a.NZ, a.freenode, a.jg0, a.d.nj));
         bs.push_back(bs.back() + 7 * g);  // the band kernel: seven parts per column block
       }
       S.fblocks = fs.back();

@@ -208,7 +208,7 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int blk, flo
     __syncthreads();
   }
   // node t of the non-united rectangle, numbered row by row
-  const NodeRect rc = node_rect(a.NY, a.NZ, a.freenode);
+  const NodeRect rc = node_rect(a.NY, a.NZ, a.freenode, a.jg0, d.nj);
   const long long tn = (long long)blk * blockDim.x + threadIdx.x;
   const bool inr = tn < rc.count();
   const int j = inr ? rc.j0 + (int)(tn % rc.w) : 0, k = inr ? rc.k0 + (int)(tn / rc.w) : 0;
@@ -385,7 +385,7 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int blk, flo
       Rr[1][m] = s1[0] * R[0][m] + s1[1] * R[1][m] + s1[2] * R[2][m];
       Rr[2][m] = s2[0] * R[0][m] + s2[1] * R[1][m] + s2[2] * R[2][m];
     }
-    double y1 = j - a.NY / 2;
+    double y1 = j + a.jg0 - a.NY / 2;
     double z1 = a.freenode ? (double)((a.NZ - 1 - k) - (int)(7.5e3 / a.DH)) : (double)(k - a.NZ / 2);
     double r = sqrt(y1 * y1 + z1 * z1) * (double)a.DH;
     double Fr = r < 3.0e3 ? exp(r * r / (r * r - 9.0e6)) : 0.0;
@@ -1107,7 +1107,8 @@ void launch_thermpress(const TpArgs& a, cudaStream_t s) {
 struct SensorGrid {
   const SensorArgs& a;
   __device__ bool inside(int j, int k) const {
-    return j + 1 >= a.fg[0] + 3 && j + 1 <= a.fg[1] - 3 && k + 1 >= a.fg[2] + 3 && k + 1 <= a.fg[3] - 3;
+    return j + 1 >= a.fg[0] + 3 && j + 1 <= a.fg[1] - 3 && k + 1 >= a.fg[2] + 3 && k + 1 <= a.fg[3] - 3 &&
+           (!a.slab || (j >= 2 && j < a.nj - 2));
   }
   // second difference of Ts1 along stride s at node (j, k), zero where the reference never
   // writes it
@@ -1144,7 +1145,7 @@ void launch_rup_sensor(const SensorArgs& a, cudaStream_t s) {
 
 void launch_fault_node(const FaultArgs& a, cudaStream_t s) {
   dim3 block(128, 1, 1);
-  dim3 grid(node_blocks(a.NY, a.NZ, a.freenode), 1, 1);
+  dim3 grid(node_blocks(a.NY, a.NZ, a.freenode, a.jg0, a.d.nj), 1, 1);
   int code = (a.FY > 0) * 2 + (a.FZ > 0);
   switch (code) {
     case 0: fault_node_kernel<-1, -1><<<grid, block, 0, s>>>(a); break;

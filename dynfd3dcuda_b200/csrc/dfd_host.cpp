@@ -115,6 +115,8 @@ void params_default(dfd_params* p) {
   p->rs_guess = 0;
   p->TP_n = 1;  // set_params.cu:103
   p->rs_guess_tol = 1e-10;
+  p->PY = 1;
+  p->rank_y = 0;
   finalize_params(p);
 }
 
@@ -192,6 +194,7 @@ int params_from_json(const char* text, dfd_params* p, std::string* err) {
     else if (k == "NormalRefine") inum(p->normal_refine);
     else if (k == "RS_guess") inum(p->rs_guess);
     else if (k == "RS_guess_tol") num(p->rs_guess_tol);
+    else if (k == "PY") inum(p->PY);
     else if (k == "TP_n") inum(p->TP_n);  // set_params.cu:281-282
     // PX/PY/PZ, igpu, vp1/vs1, RupThres, smoothing keys: accepted, not used on one GPU
   }
@@ -219,6 +222,15 @@ int check_params(const dfd_params* p, std::string* err) {
     return fail("DAMP_N too large for the grid");
   if (!(p->rs_guess_tol >= 0.0 && p->rs_guess_tol < 1.0)) return fail("RS_guess_tol must lie in [0, 1)");
   if (p->EXPORT_TIME_SKIP < 1) return fail("EXPORT_TIME_SKIP must be >= 1");
+  // decomposition along y: equal slabs (the reference's nj = NY / PY, set_params.cu), each
+  // wide enough for its PML slab and the three-column halo
+  if (p->PY < 1 || p->rank_y < 0 || p->rank_y >= p->PY) return fail("PY >= 1 and 0 <= rank_y < PY");
+  if (p->PY > 1) {
+    if (p->NY % p->PY) return fail("NY must be a multiple of PY");
+    const int nj = p->NY / p->PY;
+    if (nj < 8 || (p->use_pml && nj < p->PML_N + 4) || (p->use_cerjan && nj < p->DAMP_N + 4))
+      return fail("NY / PY too small for the PML, the sponge or the halo");
+  }
   return DFD_OK;
 }
 
@@ -329,18 +341,21 @@ void surface(const dfd_params* p, const float* fxyz, std::vector<double>& fx, st
 // friction planes (init.cu:904-1005).  vecn/vecs1/vecs2: (3, nz, ny) planes.
 void fault_init(const dfd_params* p, const float* planes, const float* vecn, const float* vecs1, const float* vecs2,
                 FaultHost& h) {
-  int nj = p->NY, nk = p->NZ, ny = nj + 6, nz = nk + 6;
+  // the slab rank_y of a domain decomposed along y: local columns j, global columns j0 + j
+  // (the masks and the input planes are global, init.cu:779-816 with gj = ranky nj + j)
+  const int nj = p->NY / p->PY, j0 = p->rank_y * nj, NYg = p->NY;
+  int nk = p->NZ, ny = nj + 6, nz = nk + 6;
   size_t nf = (size_t)nj * nk, nyz = (size_t)ny * nz;
   h.resize(nf);
   bool fs = p->free_surface != 0;
   for (int k = 0; k < nk; k++)
     for (int j = 0; j < nj; j++) {
       size_t q = j + (size_t)k * nj, f = (j + 3) + (size_t)(k + 3) * ny;
-      int gj1 = j + 1, gk1 = k + 1;
+      int gj1 = j0 + j + 1, gk1 = k + 1;
       const int* fg = p->Fault_grid;
       h.rupy[q] = (gj1 <= fg[0] + 3 || gj1 >= fg[1] - 3) ? 0 : 1;
       h.rupz[q] = (gk1 <= fg[2] + 3 || gk1 >= fg[3] - 3) ? 0 : 1;
-      bool inner = gj1 > 30 && gj1 < p->NY - 30 && gk1 > 30 && (fs || gk1 < p->NZ - 30);
+      bool inner = gj1 > 30 && gj1 < NYg - 30 && gk1 > 30 && (fs || gk1 < p->NZ - 30);
       h.united[q] = inner ? 0 : 1;
       h.faultgrid[q] = (gj1 >= fg[0] + 3 && gj1 <= fg[1] - 3 && gk1 >= fg[2] + 3 && gk1 <= fg[3] - 3) ? 1 : 0;
       // rate-and-state runs test a-b before the friction planes are read; the zero-filled
@@ -359,17 +374,20 @@ void fault_init(const dfd_params* p, const float* planes, const float* vecn, con
       }
     }
   if (p->INPORT_STRESS_TYPE == 1 && planes) {
+    // global planes (15, NZ, NY): this slab's columns
+    const size_t nfg = (size_t)NYg * nk;
+    auto pl = [&](int c, size_t q) { return planes[c * nfg + (q % nj) + j0 + (q / nj) * (size_t)NYg]; };
     std::vector<float>* dst[6] = {&h.T0x, &h.T0y, &h.T0z, &h.dT0x, &h.dT0y, &h.dT0z};
     for (int c = 0; c < 6; c++)
-      for (size_t q = 0; q < nf; q++) (*dst[c])[q] = planes[c * nf + q];
+      for (size_t q = 0; q < nf; q++) (*dst[c])[q] = pl(c, q);
     if (p->Friction_type == 0) {
       for (size_t q = 0; q < nf; q++) {
-        h.str_peak[q] = planes[6 * nf + q]; h.Dc[q] = planes[8 * nf + q]; h.C0[q] = planes[9 * nf + q];
+        h.str_peak[q] = pl(6, q); h.Dc[q] = pl(8, q); h.C0[q] = pl(9, q);
       }
     } else {
       for (size_t q = 0; q < nf; q++) {
-        h.a[q] = planes[10 * nf + q]; h.b[q] = planes[11 * nf + q]; h.L[q] = planes[12 * nf + q];
-        h.Vw[q] = planes[13 * nf + q]; h.State[q] = planes[14 * nf + q];
+        h.a[q] = pl(10, q); h.b[q] = pl(11, q); h.L[q] = pl(12, q);
+        h.Vw[q] = pl(13, q); h.State[q] = pl(14, q);
       }
     }
     // traction of the loaded stress in the local frame (init.cu:859-902)

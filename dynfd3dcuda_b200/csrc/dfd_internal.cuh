@@ -178,6 +178,7 @@ struct FaultArgs {
   float rDH, DH, DT, rka, rkb, mu_d, viscosity;
   double dDT, smooth_load_T, f0, V0, fw, Vini;
   int it, irk, FX, FY, FZ, freenode, friction_type, inport_stress, NY, NZ, rs_guess;
+  int jg0;                         // global column of local column 0 (a slab of a decomposed domain)
 };
 
 // The non-united fault nodes, where the fault node kernel works: the rectangle
@@ -188,18 +189,21 @@ struct NodeRect {
   int j0, k0, w, h;
   __host__ __device__ long long count() const { return (long long)w * h; }
 };
-__host__ __device__ inline NodeRect node_rect(int NY, int NZ, int freenode) {
+// in the local columns [0, nj) of a slab whose first column is global column jg0 (a domain
+// decomposed along y; jg0 = 0, nj = NY for one domain)
+__host__ __device__ inline NodeRect node_rect(int NY, int NZ, int freenode, int jg0, int nj) {
   NodeRect r;
-  r.j0 = 30;
+  const int jlo = 30 - jg0 > 0 ? 30 - jg0 : 0, jhi = NY - 31 - jg0 < nj ? NY - 31 - jg0 : nj;
+  r.j0 = jlo;
   r.k0 = 30;
-  r.w = NY - 61 > 0 ? NY - 61 : 0;
+  r.w = jhi - jlo > 0 ? jhi - jlo : 0;
   const int kh = freenode ? NZ : NZ - 31;
   r.h = kh - 30 > 0 ? kh - 30 : 0;
   return r;
 }
 // blocks of the fault node kernel (128 threads, one node each; at least one)
-inline int node_blocks(int NY, int NZ, int freenode) {
-  const long long c = node_rect(NY, NZ, freenode).count();
+inline int node_blocks(int NY, int NZ, int freenode, int jg0, int nj) {
+  const long long c = node_rect(NY, NZ, freenode, jg0, nj).count();
   return c > 0 ? (int)((c + 127) / 128) : 1;
 }
 
@@ -333,6 +337,7 @@ void launch_thermpress(const TpArgs& a, cudaStream_t s);
 // rupture sensor (rup_sensor.cu), once per step before the stages: from Ts1 into out
 struct SensorArgs {
   int nj, nk, fg[4];
+  int slab;  // a slab of a domain decomposed along y: no sensor within two columns of its ends
   const int* united;
   const float* Ts1;
   float* out;

@@ -65,6 +65,11 @@ typedef struct dfd_params {
    * remaining error (quadratic convergence) is at most rs_guess_tol |x|; default 1e-10,
    * which keeps the slip rate within FP32 rounding of the plain solve's */
   double rs_guess_tol;
+  /* decomposition of the domain along y (the reference's PY, mod_mpi.cu): PY equal slabs of
+   * NY / PY columns, this context holding slab rank_y; NY, Fault_grid and the input files
+   * stay global.  PY 1 (default): one domain. */
+  int PY;
+  int rank_y;
 } dfd_params;
 
 typedef struct dfd_ctx dfd_ctx;
@@ -209,6 +214,23 @@ int dfd_get_slice_noalloc(dfd_ctx *ctx, int axis, int index, float *host);
  * copy did not complete"), which stays sticky in this context; the device and other
  * contexts are unaffected.  Exercises the timeout path without faulting the GPU. */
 int dfd_test_wait_drill(dfd_ctx *ctx, int on);
+/* ---- halo exchange of a domain decomposed along y (replaces exchange_array,
+ *      exchange_wave and exchange_fault, mod_mpi.cu:104-281, mod_mpi_fault.cu:87-237) ----
+ * A slab's ghost columns next to a neighbouring slab hold that neighbour's nodes.  Side 0
+ * is the low-y side (columns 0..2 leave, ghost columns -3..-1 arrive), side 1 the high-y
+ * side (columns NY/PY-3..NY/PY-1 leave, columns NY/PY..NY/PY+2 arrive).  A message is
+ * dfd_halo_floats() floats, packed into and unpacked from DEVICE memory on the context's
+ * stream, so that it can go to the neighbour by NCCL, by a peer copy or through the host.
+ * what = DFD_HALO_SETUP once after dfd_precompute (the metric and media of the ghost
+ * columns, which the fault band's traction stencils read), then before every stage irk
+ * of every step what = irk (0..3): the stage's input wavefield (9 fields) and its
+ * split-node fault state (18 fields).  dfd_halo_pack of side s pairs with
+ * dfd_halo_unpack of side 1 - s on the neighbour.  Stepping then goes stage by stage
+ * (dfd_stage) with the exchange in between. */
+#define DFD_HALO_SETUP 4
+int dfd_halo_floats(dfd_ctx *ctx, long long *floats);
+int dfd_halo_pack(dfd_ctx *ctx, int what, int side, float *device_buf);
+int dfd_halo_unpack(dfd_ctx *ctx, int what, int side, const float *device_buf);
 /* host-side health check: 0 ok, DFD_ERR_NONFINITE if the fault state holds NaN/Inf */
 int dfd_check_finite(dfd_ctx *ctx);
 /* cumulative Newton iterations and non-converged solves of the rate-and-state trial */
