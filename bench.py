@@ -28,7 +28,10 @@ each of the four volume buffers (6.7 GB for the large domain) is far larger than
              (oracle/), the reference having no CPU path, on a bounded sample of steps
 
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-       [--config large|curved|flat|profile|ensemble] [--scenarios S]
+       [--config large|curved|flat|profile|ensemble] [--scenarios S] [--split]
+
+--split: one domain split along y over the N GPUs (strong scaling, halo exchange over
+NCCL before every RK stage) instead of the default N independent replicas.
 """
 import argparse
 import json
@@ -385,6 +388,58 @@ def run_ensemble(args, dfd, local):
     print(json.dumps(line), flush=True)
 
 
+def run_split(args, dfd, local, rank, world, dist):
+    """One domain split along y over the ranks (strong scaling): each rank holds a slab of
+    NY / N columns and swaps its boundary columns with its neighbours over NCCL before
+    every RK stage (dynfd3dcuda_b200.decomp).  Stage-by-stage stepping (the exchange sits
+    between the stages), timed between two full synchronisations with CUDA events, max
+    over ranks."""
+    import torch
+
+    from dynfd3dcuda_b200.decomp import DistributedSlab, slab_job
+
+    job, fx, st, layers, label = workload(args.config)
+    npts = job["NX"] * job["NY"] * job["NZ"]
+    sim = dfd.Simulation(slab_job(job, world, rank), fx, st, layers, device=local)
+    if dist is not None:
+        slab = DistributedSlab(sim, dist, device=f"cuda:{local}")
+        slab.setup()
+        step = slab.step
+    else:
+        def step(it):
+            for irk in range(4):
+                sim.stage(it, irk)
+    for it in range(args.warmup):
+        step(it)
+    sim.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for it in range(args.warmup, args.warmup + args.steps):
+        step(it)
+    sim.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+    sim.close()
+    line = {"metric": "Gpt-steps/s", "value": npts * args.steps / (ms / 1e3) / 1e9, "unit": "Gpt-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": label + f", split along y into {world} slabs", "nodes": npts,
+                       "parallelism": f"y-slabs x{world}, halo exchange over NCCL before every RK stage"},
+            "gpu_launches": (LAUNCHES_PER_STEP + (8 if world > 1 else 0)) * args.steps, "clocks": clocks}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,6 +450,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--scenarios", type=int, default=64, help="scenarios of the ensemble configuration")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned Newton-guess comparison")
+    ap.add_argument("--split", action="store_true",
+                    help="one domain split along y over the GPUs (strong scaling) instead of replicas")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -418,6 +475,9 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.split:
+        run_split(args, dfd, local, rank, world, dist)
+        return
     job, fx, st, layers, label = workload(args.config)
     npts = job["NX"] * job["NY"] * job["NZ"]
 

@@ -146,6 +146,12 @@ class DistributedSlab:
         if ops:
             for req in self.dist.batch_isend_irecv(ops):
                 req.wait()
+            if self.cuda:
+                # NCCL's wait orders the current stream only; the unpack runs on the
+                # context's own stream
+                import torch
+
+                torch.cuda.current_stream().synchronize()
         if below is not None:
             self._unpack(what, 0, self._recv[0])
         if above is not None:
