@@ -162,6 +162,10 @@ __device__ __forceinline__ double gt_func(double t, double T) {  // device.cu:13
   return 1.0;
 }
 
+// 16-byte pieces of the learned-guess weight vector (its last piece runs past the
+// vector's end into the allocation's slack)
+constexpr int NET_PIECES = (DFD_MLP_PARAMS + 3) / 4;
+
 // Base of the learned guess: the root asinh(Vhat e^{psi/a} / (2 V0)) of the solve without
 // the radiation-damping term, V0 = 1e-6; from its logarithm where the argument is above
 // e^18 (asinh y = ln 2y + 1/(4 y^2) + ..., the rest below FP64 rounding there), which
@@ -199,14 +203,26 @@ __device__ double newton_rs(double x, double psi, double ra, double Vhat, double
 template <int FY, int FZ>
 __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int blk, float* snet) {
   const Dims& d = a.d;
-  // learned-guess weights staged in shared memory (every thread reads the same weight at
-  // the same time: a broadcast)
+  // learned-guess weights to shared memory (the network's lanes then read the same weight
+  // at the same time: a broadcast), copied asynchronously in 16-byte pieces so that they
+  // land while the node's state update and trial traction run.  The block meets once at
+  // a barrier before the network: a thread whose node is not live arrives at once, the
+  // others before their solve; the barrier has no .aligned, which lets threads arrive from
+  // the two places.  (The weight vector's allocation and snet both extend to a whole
+  // 16-byte piece.)
   const bool learned = a.friction_type != 0 && a.rs_guess && a.guess_net;
   if (learned) {
     const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
-    for (int p = tid; p < DFD_MLP_PARAMS; p += nt) snet[p] = __ldg(a.guess_net + p);
-    __syncthreads();
+    for (int p = tid; p < NET_PIECES; p += nt)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(snet + 4 * p)),
+                   "l"(a.guess_net + 4 * p)
+                   : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
+  auto net_ready = [&]() {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("barrier.sync 0;" ::: "memory");
+  };
   // node t of the non-united rectangle, numbered row by row
   const NodeRect rc = node_rect(a.NY, a.NZ, a.freenode, a.jg0, d.nj);
   const long long tn = (long long)blk * blockDim.x + threadIdx.x;
@@ -218,7 +234,10 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int blk, flo
   // it runs where every lane's node is live (all warps but the last), the per-thread
   // network elsewhere
   const bool warp_full = __all_sync(0xffffffffu, live);
-  if (!live) return;
+  if (!live) {
+    if (learned) net_ready();
+    return;
+  }
   const long long n = d.nxyz, nyz = d.nyz;
   const int j1 = j + 3, k1 = k + 3, km = d.nk - k;
   const long long pf = j1 + (long long)k1 * d.ny;
@@ -450,6 +469,7 @@ __device__ __forceinline__ void fault_node_body(const FaultArgs& a, int blk, flo
       const double lnV = log(fmax(Vtn, 1e-300));
       float fin[4];
       features(lnV, fin);
+      net_ready();
       float res;
       if (warp_full) {
         __syncwarp();
@@ -902,7 +922,7 @@ __device__ __forceinline__ void fault_band_body(const FaultArgs& a, int bx, int 
 
 template <int FY, int FZ>
 __global__ void __launch_bounds__(128) fault_node_kernel(const __grid_constant__ FaultArgs a) {
-  __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
+  __shared__ __align__(16) float snet[4 * NET_PIECES];
   fault_node_body<FY, FZ>(a, blockIdx.x, snet);
 }
 // grid z: the part (six off-fault layers, then the split nodes), so that the seven
@@ -919,7 +939,7 @@ __global__ void __launch_bounds__(128, 4) fault_band_kernel(const __grid_constan
 template <int FY, int FZ>
 __global__ void __launch_bounds__(128) fault_node_batch(const FaultArgs* __restrict__ tab, const int* __restrict__ start,
                                                         int n) {
-  __shared__ __align__(16) float snet[DFD_MLP_PARAMS];
+  __shared__ __align__(16) float snet[4 * NET_PIECES];
   __shared__ __align__(16) unsigned char raw[sizeof(FaultArgs)];
   FaultArgs* sa = reinterpret_cast<FaultArgs*>(raw);
   int loc;
