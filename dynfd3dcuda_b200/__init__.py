@@ -201,7 +201,7 @@ class DfdParams(ctypes.Structure):
         ("use_cerjan", ctypes.c_int), ("normal_refine", ctypes.c_int), ("rs_guess", ctypes.c_int),
         ("OUT", ctypes.c_char * 1024), ("Fault_geometry", ctypes.c_char * 1024),
         ("Fault_init_stress", ctypes.c_char * 1024), ("Media1D", ctypes.c_char * 1024),
-        ("TP_n", ctypes.c_int), ("rs_guess_tol", ctypes.c_double), ("PY", ctypes.c_int), ("rank_y", ctypes.c_int),
+        ("TP_n", ctypes.c_int), ("rs_guess_tol", ctypes.c_double), ("slabs_y", ctypes.c_int), ("slab_y", ctypes.c_int),
     ]
 
 
@@ -296,7 +296,7 @@ class Simulation:
         nx, ny, nz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         L.dfd_dims(self.h, ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz))
         self.nx, self.ny, self.nz = nx.value, ny.value, nz.value
-        # NY: the columns this context holds (NY / PY for a slab of a decomposed domain)
+        # NY: the columns this context holds (NY / slabs_y for a slab of a decomposed domain)
         self.NX, self.NY, self.NZ = self.p.NX, self.ny - 6, self.p.NZ
         if fxyz is not None:
             a = np.ascontiguousarray(fxyz, np.float32)

@@ -264,8 +264,8 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return DFD_ERR_CUDA; }
   Dims& d = ctx->d;
-  // a slab of a domain decomposed along y holds NY / PY columns (PY 1: the whole domain)
-  d.ni = q.NX; d.nj = q.NY / q.PY; d.nk = q.NZ;
+  // a slab of a domain decomposed along y holds NY / slabs_y columns (1: the whole domain)
+  d.ni = q.NX; d.nj = q.NY / q.slabs_y; d.nk = q.NZ;
   d.nx = q.NX + 6; d.ny = d.nj + 6; d.nz = q.NZ + 6;
   d.i0 = d.nx / 2;
   d.N = q.PML_N;
@@ -304,7 +304,7 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
     for (int f = 0; f < 6 && !rc; f++) {
       if (f == 5 && q.free_surface) continue;
       // the y faces only on the slabs at the domain's y ends
-      if ((f == 2 && q.rank_y > 0) || (f == 3 && q.rank_y < q.PY - 1)) continue;
+      if ((f == 2 && q.slab_y > 0) || (f == 3 && q.slab_y < q.slabs_y - 1)) continue;
       const long long fs = pml_fstride(d, f);
       rc = dalloc(ctx, &ctx->aux[f][0], 27 * fs);
       if (!rc) {
@@ -446,10 +446,10 @@ int dfd_precompute(dfd_ctx* ctx) {
   // ---- grid, metric, media (FP64 on the GPU)
   x_line(&p, ctx->xl);
   surface(&p, ctx->fxyz.empty() ? nullptr : ctx->fxyz.data(), ctx->fx, ctx->fy, ctx->fz);
-  if (p.PY > 1) {
+  if (p.slabs_y > 1) {
     // this slab's columns of the domain's extended surface, its ghost columns included:
     // the neighbours' coordinates inside the domain, the extrapolated ones at its ends
-    const int nyg = p.NY + 6, j0 = p.rank_y * d.nj;
+    const int nyg = p.NY + 6, j0 = p.slab_y * d.nj;
     for (auto* v : {&ctx->fx, &ctx->fy, &ctx->fz}) {
       std::vector<double> loc((size_t)d.ny * d.nz);
       for (int k = 0; k < d.nz; k++)
@@ -509,7 +509,7 @@ int dfd_precompute(dfd_ctx* ctx) {
   // ---- PML 1-D profiles
   bool fs = p.free_surface != 0;
   int len[3] = {d.ni, d.nj, d.nk};
-  const bool ylo = p.rank_y == 0, yhi = p.rank_y == p.PY - 1;  // the slab holds a y end
+  const bool ylo = p.slab_y == 0, yhi = p.slab_y == p.slabs_y - 1;  // the slab holds a y end
   for (int a = 0; a < 3; a++) {
     std::vector<float> A, B, D, rb;
     bool lo = p.use_pml && !(a == 1 && !ylo), hi = p.use_pml && !(a == 2 && fs) && !(a == 1 && !yhi);
@@ -560,7 +560,7 @@ int dfd_precompute(dfd_ctx* ctx) {
         // this slab's columns of the (NZ, NY) plane
         std::vector<float> hy(nf);
         for (int k = 0; k < d.nk; k++)
-          for (int j = 0; j < d.nj; j++) hy[j + (size_t)k * d.nj] = ctx->tp_hy_h[p.rank_y * d.nj + j + (size_t)k * p.NY];
+          for (int j = 0; j < d.nj; j++) hy[j + (size_t)k * d.nj] = ctx->tp_hy_h[p.slab_y * d.nj + j + (size_t)k * p.NY];
         CK(cudaMemcpyAsync(ctx->tp_hy, hy.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s));
         CK(cudaStreamSynchronize(s));
       }
@@ -652,7 +652,7 @@ static FaultArgs fault_args(dfd_ctx* ctx, int pattern, int irk) {
     fa.Vini = (double)(float)p.Vini;
     fa.irk = irk; fa.FX = FX; fa.FY = FY; fa.FZ = FZ;
     fa.freenode = p.free_surface; fa.friction_type = p.Friction_type; fa.inport_stress = p.INPORT_STRESS_TYPE;
-    fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess; fa.jg0 = p.rank_y * d.nj;
+    fa.NY = p.NY; fa.NZ = p.NZ; fa.rs_guess = p.rs_guess; fa.jg0 = p.slab_y * d.nj;
     fa.prof = ctx->rs_prof; fa.judge = ctx->rs_judge; fa.guess_tol = p.rs_guess_tol;
   }
   (void)FX;
@@ -726,9 +726,9 @@ static SensorArgs sensor_args(dfd_ctx* ctx) {
   a.nj = ctx->d.nj; a.nk = ctx->d.nk;
   // a slab of a decomposed domain: the fault grid in its local columns, and no sensor where
   // the second differences would reach past the slab (as the reference's per-rank sensor)
-  const int j0 = ctx->p.rank_y * ctx->d.nj;
+  const int j0 = ctx->p.slab_y * ctx->d.nj;
   for (int i = 0; i < 4; i++) a.fg[i] = ctx->p.Fault_grid[i] - (i < 2 ? j0 : 0);
-  a.slab = ctx->p.PY > 1;
+  a.slab = ctx->p.slabs_y > 1;
   a.united = ctx->ipl + I_UNITED * nf;
   a.Ts1 = ctx->pl + (size_t)P_TS1 * nf;
   a.out = ctx->pl + (size_t)P_RUPS * nf;
@@ -1382,7 +1382,7 @@ int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
   if (p.rupture) {
     NcWriter& w = ctx->ncf;
     char fn[64];
-    snprintf(fn, sizeof fn, "/fault_mpi%06d.nc", p.rank_y);
+    snprintf(fn, sizeof fn, "/fault_mpi%06d.nc", p.slab_y);
     if (!w.open(dir + fn)) return fail(ctx, DFD_ERR_IO, "cannot create fault output");
     int nt = w.dim("nt", 0), nzd = w.dim("nz", d.nk), nyd = w.dim("ny", d.nj);
     std::vector<int> d2 = {nzd, nyd}, d3 = {nt, nzd, nyd};
@@ -1429,13 +1429,13 @@ int dfd_output_open(dfd_ctx* ctx, const char* outdir) {
   // wave slices (io_wave_xy.cu / io_wave_xz.cu / io_wave_yz.cu)
   const char* names[3] = {"wave_yz", "wave_xz", "wave_xy"};
   // the y slice in this slab's columns (written by the slab that holds it)
-  int idx[3] = {p.EXPORT_WAVE_SLICE_X, p.EXPORT_WAVE_SLICE_Y - p.rank_y * d.nj, p.EXPORT_WAVE_SLICE_Z};
+  int idx[3] = {p.EXPORT_WAVE_SLICE_X, p.EXPORT_WAVE_SLICE_Y - p.slab_y * d.nj, p.EXPORT_WAVE_SLICE_Z};
   int lim[3] = {d.ni, d.nj, d.nk};
   for (int a = 0; a < 3; a++) {
     if (idx[a] < 0 || idx[a] >= lim[a]) continue;
     NcWriter& w = ctx->ncw[a];
     char fn[64];
-    snprintf(fn, sizeof fn, "/%s_mpi%06d.nc", names[a], p.rank_y);
+    snprintf(fn, sizeof fn, "/%s_mpi%06d.nc", names[a], p.slab_y);
     if (!w.open(dir + fn)) return fail(ctx, DFD_ERR_IO, "cannot create slice output");
     int nt = w.dim("nt", 0);
     int da, db;
@@ -1525,7 +1525,7 @@ int dfd_output_write(dfd_ctx* ctx, int it_skip) {
                          ctx->s0));
     }
   }
-  const int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y - ctx->p.rank_y * ctx->d.nj,
+  const int idx[3] = {ctx->p.EXPORT_WAVE_SLICE_X, ctx->p.EXPORT_WAVE_SLICE_Y - ctx->p.slab_y * ctx->d.nj,
                       ctx->p.EXPORT_WAVE_SLICE_Z};
   for (int a = 0; a < 3; a++)
     if (o.slice_n[a])

@@ -115,8 +115,8 @@ void params_default(dfd_params* p) {
   p->rs_guess = 0;
   p->TP_n = 1;  // set_params.cu:103
   p->rs_guess_tol = 1e-10;
-  p->PY = 1;
-  p->rank_y = 0;
+  p->slabs_y = 1;
+  p->slab_y = 0;
   finalize_params(p);
 }
 
@@ -194,7 +194,6 @@ int params_from_json(const char* text, dfd_params* p, std::string* err) {
     else if (k == "NormalRefine") inum(p->normal_refine);
     else if (k == "RS_guess") inum(p->rs_guess);
     else if (k == "RS_guess_tol") num(p->rs_guess_tol);
-    else if (k == "PY") inum(p->PY);
     else if (k == "TP_n") inum(p->TP_n);  // set_params.cu:281-282
     // PX/PY/PZ, igpu, vp1/vs1, RupThres, smoothing keys: accepted, not used on one GPU
   }
@@ -224,12 +223,12 @@ int check_params(const dfd_params* p, std::string* err) {
   if (p->EXPORT_TIME_SKIP < 1) return fail("EXPORT_TIME_SKIP must be >= 1");
   // decomposition along y: equal slabs (the reference's nj = NY / PY, set_params.cu), each
   // wide enough for its PML slab and the three-column halo
-  if (p->PY < 1 || p->rank_y < 0 || p->rank_y >= p->PY) return fail("PY >= 1 and 0 <= rank_y < PY");
-  if (p->PY > 1) {
-    if (p->NY % p->PY) return fail("NY must be a multiple of PY");
-    const int nj = p->NY / p->PY;
+  if (p->slabs_y < 1 || p->slab_y < 0 || p->slab_y >= p->slabs_y) return fail("slabs_y >= 1 and 0 <= slab_y < slabs_y");
+  if (p->slabs_y > 1) {
+    if (p->NY % p->slabs_y) return fail("NY must be a multiple of slabs_y");
+    const int nj = p->NY / p->slabs_y;
     if (nj < 8 || (p->use_pml && nj < p->PML_N + 4) || (p->use_cerjan && nj < p->DAMP_N + 4))
-      return fail("NY / PY too small for the PML, the sponge or the halo");
+      return fail("NY / slabs_y too small for the PML, the sponge or the halo");
   }
   return DFD_OK;
 }
@@ -341,9 +340,9 @@ void surface(const dfd_params* p, const float* fxyz, std::vector<double>& fx, st
 // friction planes (init.cu:904-1005).  vecn/vecs1/vecs2: (3, nz, ny) planes.
 void fault_init(const dfd_params* p, const float* planes, const float* vecn, const float* vecs1, const float* vecs2,
                 FaultHost& h) {
-  // the slab rank_y of a domain decomposed along y: local columns j, global columns j0 + j
+  // slab slab_y of a domain decomposed along y: local columns j, global columns j0 + j
   // (the masks and the input planes are global, init.cu:779-816 with gj = ranky nj + j)
-  const int nj = p->NY / p->PY, j0 = p->rank_y * nj, NYg = p->NY;
+  const int nj = p->NY / p->slabs_y, j0 = p->slab_y * nj, NYg = p->NY;
   int nk = p->NZ, ny = nj + 6, nz = nk + 6;
   size_t nf = (size_t)nj * nk, nyz = (size_t)ny * nz;
   h.resize(nf);

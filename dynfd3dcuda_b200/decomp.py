@@ -6,7 +6,7 @@ split-node state with the neighbouring ranks (exchange_wave and exchange_fault,
 mod_mpi.cu:104-281, mod_mpi_fault.cu:87-237); the metric's ghost columns are swapped once
 (exchange_array, main.cu:277-297).  Here a domain splits along y into PY slabs of NY / PY
 columns: each slab is a context built from the domain's global job and input arrays with
-PY and its rank_y (the PML, the sponge, the masks and the output files follow the slab's
+slabs_y = PY and its slab_y (the PML, the sponge, the masks and the output files follow the slab's
 place), and the library packs and unpacks the messages in device memory
 (dfd_halo_pack / dfd_halo_unpack).  How a message travels is the caller's:
 
@@ -25,8 +25,8 @@ from . import HALO_SETUP, Simulation
 def slab_job(job, PY, rank):
     """The job of slab rank of a domain split into PY slabs along y."""
     j = dict(job)
-    j["PY"] = int(PY)
-    j["rank_y"] = int(rank)
+    j["slabs_y"] = int(PY)
+    j["slab_y"] = int(rank)
     return j
 
 

@@ -65,11 +65,13 @@ typedef struct dfd_params {
    * remaining error (quadratic convergence) is at most rs_guess_tol |x|; default 1e-10,
    * which keeps the slip rate within FP32 rounding of the plain solve's */
   double rs_guess_tol;
-  /* decomposition of the domain along y (the reference's PY, mod_mpi.cu): PY equal slabs of
-   * NY / PY columns, this context holding slab rank_y; NY, Fault_grid and the input files
-   * stay global.  PY 1 (default): one domain. */
-  int PY;
-  int rank_y;
+  /* decomposition of the domain along y (the reference's PY ranks, mod_mpi.cu): slabs_y
+   * equal slabs of NY / slabs_y columns, this context holding slab slab_y; NY, Fault_grid
+   * and the input files stay global.  Set by the caller, not read from a job file (a
+   * reference job's PX, PY, PZ are accepted and ignored: the whole domain runs in one
+   * context unless the caller splits it).  slabs_y 1 (default): one domain. */
+  int slabs_y;
+  int slab_y;
 } dfd_params;
 
 typedef struct dfd_ctx dfd_ctx;
@@ -214,11 +216,11 @@ int dfd_get_slice_noalloc(dfd_ctx *ctx, int axis, int index, float *host);
  * copy did not complete"), which stays sticky in this context; the device and other
  * contexts are unaffected.  Exercises the timeout path without faulting the GPU. */
 int dfd_test_wait_drill(dfd_ctx *ctx, int on);
-/* ---- halo exchange of a domain decomposed along y (replaces exchange_array,
+/* ---- halo exchange of a domain decomposed along y (slabs_y > 1) (replaces exchange_array,
  *      exchange_wave and exchange_fault, mod_mpi.cu:104-281, mod_mpi_fault.cu:87-237) ----
  * A slab's ghost columns next to a neighbouring slab hold that neighbour's nodes.  Side 0
  * is the low-y side (columns 0..2 leave, ghost columns -3..-1 arrive), side 1 the high-y
- * side (columns NY/PY-3..NY/PY-1 leave, columns NY/PY..NY/PY+2 arrive).  A message is
+ * side (the last three columns leave, the three ghost columns after them arrive).  A message is
  * dfd_halo_floats() floats, packed into and unpacked from DEVICE memory on the context's
  * stream, so that it can go to the neighbour by NCCL, by a peer copy or through the host.
  * what = DFD_HALO_SETUP once after dfd_precompute (the metric and media of the ghost

@@ -70,7 +70,7 @@ def test_json_keys_and_quirks(tmp_path):
            "Friction_type": 1, "RS_V0": 1e-6, "RS_Vini": 1e-12, "RS_f0": 0.6, "RS_fw": 0.2, "RS_L": 0.02,
            "rho1": 2500.0, "bi_vs2": 3000.0, "PML_N": 12, "PML_velocity": 6000.0, "Fault_grid": [51, 350, 51, 200],
            "Asp_grid": [1, 2, 3, 4], "OUT": "out_dir", "EXPORT_TIME_SKIP": 5, "useCerjan": 1, "FreeSurface": 0,
-           "PX": 2, "igpu": 3, "TP_n": 64}
+           "PX": 2, "PY": 4, "PZ": 2, "igpu": 3, "TP_n": 64}
     r, s = load_json(tmp_path, job)
     assert r == 0
     assert (s.NX, s.NY, s.NZ, s.Friction_type, s.PML_N, s.EXPORT_TIME_SKIP) == (300, 400, 200, 1, 12, 5)
@@ -81,8 +81,10 @@ def test_json_keys_and_quirks(tmp_path):
     assert s.TP_n == 64
     # NT = (int)(TMAX / DT) in single precision (set_params.cu:286-295)
     assert s.NT == int(np.float32(5.0031) / np.float32(0.006))
-    # unknown and multi-rank keys are accepted and leave the defaults alone
+    # unknown and multi-rank keys are accepted and leave the defaults alone: a reference
+    # job's PX/PY/PZ do not split the domain (the caller sets slabs_y / slab_y)
     assert s.mu_s == 0.677
+    assert (s.slabs_y, s.slab_y) == (1, 0)
 
 
 @pytest.mark.parametrize("path", REF_JOBS, ids=[os.path.basename(os.path.dirname(p)) for p in REF_JOBS])
@@ -110,7 +112,11 @@ def test_malformed_and_missing_json(tmp_path):
 # is infinite and the reference's heat source is NaN
 @pytest.mark.parametrize("bad", [{"PML_N": 31}, {"Friction_type": 3}, {"Friction_type": 3, "TP_n": 5000},
                                  {"Friction_type": 4}, {"NX": 4}, {"DT": 0.0},
-                                 {"EXPORT_TIME_SKIP": 0}, {"PML_N": 60, "NY": 100}])
+                                 {"EXPORT_TIME_SKIP": 0}, {"PML_N": 60, "NY": 100},
+                                 # slabs of a domain split along y: NY a multiple of slabs_y,
+                                 # slab_y in range, slabs wide enough for the PML and halo
+                                 {"slabs_y": 3}, {"slabs_y": 2, "slab_y": 2}, {"slabs_y": 0},
+                                 {"slabs_y": 5, "PML_N": 20}])
 def test_bad_jobs_rejected_before_device_work(bad):
     """dfd_create validates the job on the host and returns DFD_ERR_PARAM without touching a GPU."""
     job = {"NX": 100, "NY": 100, "NZ": 100}
