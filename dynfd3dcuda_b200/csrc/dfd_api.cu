@@ -128,7 +128,7 @@ struct dfd_ctx {
   float* mplane = nullptr;          // separable metric / media planes (12, nz, py)
   float* rxa = nullptr;             // 1/(d x / d xi) per padded x index
   float *rB[3] = {}, *B[3] = {}, *Dp[3] = {}, *Ap[3] = {};
-  float* aux[6][3] = {};
+  float* aux[6] = {};
   float *mVx2Vz = nullptr, *mVy2Vz = nullptr;
   float* damp[3] = {};
   float *FW[2] = {}, *Fm = nullptr, *Ft = nullptr, *T1 = nullptr, *mT1 = nullptr, *hT1 = nullptr;
@@ -300,17 +300,13 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
     if (!rc) rc = dalloc(ctx, &ctx->Ap[a], len[a]);
   }
   if (!rc && q.use_pml) {
-    // one block of 27 fields per face: value, RK accumulator, step-start copy
+    // 27 fields per face: three blocks of nine cycled through the RK stages
     for (int f = 0; f < 6 && !rc; f++) {
       if (f == 5 && q.free_surface) continue;
       // the y faces only on the slabs at the domain's y ends
       if ((f == 2 && q.slab_y > 0) || (f == 3 && q.slab_y < q.slabs_y - 1)) continue;
       const long long fs = pml_fstride(d, f);
-      rc = dalloc(ctx, &ctx->aux[f][0], 27 * fs);
-      if (!rc) {
-        ctx->aux[f][2] = ctx->aux[f][0] + 9 * fs;   // accumulator
-        ctx->aux[f][1] = ctx->aux[f][0] + 18 * fs;  // step start
-      }
+      rc = dalloc(ctx, &ctx->aux[f], 27 * fs);
     }
   }
   if (!rc) rc = dalloc(ctx, &ctx->mVx2Vz, 9LL * d.nx * d.ny);
@@ -355,7 +351,7 @@ int dfd_create(const dfd_params* p, int device, dfd_ctx** out) {
   const char* tv = getenv("DFD_TILE");
   const int mode = tv && tv[0] == '0' ? 0 : 1;
   float* auxb[6];
-  for (int f = 0; f < 6; f++) auxb[f] = ctx->aux[f][0];
+  for (int f = 0; f < 6; f++) auxb[f] = ctx->aux[f];
   ctx->use_tile =
       mode > 0 && tile_setup(&ctx->tile, d, ctx->W, ctx->mplane, auxb, ctx->tile_err, ctx->tile_sched, device);
   const char* sv = getenv("DFD_STREAMS");
@@ -584,7 +580,7 @@ int dfd_precompute(dfd_ctx* ctx) {
   }
   for (int b = 0; b < 4; b++) CK(cudaMemsetAsync(ctx->W[b], 0, sizeof(float) * 9 * d.nxyz, s));
   for (int f = 0; f < 6; f++)
-    if (ctx->aux[f][0]) CK(cudaMemsetAsync(ctx->aux[f][0], 0, sizeof(float) * 27 * pml_fstride(d, f), s));
+    if (ctx->aux[f]) CK(cudaMemsetAsync(ctx->aux[f], 0, sizeof(float) * 27 * pml_fstride(d, f), s));
   CK(cudaMemsetAsync(ctx->newton, 0, 8 * sizeof(unsigned long long), s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
@@ -679,7 +675,7 @@ static VolArgs vol_args(dfd_ctx* ctx, int pattern, int irk) {
   va.Bx = ctx->B[0]; va.By = ctx->B[1]; va.Bz = ctx->B[2];
   va.Dpx = ctx->Dp[0]; va.Dpy = ctx->Dp[1]; va.Dpz = ctx->Dp[2];
   va.Apx = ctx->Ap[0]; va.Apy = ctx->Ap[1]; va.Apz = ctx->Ap[2];
-  for (int f = 0; f < 6; f++) { va.aux[f] = ctx->aux[f][0]; va.aux0[f] = ctx->aux[f][1]; va.auxT[f] = ctx->aux[f][2]; }
+  for (int f = 0; f < 6; f++) va.aux[f] = ctx->aux[f];
   va.mVx2Vz = ctx->mVx2Vz; va.mVy2Vz = ctx->mVy2Vz;
   va.dampx = ctx->damp[0]; va.dampy = ctx->damp[1]; va.dampz = ctx->damp[2];
   va.united = p.rupture ? ctx->ipl + I_UNITED * nf : nullptr;
@@ -1693,7 +1689,7 @@ static int ens_build(dfd_ens* e) {
           }
         }
         TileScen& t = ts[i];
-        t.mp = tile_maps(c->tile, bin[irk]);
+        t.mp = tile_maps(c->tile, bin[irk], irk);
         t.u.a = a;
         t.u.sc = sch;
         t.u.unit0 = units;
@@ -1745,8 +1741,8 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
     // the general kernel beside the fault band kernel
     cudaEventRecord(e->ev_fork, e->s0);
     cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
-    launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, e->s2);
-    launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s2);
+    launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, irk, e->s2);
+    launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, irk, e->s2);
     cudaEventRecord(e->ev_join2, e->s2);
     if (nr) launch_fault_band_batch(S.fault, S.bstart, nr, S.bblocks, S.FX, S.FY, S.FZ, e->s0);
     cudaStreamWaitEvent(e->s0, e->ev_join2, 0);
@@ -1760,8 +1756,8 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
     cudaEventRecord(e->ev_join, e->s1);
   }
   cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
-  launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, e->s2);
-  launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, e->s2);
+  launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, irk, e->s2);
+  launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, irk, e->s2);
   cudaEventRecord(e->ev_join2, e->s2);
   launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
   launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, S.nunits > 0,

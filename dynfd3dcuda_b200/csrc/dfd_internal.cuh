@@ -6,7 +6,7 @@
 //             a step cycles A -> B -> C -> B -> A so that the stencil input of a stage is
 //             never written during that stage and no right-hand-side array exists
 //   M         13 fields xix xiy xiz etx ety etz ztx zty ztz jac lam mu rho, same layout
-//   aux       per PML face, 3 buffers (current, step start, RK accumulator) of 9 fields
+//   aux       per PML face, 3 blocks of 9 fields cycled through the RK stages (aux_cur)
 //   FW[2]     split-node state ping-pong (9, 2, nz, ny); Fm / Ft RK registers
 //   tables    fault coefficient tables as planes [table][element][nz*ny] (coalesced)
 #pragma once
@@ -45,6 +45,11 @@ enum Tab {
 // free-surface row tables, 9 elements per j
 enum TabF { TF_VX2VZ1 = 0, TF_VY2VZ1, TF_VX2VZ2, TF_VY2VZ2, TF_P2M1, TF_P2M2, TF_P2M3, TF_M2P1, TF_M2P2, TF_M2P3, NTABF };
 
+// The volume buffer cycle of a step: stage inputs A B C B, outputs B C B A (buffers 0..2),
+// buffer 3 the RK accumulator.
+__host__ __device__ constexpr int stage_in(int irk) { return irk == 0 ? 0 : irk == 2 ? 2 : 1; }
+__host__ __device__ constexpr int stage_out(int irk) { return irk == 1 ? 2 : irk == 3 ? 0 : 1; }
+
 // Volume fields are stored with a padded row pitch: node (i, j, k) (padded indices, 3 ghost
 // nodes per side) of a field sits at element (j + oy) + k*py + i*sx.  The row offset oy = 1
 // puts the first interior node of every row (j = 3) on a 16-byte boundary and the pitch
@@ -63,9 +68,9 @@ struct Dims {
   int yb3;              // first stored column of the y2-face PML state (a multiple of 4)
 };
 
-// ADE state of PML face f (x1 x2 y1 y2 z1 z2): one block of 27 fields per face, the
-// current value (fields 0..8), the RK accumulator (9..17) and the step-start copy
-// (18..26), each field pml_fstride apart.  The layouts keep the volume's row frame, so
+// ADE state of PML face f (x1 x2 y1 y2 z1 z2): 27 fields per face, three blocks of nine
+// (0..8, 9..17, 18..26) that hold the step-start value, the stage values and the RK
+// accumulator in turn (aux_cur, dfd_stencil.cuh), each field pml_fstride apart.  The layouts keep the volume's row frame, so
 // that a 32 x 8 tile of nodes is one TMA box at a 16-byte aligned column:
 //   x faces: N planes of (nz rows, py columns), column j + 3 + oy, row k + 3;
 //   y faces: ni planes of (nz rows, wy columns), column j + 3 + oy - (0 | yb3), row k + 3;
@@ -93,8 +98,8 @@ struct VolArgs {
   Dims d;
   const float* __restrict__ Win;   // stencil input of this stage
   const float* __restrict__ W0;    // step-start state (stages 1, 2)
-  float* __restrict__ Wout;        // output of this stage
-  float* __restrict__ T;           // RK accumulator
+  float* __restrict__ Wout;        // output of this stage (at stage 2 first read: the stage-1 input)
+  float* __restrict__ T;           // RK accumulator (written at stage 2, read at stage 3)
   const float* __restrict__ M;
   const float* __restrict__ rBx;   // 1/beta per axis (PML), 1 outside
   const float* __restrict__ rBy;
@@ -108,9 +113,7 @@ struct VolArgs {
   const float* __restrict__ Apx;   // alpha per axis
   const float* __restrict__ Apy;
   const float* __restrict__ Apz;
-  float* aux[6];                   // current PML state per face (x1 x2 y1 y2 z1 z2) or null
-  float* aux0[6];                  // step-start copy
-  float* auxT[6];                  // RK accumulator
+  float* aux[6];                   // PML state per face (x1 x2 y1 y2 z1 z2, 27 fields) or null
   const float* __restrict__ mVx2Vz;  // (nx, ny, 9) free-surface transforms
   const float* __restrict__ mVy2Vz;
   const float* __restrict__ dampx;   // Cerjan 1-D profiles (padded index) or null
@@ -229,7 +232,7 @@ constexpr int TILE_J = 32, TILE_K = 8, STRIP = 16;
 struct TileMaps {
   CUtensorMap win;  // stencil input, halo box
   CUtensorMap w0;   // step-start state, pointwise box
-  CUtensorMap t;    // RK accumulator, pointwise box
+  CUtensorMap t;    // second pointwise box: stage 2 the stage-1 input, stage 3 the accumulator
   CUtensorMap plane;  // separable metric / media planes (12, nz, py)
   CUtensorMap aux[6];  // PML state of each face (27 fields), pointwise box of 9 fields
   // the same for the 16 x 16 strip tiles (halo box 24 x 20)
@@ -252,7 +255,7 @@ struct TileCtx {
 bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, float* const aux[6], int* err,
                 int* sched, int device);
 // every map the tiled kernels read at a stage whose stencil input is buffer `bin`
-TileMaps tile_maps(const TileCtx& tc, int bin);
+TileMaps tile_maps(const TileCtx& tc, int bin, int irk);
 // Units of a tiled kernel: tile columns times chunks of x planes.
 //   interior kernel: the 32 x 8 tiles of the box lo..hi (the last ones partial);
 //   PML kernel: the nodes below the free-surface rows (k < ktop) outside the interior
@@ -318,9 +321,10 @@ void launch_pml_batch(const TileScen& first, const TileScen* tab, int n, int nun
 // batched launches (dfd_volume.cu, dfd_tile.cu, dfd_fault.cu)
 void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,
                        int FZ, int* err, int* sched, cudaStream_t s);
-// top: the free-surface boxes (start: per-scenario block starts of those), else the others
+// top: the free-surface boxes (start: per-scenario block starts of those), else the others;
+// irk: the stage of every scenario's arguments
 void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, int FX, int FY,
-                        int FZ, bool top, cudaStream_t s);
+                        int FZ, bool top, int irk, cudaStream_t s);
 void launch_fault_node_batch(const FaultArgs* tab, const int* start, int n, int blocks, int FY, int FZ,
                              cudaStream_t s);
 // thermal pressurisation (Friction_type 3): node-major columns of n points across the

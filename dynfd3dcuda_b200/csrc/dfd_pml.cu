@@ -22,7 +22,9 @@
 namespace dfd {
 
 namespace {
-constexpr int PSLOT_M = 45 * PB;  // W0 9, T 9, then the face's ADE state: value 9, accumulator 9, step start 9
+// W0 9, the stage-1 input or T 9, then the face's ADE state: the current value 9, y0 or the
+// accumulator 9, y1 9 (aux_block)
+constexpr int PSLOT_M = 45 * PB;
 constexpr int MS = 6, MP = 2, MQ = 2;  // ring depths (stencil planes, pointwise planes, unit planes)
 constexpr int PCW = TK;                 // computing warps: one per row of the tile, all nine fields
 constexpr int PTOT = PCW * 32 + 32;     // plus one copy-issuing warp
@@ -90,12 +92,18 @@ __device__ __forceinline__ PmlUnit pml_unit(const TileSched& sc, const VolArgs& 
   return r;
 }
 
+// Block of the ADE state staged in slot n (0..2) of a pointwise slot at stage irk: the
+// current value, then y0 (stages 1, 2) or the accumulator (stage 3), then y1 (stage 2).
+__host__ __device__ constexpr int aux_block(int irk, int n) {
+  return n == 0 ? aux_cur(irk) : n == 1 ? (irk == 3 ? 2 : 0) : 1;
+}
+
 // ADE update of face `face` for fields F0..F0+2 at this node (pml_update of
 // dfd_stencil.cuh, restricted to three fields): adds -aux/beta to the rates p and advances
-// the state in place with the RK4 registers.  The state comes from shared memory (A, the
-// staged own face) or from global memory; every load precedes the stores, which may alias
-// them as far as the compiler knows.
-template <int F0, int AX>
+// the state with the RK4 blocks of aux_cur.  The state comes from shared memory (A, the
+// staged own face, in the order of aux_block) or from global memory; every load precedes
+// the stores, which may alias them as far as the compiler knows.
+template <int F0, int AX, int IRK>
 __device__ __forceinline__ void role_face(const VolArgs& a, int face, bool staged, const float* A, int i, int j,
                                           int k, float rb, float dd, float al, const float* D, float* p) {
   const Dims& d = a.d;
@@ -113,37 +121,48 @@ __device__ __forceinline__ void role_face(const VolArgs& a, int face, bool stage
     qa = (long long)(j + 3 + d.oy) + (long long)kz * d.py + (long long)i * d.py * d.N;
   }
   float* base = a.aux[face];
-  const int irk = a.irk;
+  constexpr int irk = IRK;
+  const long long b9 = 9 * fs;
   const float ad = -(al + dd);
-  float w[3], t[3], w0[3];
+  float w[3], s2[3], y1[3];  // current value; y0 or the accumulator; y1
 #pragma unroll
   for (int m = 0; m < 3; m++) {
     const int f = F0 + m;
     if (staged) {
       w[m] = A[f * PB];
-      if (irk >= 1) t[m] = A[(9 + f) * PB];
-      if (irk == 1 || irk == 2) w0[m] = A[(18 + f) * PB];
+      if (irk >= 1) s2[m] = A[(9 + f) * PB];
+      if (irk == 2) y1[m] = A[(18 + f) * PB];
     } else {
-      const long long x = f * fs + qa;
-      w[m] = base[x];
-      if (irk >= 1) t[m] = base[x + 9 * fs];
-      if (irk == 1 || irk == 2) w0[m] = base[x + 18 * fs];
+      const float* x = base + f * fs + qa;
+      if (irk == 0) {
+        w[m] = x[0];
+      } else if (irk == 1) {
+        w[m] = x[b9];
+        s2[m] = x[0];
+      } else if (irk == 2) {
+        w[m] = x[2 * b9];
+        s2[m] = x[0];
+        y1[m] = x[b9];
+      } else {
+        w[m] = x[b9];
+        s2[m] = x[2 * b9];
+      }
     }
   }
 #pragma unroll
   for (int m = 0; m < 3; m++) {
-    const long long x = (F0 + m) * fs + qa;
+    float* x = base + (F0 + m) * fs + qa;
     p[m] += -w[m] * rb;
     const float h = ad * w[m] + dd * D[m];
     if (irk == 0) {
-      base[x + 18 * fs] = w[m];
-      base[x + 9 * fs] = fmaf(a.rkb, h, w[m]);
-      base[x] = fmaf(a.rka, h, w[m]);
-    } else if (irk < 3) {
-      base[x + 9 * fs] = fmaf(a.rkb, h, t[m]);
-      base[x] = fmaf(a.rka, h, w0[m]);
+      x[b9] = fmaf(a.rka, h, w[m]);
+    } else if (irk == 1) {
+      x[2 * b9] = fmaf(a.rka, h, s2[m]);
+    } else if (irk == 2) {
+      x[2 * b9] = rk_acc(rk_sum(y1[m], w[m]), 1.0f / 3.0f, a.rkb, h);
+      x[b9] = fmaf(a.rka, h, s2[m]);
     } else {
-      base[x] = fmaf(a.rkb, h, t[m]);
+      x[0] = fmaf(a.rkb, h, s2[m]);
     }
   }
 }
@@ -206,7 +225,7 @@ struct YZFactors {
   float rby, ddy, aly, rbz, ddz, alz;
 };
 
-template <int FX, int FY, int FZ>
+template <int FX, int FY, int FZ, int IRK>
 __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* x0, const float* x1, const float* x2,
                                          const float* x3, const float* x4, const float* cur, const NodeMetric& g,
                                          int i, int j, int k, int fx, int fy, int fz, int own, const float* A,
@@ -230,9 +249,9 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
     if (fx >= 0) {
       const bool st = fx == own;
       const float dd = ddx, al = alx;
-      role_face<0, 0>(a, fx, st, A, i, j, k, rb, dd, al, D, hv + 0);
-      role_face<3, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
-      role_face<6, 0>(a, fx, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
+      role_face<0, 0, IRK>(a, fx, st, A, i, j, k, rb, dd, al, D, hv + 0);
+      role_face<3, 0, IRK>(a, fx, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
+      role_face<6, 0, IRK>(a, fx, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
     }
   }
   // y
@@ -248,9 +267,9 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
     if (fy >= 0) {
       const bool st = fy == own;
       const float dd = yz.ddy, al = yz.aly;
-      role_face<0, 1>(a, fy, st, A, i, j, k, rb, dd, al, D, hv + 0);
-      role_face<3, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
-      role_face<6, 1>(a, fy, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
+      role_face<0, 1, IRK>(a, fy, st, A, i, j, k, rb, dd, al, D, hv + 0);
+      role_face<3, 1, IRK>(a, fy, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
+      role_face<6, 1, IRK>(a, fy, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
     }
   }
   // z
@@ -266,12 +285,12 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
     if (fz >= 0) {
       const bool st = fz == own;
       const float dd = yz.ddz, al = yz.alz;
-      role_face<0, 2>(a, fz, st, A, i, j, k, rb, dd, al, D, hv + 0);
-      role_face<3, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
-      role_face<6, 2>(a, fz, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
+      role_face<0, 2, IRK>(a, fz, st, A, i, j, k, rb, dd, al, D, hv + 0);
+      role_face<3, 2, IRK>(a, fz, st, A, i, j, k, rb, dd, al, D + 3, hv + 3);
+      role_face<6, 2, IRK>(a, fz, st, A, i, j, k, rb, dd, al, D + 6, hv + 6);
     }
   }
-  rk_tile_store<0, 9>(a, a.d.nxyz, q, cur, P, hv, damp);
+  rk_tile_store<0, 9, IRK>(a, a.d.nxyz, q, cur, P, hv, damp);
 }
 
 // Warp PCW issues the copies; warps 0..PCW-1 compute, one per row of nodes, all nine
@@ -280,9 +299,10 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
 // partitions), what the ADE path needs without spilling.  Rings as in the interior
 // kernel, with shallower stencil and pointwise rings: a pointwise slot also holds the own
 // face's ADE state, so it is 2.5 times larger.
-// BATCH: the units of the nscen scenarios of tab in one launch; mp0, a0, sc0 describe
-// scenario 0 and give the stage's common values.
-template <int FX, int FY, int FZ, bool BATCH>
+// IRK: the RK stage, compiled per stage as in the interior kernel.  BATCH: the units of
+// the nscen scenarios of tab in one launch; mp0, a0, sc0 describe scenario 0 and give the
+// stage's common values.
+template <int FX, int FY, int FZ, int IRK, bool BATCH>
 __global__ void __maxnreg__(168)
     volume_pml_kernel(const __grid_constant__ TileMaps mp0, const __grid_constant__ VolArgs a0,
                       const __grid_constant__ TileSched sc0, const TileScen* __restrict__ tab, int nscen, int nunits,
@@ -302,9 +322,11 @@ __global__ void __maxnreg__(168)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int XLO = FX == 1 ? -1 : -3;
   constexpr int RZ = FZ == 1 ? 1 : 3;
-  const int irk = a0.irk;
-  const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1;
-  const int naux = irk == 0 ? 9 : irk == 3 ? 18 : 27;  // ADE fields staged per plane
+  constexpr int irk = IRK;
+  // pointwise boxes as in the interior kernel: y0 at stages 1 and 2, the second box (the
+  // stage-1 input, the accumulator) at stages 2 and 3
+  constexpr bool needW0 = irk == 1 || irk == 2, needT = irk >= 2;
+  constexpr int naux = irk == 0 ? 9 : irk == 2 ? 27 : 18;  // ADE fields staged per plane
   const int G = gridDim.x;
 
   if (threadIdx.x == 0) {
@@ -376,7 +398,8 @@ __global__ void __maxnreg__(168)
         mbar_expect_tx(b, ptx);
         if (needW0) tma_load4(dst, m_w0, cp0, cp1, i + 3, 0, b);
         if (needT) tma_load4(dst + 9 * PB, m_t, cp0, cp1, i + 3, 0, b);
-        for (int fb = 0; fb < na; fb += 9) tma_load4(dst + (18 + fb) * PB, m_aux, ac0, ac1, i - aoff, fb, b);
+        for (int nb = 0; nb * 9 < na; nb++)
+          tma_load4(dst + (18 + 9 * nb) * PB, m_aux, ac0, ac1, i - aoff, 9 * aux_block(irk, nb), b);
         pr.next<MP>();
         pcount++;
       }
@@ -486,13 +509,13 @@ __global__ void __maxnreg__(168)
         const long long q = qyz + (long long)(i + 3) * d.sx;
         if (pu.strip || pml) {
           // (strips hold y-slab nodes and the few interior columns beside them)
-          pml_node<FX, FY, FZ>(a, pu.strip ? STRIP + 8 : HW, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face,
+          pml_node<FX, FY, FZ, IRK>(a, pu.strip ? STRIP + 8 : HW, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face,
                                P + 18 * PB, q, P, damp, rbx, ddx, alx, yz);
         } else {
           float hv[9];
           lean_velocity<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);
           lean_stress<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);
-          rk_tile_store<0, 9>(a, d.nxyz, q, cur, P, hv, damp);
+          rk_tile_store<0, 9, IRK>(a, d.nxyz, q, cur, P, hv, damp);
         }
       }
       __syncwarp();
@@ -515,13 +538,18 @@ __global__ void __maxnreg__(168)
 
 // ---------------- host side
 
-template <int FX, int FY, int FZ>
-static bool pml_smem() {
+template <int FX, int FY, int FZ, int IRK>
+static bool pml_smem_k() {
   auto one = [](const void* f) {
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PML_SMEM) == cudaSuccess;
   };
-  return one((const void*)volume_pml_kernel<FX, FY, FZ, false>) &&
-         one((const void*)volume_pml_kernel<FX, FY, FZ, true>);
+  return one((const void*)volume_pml_kernel<FX, FY, FZ, IRK, false>) &&
+         one((const void*)volume_pml_kernel<FX, FY, FZ, IRK, true>);
+}
+template <int FX, int FY, int FZ>
+static bool pml_smem() {
+  return pml_smem_k<FX, FY, FZ, 0>() && pml_smem_k<FX, FY, FZ, 1>() && pml_smem_k<FX, FY, FZ, 2>() &&
+         pml_smem_k<FX, FY, FZ, 3>();
 }
 
 bool pml_setup() {
@@ -593,13 +621,15 @@ static void pml_launch(const TileMaps& mp, const VolArgs& a, const TileSched& sc
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, volume_pml_kernel<FX, FY, FZ, BATCH>, mp, a, sc, tab, n, nunits, err, sched + 2);
+#define DFD_L(K) cudaLaunchKernelEx(&cfg, volume_pml_kernel<FX, FY, FZ, K, BATCH>, mp, a, sc, tab, n, nunits, err, sched + 2)
+  DFD_BY_STAGE(a.irk, DFD_L);
+#undef DFD_L
 }
 
 template <int FX, int FY, int FZ>
 static void launch_p(const TileCtx& tc, const VolArgs& a, int bin, const TileSched& ps, int grid, bool pdl,
                      cudaStream_t s) {
-  const TileMaps mp = tile_maps(tc, bin);
+  const TileMaps mp = tile_maps(tc, bin, a.irk);
   pml_launch<FX, FY, FZ, false>(mp, a, ps, nullptr, 1, ps.nunits, grid, tc.err, tc.sched, pdl, s);
 }
 

@@ -21,34 +21,80 @@ __device__ __forceinline__ void axis_terms(const float* d, float e0, float e1, f
   D[8] = (d[1] * e2 + d[2] * e1) * mu;
 }
 
-// ADE state of one PML face for this node, loaded ahead of its use: current value, and the
-// RK registers the stage needs (accumulator for stages 1..3, step start for stages 1, 2).
+// CALL(K) with the stage irk as the compile-time constant K
+#define DFD_BY_STAGE(irk, CALL) \
+  do {                          \
+    switch (irk) {              \
+      case 0: CALL(0); break;   \
+      case 1: CALL(1); break;   \
+      case 2: CALL(2); break;   \
+      default: CALL(3); break;  \
+    }                           \
+  } while (0)
+
+// Classic RK4 without storing the accumulator at stages 0 and 1.  With step-start value y0
+// and stage inputs y1 = y0 + (dt/2) k1, y2 = y0 + (dt/2) k2, the sum
+//   (y1 + 2 y2) / 3 = y0 + (dt/6) k1 + (dt/3) k2
+// is the accumulator after stage 1, so after stage 2 it is (y1 + 2 y2) / 3 + rkb h with
+// rkb h = (dt/3) k3.  Stages 0 and 1 therefore write no accumulator and stage 1 reads
+// none; stage 2 re-reads its node's stage-1 input (the buffer it is about to overwrite)
+// and writes the accumulator that stage 3 completes (rk4.cu:20-33 forms the same sums term
+// by term).  Stored stage inputs carry the sponge factor damp, hence the factor
+// r3 = 1 / (3 damp).
+__device__ __forceinline__ float rk_sum(float y1, float y2) { return fmaf(2.0f, y2, y1); }
+__device__ __forceinline__ float rk_acc(float s, float r3, float rkb, float h) { return fmaf(rkb, h, s * r3); }
+__device__ __forceinline__ float rk_r3(float damp) { return __fdividef(1.0f / 3.0f, damp); }
+
+// The ADE state of a PML face is pointwise, so its three 9-field blocks cycle like the
+// volume buffers with the accumulator in the block the stage no longer needs:
+//   stage 0: current block 0 (y0)                   -> block 1 = y0 + rka h
+//   stage 1: current block 1, y0 in block 0         -> block 2 = y0 + rka h
+//   stage 2: current block 2, y0 in 0, y1 in 1      -> block 1 = y0 + rka h, block 2 = acc
+//   stage 3: current block 1, acc in block 2        -> block 0 = acc + rkb h
+// Between steps block 0 holds the state.  Block of the current value at stage irk:
+__host__ __device__ constexpr int aux_cur(int irk) { return irk == 0 ? 0 : irk == 2 ? 2 : 1; }
+
+// ADE state of one PML face for this node, loaded ahead of its use: the current value
+// and the registers the stage needs (y0 at stages 1 and 2, y1 at stage 2, the accumulator
+// at stage 3), blocks st * 9 apart.
 struct PmlState {
-  float w[9], t[9], w0[9];
+  float w[9], s[9], y1[9];
 };
+// IRK: the stage as a compile-time constant, or -1 to take it from a.irk
+template <int IRK>
 __device__ __forceinline__ void pml_load(const VolArgs& a, int face, long long qa, long long st, PmlState& ps) {
-  const float* aux = a.aux[face];
-  const float* aux0 = a.aux0[face];
-  const float* auxT = a.auxT[face];
+  const int irk = IRK >= 0 ? IRK : a.irk;
+  const long long b9 = 9 * st;
 #pragma unroll
   for (int f = 0; f < 9; f++) {
-    const long long x = f * st + qa;
-    ps.w[f] = aux[x];
-    if (a.irk >= 1) ps.t[f] = auxT[x];
-    if (a.irk == 1 || a.irk == 2) ps.w0[f] = aux0[x];
+    // the blocks of each stage spelled out: constant multiples of the block stride
+    const float* x = a.aux[face] + f * st + qa;
+    if (irk == 0) {
+      ps.w[f] = x[0];
+    } else if (irk == 1) {
+      ps.w[f] = x[b9];
+      ps.s[f] = x[0];
+    } else if (irk == 2) {
+      ps.w[f] = x[2 * b9];
+      ps.s[f] = x[0];
+      ps.y1[f] = x[b9];
+    } else {
+      ps.w[f] = x[b9];
+      ps.s[f] = x[2 * b9];
+    }
   }
 }
 
 // PML auxiliary update of one face for this node from its loaded state: accumulates
-// -aux/beta into p[] and advances aux in place with the RK4 registers (pmlx.cu:165-208,
+// -aux/beta into p[] and advances the state with the RK4 blocks above (pmlx.cu:165-208,
 // rk4.cu:208-255).
+template <int IRK>
 __device__ __forceinline__ void pml_update(const VolArgs& a, int face, long long qa, long long st, float rb, float b,
                                            float dd, float al, const float* Dv, const float* dzv, float ez0,
                                            float ez1, float ez2, float lam, float mu, const PmlState& ps,
                                            float* p) {
-  float* aux = a.aux[face];
-  float* aux0 = a.aux0[face];
-  float* auxT = a.auxT[face];
+  const int irk = IRK >= 0 ? IRK : a.irk;
+  const long long b9 = 9 * st;
   float ad = -(al + dd);
   float add[6];
   if (dzv) {
@@ -62,48 +108,55 @@ __device__ __forceinline__ void pml_update(const VolArgs& a, int face, long long
   }
 #pragma unroll
   for (int f = 0; f < 9; f++) {
-    const long long x = f * st + qa;
+    float* x = a.aux[face] + f * st + qa;
     p[f] += -ps.w[f] * rb;
     float h = ad * ps.w[f] + dd * Dv[f];
     if (dzv && f >= 3) h += add[f - 3];
-    if (a.irk == 0) {
-      aux0[x] = ps.w[f];
-      auxT[x] = fmaf(a.rkb, h, ps.w[f]);
-      aux[x] = fmaf(a.rka, h, ps.w[f]);
-    } else if (a.irk < 3) {
-      auxT[x] = fmaf(a.rkb, h, ps.t[f]);
-      aux[x] = fmaf(a.rka, h, ps.w0[f]);
+    if (irk == 0) {
+      x[b9] = fmaf(a.rka, h, ps.w[f]);
+    } else if (irk == 1) {
+      x[2 * b9] = fmaf(a.rka, h, ps.s[f]);
+    } else if (irk == 2) {
+      x[2 * b9] = rk_acc(rk_sum(ps.y1[f], ps.w[f]), 1.0f / 3.0f, a.rkb, h);
+      x[b9] = fmaf(a.rka, h, ps.s[f]);
     } else {
-      aux[x] = fmaf(a.rkb, h, ps.t[f]);
+      x[0] = fmaf(a.rkb, h, ps.s[f]);
     }
   }
 }
 
 // Both steps at once: every load of the face precedes every store (the compiler cannot
-// prove the three buffers distinct, and a load issued after a store would wait for a full
+// prove the blocks distinct, and a load issued after a store would wait for a full
 // memory round trip per field).
+template <int IRK>
 __device__ __forceinline__ void pml_face(const VolArgs& a, int face, long long qa, long long st, float rb, float b,
                                          float dd, float al, const float* Dv, const float* dzv, float ez0,
                                          float ez1, float ez2, float lam, float mu, float* p) {
   PmlState ps;
-  pml_load(a, face, qa, st, ps);
-  pml_update(a, face, qa, st, rb, b, dd, al, Dv, dzv, ez0, ez1, ez2, lam, mu, ps, p);
+  pml_load<IRK>(a, face, qa, st, ps);
+  pml_update<IRK>(a, face, qa, st, rb, b, dd, al, Dv, dzv, ez0, ez1, ez2, lam, mu, ps, p);
 }
 
-// RK4 register update of the nine fields of node q with right-hand side h (+ p), then the
-// sponge factor (rk4.cu:20-33, cerjan.cu:166-200).  Every load precedes every store.
+// RK4 update of the nine fields of node q with right-hand side h (+ p), then the sponge
+// factor (rk4.cu:20-33, cerjan.cu:166-200); the accumulator only at stages 2 and 3 (rk_acc).
+// Every load precedes every store.
+template <int IRK>
 __device__ __forceinline__ void rk_store(const VolArgs& a, long long q, const float* h, const float* p,
                                          float damp) {
+  const int irk = IRK >= 0 ? IRK : a.irk;
   const long long n = a.d.nxyz;
+  const float r3 = irk == 2 ? rk_r3(damp) : 0.0f;
   float r0[9], r1[9];
 #pragma unroll
   for (int f = 0; f < 9; f++) {
     const long long x = f * n + q;
-    if (a.irk == 0) {
+    if (irk == 0) {
       r0[f] = __ldg(a.Win + x);
-    } else if (a.irk < 3) {
+    } else if (irk == 1) {
       r0[f] = __ldg(a.W0 + x);
-      r1[f] = a.T[x];
+    } else if (irk == 2) {
+      r0[f] = __ldg(a.W0 + x);
+      r1[f] = rk_sum(a.Wout[x], __ldg(a.Win + x));  // the stage-1 input, overwritten below
     } else {
       r1[f] = a.T[x];
     }
@@ -113,11 +166,10 @@ __device__ __forceinline__ void rk_store(const VolArgs& a, long long q, const fl
     const long long x = f * n + q;
     const float hf = p ? h[f] + p[f] : h[f];
     float w;
-    if (a.irk == 0) {
-      a.T[x] = fmaf(a.rkb, hf, r0[f]);
+    if (irk < 2) {
       w = fmaf(a.rka, hf, r0[f]);
-    } else if (a.irk < 3) {
-      a.T[x] = fmaf(a.rkb, hf, r1[f]);
+    } else if (irk == 2) {
+      a.T[x] = rk_acc(r1[f], r3, a.rkb, hf);
       w = fmaf(a.rka, hf, r0[f]);
     } else {
       w = fmaf(a.rkb, hf, r1[f]);

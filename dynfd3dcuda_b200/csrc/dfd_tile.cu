@@ -6,12 +6,14 @@
 //     x-3..x+1 (backward), with a y/z halo on the current plane: one 4-D TMA box
 //     (40 y, 12 z, 1 x, 9 fields) per plane, held in a ring of NS plane slots;
 //   - the pointwise streams of the node: 12 metric/media fields, and the RK registers
-//     W0 (stages 1, 2) and T (stages 1..3): TMA boxes (32, 8, 1, n) in a ring of NP slots.
+//     W0 (stages 1, 2), the stage-1 input (stage 2) and T (stage 3): TMA boxes (32, 8, 1, n)
+//     in a ring of NP slots.
 // A dedicated warp issues the copies ahead of the sixteen computing warps (full/empty
 // mbarrier pairs per slot, no block-wide barrier in the loop), so HBM traffic stays in
 // flight while the stencils are evaluated from shared memory with immediate offsets.
 // No node of the box lies in a PML slab or the free-surface rows (dfd_pml.cu and the
-// general kernel take those).  Outputs (Wout, T) are written straight from registers.
+// general kernel take those).  Outputs (Wout, and T at stage 2) are written straight from
+// registers.
 //
 // The kernel is persistent: one CTA per SM takes units (tile column x chunk) from a global
 // counter, and its copy stream runs across unit boundaries, so the next unit's planes
@@ -27,7 +29,7 @@
 namespace dfd {
 
 namespace {
-constexpr int PSLOT = 18 * PB;       // RK registers W0 9 + T 9
+constexpr int PSLOT = 18 * PB;       // RK registers: W0 9, then the stage-1 input or T 9
 constexpr int NS = 8, NP = 3, NQ = 2;  // ring depths (stencil planes, RK registers, unit planes)
 constexpr size_t SMEM_BYTES =
     (size_t)(NS * HSLOT + NP * PSLOT + NQ * QSLOT) * 4 + NQ * sizeof(TileUnit) + 2 * (NS + NP + NQ) * 8 + NQ * 4;
@@ -43,9 +45,11 @@ static_assert((PSLOT * 4) % 128 == 0, "slot alignment");
 // most 96 registers: the 17 warps are spread over the SM's four 16 K-register partitions,
 // five warps on one of them.
 
-// BATCH: the units of the nscen scenarios of tab (an ensemble) in one launch; the
-// parameters mp0, a0, sc0 then describe scenario 0 and give the stage's common values.
-template <int FX, int FY, int FZ, bool BATCH>
+// IRK: the RK stage (a0.irk), a compile-time constant so that each stage's code and
+// register allocation carry only its own RK registers.  BATCH: the units of the nscen
+// scenarios of tab (an ensemble) in one launch; the parameters mp0, a0, sc0 then
+// describe scenario 0 and give the stage's common values.
+template <int FX, int FY, int FZ, int IRK, bool BATCH>
 __global__ void __maxnreg__(96)
     volume_tile_kernel(const __grid_constant__ TileMaps mp0, const __grid_constant__ VolArgs a0,
                        const __grid_constant__ TileSched sc0, const TileScen* __restrict__ tab, int nscen,
@@ -65,8 +69,10 @@ __global__ void __maxnreg__(96)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int XLO = FX == 1 ? -1 : -3;  // first stencil plane relative to x
   constexpr int RZ = FZ == 1 ? 1 : 3;     // row of the tile's first z node inside the halo box
-  const int irk = a0.irk;
-  const bool needW0 = irk == 1 || irk == 2, needT = irk >= 1, usep = needW0 || needT;
+  constexpr int irk = IRK;
+  // pointwise boxes: y0 at stages 1 and 2, a second box at stages 2 (the stage-1 input)
+  // and 3 (the accumulator); stage 0 takes everything from the stencil planes
+  constexpr bool needW0 = irk == 1 || irk == 2, needT = irk >= 2, usep = needW0 || needT;
   const int G = gridDim.x;
   // the PML kernel that follows on the stream touches other nodes only: it may take the
   // SMs that this persistent grid's CTAs leave as they finish
@@ -237,10 +243,10 @@ __global__ void __maxnreg__(96)
         float hv[9];
         if (role == 0) {
           lean_velocity<FX, FY, FZ>(xs0, xs1, xs2, xs3, xs4, cur, g, a.rDH, hv);
-          rk_tile_store<0, 3>(a, n, q, cur, P, hv, damp);
+          rk_tile_store<0, 3, IRK>(a, n, q, cur, P, hv, damp);
         } else {
           lean_stress<FX, FY, FZ>(xs0, xs1, xs2, xs3, xs4, cur, g, a.rDH, hv);
-          rk_tile_store<3, 9>(a, n, q, cur, P, hv, damp);
+          rk_tile_store<3, 9, IRK>(a, n, q, cur, P, hv, damp);
         }
       }
       // release the slots this warp has finished with
@@ -290,13 +296,18 @@ static bool make_map(CUtensorMap* m, const Dims& d, const float* base, int nf, i
   return r == CUDA_SUCCESS;
 }
 
-template <int FX, int FY, int FZ>
-static bool set_smem() {
+template <int FX, int FY, int FZ, int IRK>
+static bool set_smem_k() {
   auto one = [](const void* f) {
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES) == cudaSuccess;
   };
-  return one((const void*)volume_tile_kernel<FX, FY, FZ, false>) &&
-         one((const void*)volume_tile_kernel<FX, FY, FZ, true>);
+  return one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, false>) &&
+         one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, true>);
+}
+template <int FX, int FY, int FZ>
+static bool set_smem() {
+  return set_smem_k<FX, FY, FZ, 0>() && set_smem_k<FX, FY, FZ, 1>() && set_smem_k<FX, FY, FZ, 2>() &&
+         set_smem_k<FX, FY, FZ, 3>();
 }
 
 // 3-D map over the 12 metric / media planes (py, nz, 12) with box (bw, bh, 12)
@@ -384,17 +395,20 @@ TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid) {
   return s;
 }
 
-TileMaps tile_maps(const TileCtx& tc, int bin) {
+// maps of stage irk with stencil input buffer bin; the second pointwise box reads, at
+// stage 2, the stage-1 input (the buffer the stage overwrites) and otherwise the accumulator
+TileMaps tile_maps(const TileCtx& tc, int bin, int irk) {
   TileMaps mp;
   memset(&mp, 0, sizeof mp);
+  const int p2 = irk == 2 ? stage_out(2) : 3;
   mp.win = tc.halo[bin];
   mp.w0 = tc.centre[0];
-  mp.t = tc.centre[3];
+  mp.t = tc.centre[p2];
   mp.plane = tc.plane;
   for (int f = 0; f < 6; f++) mp.aux[f] = tc.aux[f];
   mp.win_s = tc.halo_s[bin];
   mp.w0_s = tc.centre_s[0];
-  mp.t_s = tc.centre_s[3];
+  mp.t_s = tc.centre_s[p2];
   mp.plane_s = tc.plane_s;
   mp.auxy_s[0] = tc.auxy_s[0];
   mp.auxy_s[1] = tc.auxy_s[1];
@@ -403,12 +417,14 @@ TileMaps tile_maps(const TileCtx& tc, int bin) {
 
 template <int FX, int FY, int FZ>
 static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
-  const TileMaps mp = tile_maps(tc, bin);
+  const TileMaps mp = tile_maps(tc, bin, a.irk);
   int grid = 0;
   TileSched sc = tile_plan(lo, hi, tc.nsm, &grid);
   sc.drill = tc.drill;
-  volume_tile_kernel<FX, FY, FZ, false>
-      <<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, nullptr, 1, sc.nunits, tc.err, tc.sched);
+#define DFD_L(K) \
+  volume_tile_kernel<FX, FY, FZ, K, false><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, nullptr, 1, sc.nunits, tc.err, tc.sched)
+  DFD_BY_STAGE(a.irk, DFD_L);
+#undef DFD_L
 }
 
 // true when the tiled kernel can take the box lo..hi
@@ -420,8 +436,10 @@ bool tile_feasible(const TileCtx* tc, const VolArgs& a, int3 lo, int3 hi) {
 template <int FX, int FY, int FZ>
 static void launch_tb(const TileScen& f, const TileScen* tab, int n, int nunits, int grid, int* err, int* sched,
                       cudaStream_t s) {
-  volume_tile_kernel<FX, FY, FZ, true>
-      <<<grid, NTOT, SMEM_BYTES, s>>>(f.mp, f.u.a, f.u.sc, tab, n, nunits, err, sched);
+#define DFD_L(K) \
+  volume_tile_kernel<FX, FY, FZ, K, true><<<grid, NTOT, SMEM_BYTES, s>>>(f.mp, f.u.a, f.u.sc, tab, n, nunits, err, sched)
+  DFD_BY_STAGE(f.u.a.irk, DFD_L);
+#undef DFD_L
 }
 // every scenario of an ensemble in one persistent launch (units numbered across them)
 void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,

@@ -112,20 +112,24 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
 
 // RK4 register update of fields F0..F1-1 of node q with right-hand side hv, then the
 // sponge factor (rk4.cu:20-33, cerjan.cu:166-200): step-start values from the stencil
-// input at stage 0, the RK registers from the pointwise slot P at stages 1..3.
-template <int F0, int F1>
+// input at stage 0, from the pointwise slot P at stages 1 and 2; at stage 2 the slot's
+// second box holds the stage-1 input, from which, with the stage input, the accumulator
+// is formed (rk_sum, rk_acc); at stage 3 that box holds the accumulator.  IRK: the
+// stage (the kernels are compiled per stage).
+template <int F0, int F1, int IRK>
 __device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, long long q, const float* cur,
                                               const float* P, const float* hv, float damp) {
+  const float r3 = IRK == 2 ? rk_r3(damp) : 0.0f;
 #pragma unroll
   for (int f = F0; f < F1; f++) {
     const long long x = f * n + q;
     float w;
-    if (a.irk == 0) {
-      const float w0 = cur[f * HBOX];
-      a.T[x] = fmaf(a.rkb, hv[f], w0);
-      w = fmaf(a.rka, hv[f], w0);
-    } else if (a.irk < 3) {
-      a.T[x] = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
+    if (IRK == 0) {
+      w = fmaf(a.rka, hv[f], cur[f * HBOX]);
+    } else if (IRK == 1) {
+      w = fmaf(a.rka, hv[f], P[f * PB]);
+    } else if (IRK == 2) {
+      a.T[x] = rk_acc(rk_sum(P[(9 + f) * PB], cur[f * HBOX]), r3, a.rkb, hv[f]);
       w = fmaf(a.rka, hv[f], P[f * PB]);
     } else {
       w = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);

@@ -46,7 +46,7 @@ __device__ __forceinline__ void traction(const float* __restrict__ W, const floa
 // General node update: every boundary treatment (PML faces, free-surface rows and
 // traction image, sponge).  Used for the shell of the domain outside the interior box;
 // TOP = false leaves out the free-surface terms (nodes below the top three rows).
-template <int FX, int FY, int FZ, bool TOP>
+template <int FX, int FY, int FZ, bool TOP, int IRK>
 __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, int j, int k) {
   const Dims& d = a.d;
   int i1 = i + 3, j1 = j + 3, k1 = k + 3;
@@ -87,7 +87,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
     }
     const int fc = px1 ? 0 : 1;
     const long long st = pml_fstride(d, fc), qa = pml_index(d, fc, i, j, k);
-    pml_face(a, fc, qa, st, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D,
+    pml_face<IRK>(a, fc, qa, st, rb1, __ldg(a.Bx + i), __ldg(a.Dpx + i), __ldg(a.Apx + i), D,
              top ? dz : nullptr, ez0, ez1, ez2, lam, mu, p);
   }
   // ---- y ----
@@ -106,7 +106,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
     }
     const int fc = py1 ? 2 : 3;
     const long long st = pml_fstride(d, fc), qa = pml_index(d, fc, i, j, k);
-    pml_face(a, fc, qa, st, rb2, __ldg(a.By + j), __ldg(a.Dpy + j), __ldg(a.Apy + j), D,
+    pml_face<IRK>(a, fc, qa, st, rb2, __ldg(a.By + j), __ldg(a.Dpy + j), __ldg(a.Apy + j), D,
              top ? dz : nullptr, ez0, ez1, ez2, lam, mu, p);
   }
   // ---- z ----
@@ -154,7 +154,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
   if (pz1 || pz2) {
     const int fc = pz1 ? 4 : 5;
     const long long st = pml_fstride(d, fc), qa = pml_index(d, fc, i, j, k);
-    pml_face(a, fc, qa, st, rb3, __ldg(a.Bz + k), __ldg(a.Dpz + k), __ldg(a.Apz + k), Dz_plain, nullptr,
+    pml_face<IRK>(a, fc, qa, st, rb3, __ldg(a.Bz + k), __ldg(a.Dpz + k), __ldg(a.Apz + k), Dz_plain, nullptr,
              ez0, ez1, ez2, lam, mu, p);
   }
   // ---- traction image for the momentum equation on the top three rows (wave.cu:398-487)
@@ -182,7 +182,7 @@ __device__ __forceinline__ void volume_point_general(const VolArgs& a, int i, in
   // ---- RK4 registers and Cerjan sponge
   float damp = 1.0f;
   if (a.dampx) damp = fminf(fminf(__ldg(a.dampx + i1), __ldg(a.dampy + j1)), __ldg(a.dampz + k1));
-  rk_store(a, q, h, p, damp);
+  rk_store<IRK>(a, q, h, p, damp);
 }
 
 
@@ -199,8 +199,8 @@ constexpr int SHELL_THREADS = 128;
 
 // block blk of the shell grid of one scenario: of the boxes below the free-surface rows
 // (TOP = false, blk counted from box 0) or of the free-surface boxes (TOP, blk counted
-// from box ntop)
-template <int FX, int FY, int FZ, bool TOP>
+// from box ntop); IRK: the stage (compiled per stage for the free-surface rows), or -1
+template <int FX, int FY, int FZ, bool TOP, int IRK>
 __device__ __forceinline__ void volume_shell_body(const VolArgs& a, const Boxes& bx, int blk) {
   int b = TOP ? bx.ntop : 0;
   const int bend = TOP ? bx.n : bx.ntop;
@@ -224,15 +224,15 @@ __device__ __forceinline__ void volume_shell_body(const VolArgs& a, const Boxes&
     i = bi;
     if (i >= ni || j >= nj || k >= nk) return;
   }
-  volume_point_general<FX, FY, FZ, TOP>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
+  volume_point_general<FX, FY, FZ, TOP, IRK>(a, bx.lo[b][0] + i, bx.lo[b][1] + j, bx.lo[b][2] + k);
 }
-template <int FX, int FY, int FZ, bool TOP>
+template <int FX, int FY, int FZ, bool TOP, int IRK>
 __global__ void __launch_bounds__(SHELL_THREADS, 3)
     volume_shell_kernel(const __grid_constant__ VolArgs a, const __grid_constant__ Boxes bx) {
-  volume_shell_body<FX, FY, FZ, TOP>(a, bx, blockIdx.x);
+  volume_shell_body<FX, FY, FZ, TOP, IRK>(a, bx, blockIdx.x);
 }
 // all scenarios of an ensemble in one launch: scenario s owns blocks [start[s], start[s+1])
-template <int FX, int FY, int FZ, bool TOP>
+template <int FX, int FY, int FZ, bool TOP, int IRK>
 __global__ void __launch_bounds__(SHELL_THREADS, 3)
     volume_shell_batch(const VolArgs* __restrict__ tab, const Boxes* __restrict__ boxes,
                        const int* __restrict__ start, int n) {
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(SHELL_THREADS, 3)
   stage_args(sa, tab + sc);
   stage_args(sb, boxes + sc);
   __syncthreads();
-  volume_shell_body<FX, FY, FZ, TOP>(*sa, *sb, loc);
+  volume_shell_body<FX, FY, FZ, TOP, IRK>(*sa, *sb, loc);
 }
 
 // Interior kernel: no PML (beta = 1, no auxiliary state), no free-surface rows.  Each
@@ -285,7 +285,7 @@ __device__ __forceinline__ void interior_point(const VolArgs& a, long long q, fl
   DFD_AXIS(FZ, a.d.py, 6)
 #undef DFD_AXIS
   const float hv[9] = {h0, h1, h2, h3, h4, h5, h6, h7, h8};
-  rk_store(a, q, hv, nullptr, damp);
+  rk_store<-1>(a, q, hv, nullptr, damp);
 }
 
 template <int FX, int FY, int FZ>
@@ -420,30 +420,39 @@ static long long launch_flags(const VolArgs& a, cudaStream_t s, cudaStream_t s_s
     cudaStreamWaitEvent(s_shell, *fork, 0);
   }
   const int below = pl.bx.start[pl.bx.ntop], above = pl.bx.start[pl.bx.n] - below;
-  if (below > 0) volume_shell_kernel<FX, FY, FZ, false><<<below, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
-  if (above > 0) volume_shell_kernel<FX, FY, FZ, true><<<above, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
+  if (below > 0) volume_shell_kernel<FX, FY, FZ, false, -1><<<below, SHELL_THREADS, 0, s_shell>>>(a, pl.bx);
+  if (above > 0) {
+#define DFD_L(K) volume_shell_kernel<FX, FY, FZ, true, K><<<above, SHELL_THREADS, 0, s_shell>>>(a, pl.bx)
+    DFD_BY_STAGE(a.irk, DFD_L);
+#undef DFD_L
+  }
   return pl.nodes;
 }
 
 template <int FX, int FY, int FZ>
 static void shell_batch_t(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, bool top,
-                          cudaStream_t s) {
-  if (top) volume_shell_batch<FX, FY, FZ, true><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n);
-  else volume_shell_batch<FX, FY, FZ, false><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n);
+                          int irk, cudaStream_t s) {
+  if (top) {
+#define DFD_L(K) volume_shell_batch<FX, FY, FZ, true, K><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n)
+    DFD_BY_STAGE(irk, DFD_L);
+#undef DFD_L
+  } else {
+    volume_shell_batch<FX, FY, FZ, false, -1><<<blocks, SHELL_THREADS, 0, s>>>(tab, boxes, start, n);
+  }
 }
 void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, int FX, int FY,
-                        int FZ, bool top, cudaStream_t s) {
+                        int FZ, bool top, int irk, cudaStream_t s) {
   if (blocks <= 0) return;
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: shell_batch_t<-1, -1, -1>(tab, boxes, start, n, blocks, top, s); break;
-    case 1: shell_batch_t<-1, -1, 1>(tab, boxes, start, n, blocks, top, s); break;
-    case 2: shell_batch_t<-1, 1, -1>(tab, boxes, start, n, blocks, top, s); break;
-    case 3: shell_batch_t<-1, 1, 1>(tab, boxes, start, n, blocks, top, s); break;
-    case 4: shell_batch_t<1, -1, -1>(tab, boxes, start, n, blocks, top, s); break;
-    case 5: shell_batch_t<1, -1, 1>(tab, boxes, start, n, blocks, top, s); break;
-    case 6: shell_batch_t<1, 1, -1>(tab, boxes, start, n, blocks, top, s); break;
-    default: shell_batch_t<1, 1, 1>(tab, boxes, start, n, blocks, top, s); break;
+    case 0: shell_batch_t<-1, -1, -1>(tab, boxes, start, n, blocks, top, irk, s); break;
+    case 1: shell_batch_t<-1, -1, 1>(tab, boxes, start, n, blocks, top, irk, s); break;
+    case 2: shell_batch_t<-1, 1, -1>(tab, boxes, start, n, blocks, top, irk, s); break;
+    case 3: shell_batch_t<-1, 1, 1>(tab, boxes, start, n, blocks, top, irk, s); break;
+    case 4: shell_batch_t<1, -1, -1>(tab, boxes, start, n, blocks, top, irk, s); break;
+    case 5: shell_batch_t<1, -1, 1>(tab, boxes, start, n, blocks, top, irk, s); break;
+    case 6: shell_batch_t<1, 1, -1>(tab, boxes, start, n, blocks, top, irk, s); break;
+    default: shell_batch_t<1, 1, 1>(tab, boxes, start, n, blocks, top, irk, s); break;
   }
 }
 
