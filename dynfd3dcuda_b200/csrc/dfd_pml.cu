@@ -159,7 +159,7 @@ __device__ __forceinline__ void role_face(const VolArgs& a, int face, bool stage
     } else if (irk == 1) {
       x[2 * b9] = fmaf(a.rka, h, s2[m]);
     } else if (irk == 2) {
-      x[2 * b9] = rk_acc(rk_sum(y1[m], w[m]), 1.0f / 3.0f, a.rkb, h);
+      x[2 * b9] = rk_acc(s2[m], rk_sum(s2[m], y1[m], w[m], 1.0f), a.rkb, h);
       x[b9] = fmaf(a.rka, h, s2[m]);
     } else {
       x[0] = fmaf(a.rkb, h, s2[m]);

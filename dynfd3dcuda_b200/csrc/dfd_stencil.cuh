@@ -33,17 +33,22 @@ __device__ __forceinline__ void axis_terms(const float* d, float e0, float e1, f
   } while (0)
 
 // Classic RK4 without storing the accumulator at stages 0 and 1.  With step-start value y0
-// and stage inputs y1 = y0 + (dt/2) k1, y2 = y0 + (dt/2) k2, the sum
-//   (y1 + 2 y2) / 3 = y0 + (dt/6) k1 + (dt/3) k2
-// is the accumulator after stage 1, so after stage 2 it is (y1 + 2 y2) / 3 + rkb h with
+// and stage inputs y1 = y0 + (dt/2) k1, y2 = y0 + (dt/2) k2,
+//   y0 + (dt/6) k1 + (dt/3) k2 = y0 + (u + 2 v) / 3,   u = y1 - y0, v = y2 - y0,
+// is the accumulator after stage 1, so after stage 2 it is y0 + (u + 2 v) / 3 + rkb h with
 // rkb h = (dt/3) k3.  Stages 0 and 1 therefore write no accumulator and stage 1 reads
 // none; stage 2 re-reads its node's stage-1 input (the buffer it is about to overwrite)
 // and writes the accumulator that stage 3 completes (rk4.cu:20-33 forms the same sums term
-// by term).  Stored stage inputs carry the sponge factor damp, hence the factor
-// r3 = 1 / (3 damp).
-__device__ __forceinline__ float rk_sum(float y1, float y2) { return fmaf(2.0f, y2, y1); }
-__device__ __forceinline__ float rk_acc(float s, float r3, float rkb, float h) { return fmaf(rkb, h, s * r3); }
-__device__ __forceinline__ float rk_r3(float damp) { return __fdividef(1.0f / 3.0f, damp); }
+// by term).  The increments, not y0, are scaled by the rounded 1/3: (y1 + 2 y2) / 3 would
+// scale y0 itself by 1 + 3e-8 every step.  Stored stage inputs carry the sponge factor
+// damp, so they are scaled back by rd = 1 / damp (exactly 1 outside the sponge).
+__device__ __forceinline__ float rk_rd(float damp) { return damp == 1.0f ? 1.0f : __frcp_rn(damp); }
+__device__ __forceinline__ float rk_sum(float y0, float y1, float y2, float rd) {
+  return fmaf(2.0f, fmaf(y2, rd, -y0), fmaf(y1, rd, -y0));  // u + 2 v
+}
+__device__ __forceinline__ float rk_acc(float y0, float s, float rkb, float h) {
+  return fmaf(rkb, h, fmaf(s, 1.0f / 3.0f, y0));
+}
 
 // The ADE state of a PML face is pointwise, so its three 9-field blocks cycle like the
 // volume buffers with the accumulator in the block the stage no longer needs:
@@ -117,7 +122,7 @@ __device__ __forceinline__ void pml_update(const VolArgs& a, int face, long long
     } else if (irk == 1) {
       x[2 * b9] = fmaf(a.rka, h, ps.s[f]);
     } else if (irk == 2) {
-      x[2 * b9] = rk_acc(rk_sum(ps.y1[f], ps.w[f]), 1.0f / 3.0f, a.rkb, h);
+      x[2 * b9] = rk_acc(ps.s[f], rk_sum(ps.s[f], ps.y1[f], ps.w[f], 1.0f), a.rkb, h);
       x[b9] = fmaf(a.rka, h, ps.s[f]);
     } else {
       x[0] = fmaf(a.rkb, h, ps.s[f]);
@@ -145,7 +150,7 @@ __device__ __forceinline__ void rk_store(const VolArgs& a, long long q, const fl
                                          float damp) {
   const int irk = IRK >= 0 ? IRK : a.irk;
   const long long n = a.d.nxyz;
-  const float r3 = irk == 2 ? rk_r3(damp) : 0.0f;
+  const float rd = irk == 2 ? rk_rd(damp) : 1.0f;
   float r0[9], r1[9];
 #pragma unroll
   for (int f = 0; f < 9; f++) {
@@ -156,7 +161,7 @@ __device__ __forceinline__ void rk_store(const VolArgs& a, long long q, const fl
       r0[f] = __ldg(a.W0 + x);
     } else if (irk == 2) {
       r0[f] = __ldg(a.W0 + x);
-      r1[f] = rk_sum(a.Wout[x], __ldg(a.Win + x));  // the stage-1 input, overwritten below
+      r1[f] = rk_sum(r0[f], a.Wout[x], __ldg(a.Win + x), rd);  // the stage-1 input, overwritten below
     } else {
       r1[f] = a.T[x];
     }
@@ -169,7 +174,7 @@ __device__ __forceinline__ void rk_store(const VolArgs& a, long long q, const fl
     if (irk < 2) {
       w = fmaf(a.rka, hf, r0[f]);
     } else if (irk == 2) {
-      a.T[x] = rk_acc(r1[f], r3, a.rkb, hf);
+      a.T[x] = rk_acc(r0[f], r1[f], a.rkb, hf);
       w = fmaf(a.rka, hf, r0[f]);
     } else {
       w = fmaf(a.rkb, hf, r1[f]);

@@ -113,13 +113,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
 // RK4 register update of fields F0..F1-1 of node q with right-hand side hv, then the
 // sponge factor (rk4.cu:20-33, cerjan.cu:166-200): step-start values from the stencil
 // input at stage 0, from the pointwise slot P at stages 1 and 2; at stage 2 the slot's
-// second box holds the stage-1 input, from which, with the stage input, the accumulator
-// is formed (rk_sum, rk_acc); at stage 3 that box holds the accumulator.  IRK: the
+// second box holds the stage-1 input, from which, with y0 and the stage input, the
+// accumulator is formed (rk_sum, rk_acc); at stage 3 that box holds the accumulator.  IRK: the
 // stage (the kernels are compiled per stage).
 template <int F0, int F1, int IRK>
 __device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, long long q, const float* cur,
                                               const float* P, const float* hv, float damp) {
-  const float r3 = IRK == 2 ? rk_r3(damp) : 0.0f;
+  const float rd = IRK == 2 ? rk_rd(damp) : 1.0f;
 #pragma unroll
   for (int f = F0; f < F1; f++) {
     const long long x = f * n + q;
@@ -129,8 +129,9 @@ __device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, lon
     } else if (IRK == 1) {
       w = fmaf(a.rka, hv[f], P[f * PB]);
     } else if (IRK == 2) {
-      a.T[x] = rk_acc(rk_sum(P[(9 + f) * PB], cur[f * HBOX]), r3, a.rkb, hv[f]);
-      w = fmaf(a.rka, hv[f], P[f * PB]);
+      const float y0 = P[f * PB];
+      a.T[x] = rk_acc(y0, rk_sum(y0, P[(9 + f) * PB], cur[f * HBOX], rd), a.rkb, hv[f]);
+      w = fmaf(a.rka, hv[f], y0);
     } else {
       w = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
     }
