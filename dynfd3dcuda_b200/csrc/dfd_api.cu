@@ -202,13 +202,25 @@ static int cuda_check(dfd_ctx* c, cudaError_t e, const char* where) {
     if (_r) return _r;                                               \
   } while (0)
 
+// Host-to-device copies and clears go through the context's stepping stream s0 and are
+// complete when the call returns.  A plain cudaMemcpy from pageable host memory (and a
+// plain cudaMemset) runs on the legacy default stream, may still be in flight when it
+// returns, and is not ordered with the non-blocking context streams: a kernel launched on
+// s0 right after it could read the buffer before the copy lands.
+static cudaError_t h2d(dfd_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->s0);
+  return e == cudaSuccess ? cudaStreamSynchronize(ctx->s0) : e;
+}
+
 template <typename T>
 static int dalloc(dfd_ctx* ctx, T** p, size_t n) {
   void* v = nullptr;
   cudaError_t e = cudaMalloc(&v, n * sizeof(T) + 16);
   if (e != cudaSuccess) return cuda_check(ctx, e, "cudaMalloc");
   ctx->allocs.push_back(v);
-  cudaMemset(v, 0, n * sizeof(T) + 16);
+  e = cudaMemsetAsync(v, 0, n * sizeof(T) + 16, ctx->s0);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->s0);
+  if (e != cudaSuccess) return cuda_check(ctx, e, "cudaMemset");
   *p = (T*)v;
   return DFD_OK;
 }
@@ -459,13 +471,13 @@ int dfd_precompute(dfd_ctx* ctx) {
   CK(cudaMalloc(&dfx, sizeof(double) * ctx->fx.size()));
   CK(cudaMalloc(&dfy, sizeof(double) * ctx->fy.size()));
   CK(cudaMalloc(&dfz, sizeof(double) * ctx->fz.size()));
-  CK(cudaMemcpy(dxl, ctx->xl.data(), sizeof(double) * ctx->xl.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dfx, ctx->fx.data(), sizeof(double) * ctx->fx.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dfy, ctx->fy.data(), sizeof(double) * ctx->fy.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dfz, ctx->fz.data(), sizeof(double) * ctx->fz.size(), cudaMemcpyHostToDevice));
+  CK(h2d(ctx, dxl, ctx->xl.data(), sizeof(double) * ctx->xl.size()));
+  CK(h2d(ctx, dfx, ctx->fx.data(), sizeof(double) * ctx->fx.size()));
+  CK(h2d(ctx, dfy, ctx->fy.data(), sizeof(double) * ctx->fy.size()));
+  CK(h2d(ctx, dfz, ctx->fz.data(), sizeof(double) * ctx->fz.size()));
   if (!ctx->layers.empty()) {
     CK(cudaMalloc(&dlay, sizeof(float) * ctx->layers.size()));
-    CK(cudaMemcpy(dlay, ctx->layers.data(), sizeof(float) * ctx->layers.size(), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, dlay, ctx->layers.data(), sizeof(float) * ctx->layers.size()));
   }
   GridArgs g;
   g.d = d; g.xl = dxl; g.fx = dfx; g.fy = dfy; g.fz = dfz; g.layers = dlay;
@@ -512,17 +524,17 @@ int dfd_precompute(dfd_ctx* ctx) {
     pml_profile(&p, len[a], lo, hi, A, B, D);
     rb.resize(B.size());
     for (size_t i = 0; i < B.size(); i++) rb[i] = 1.0f / B[i];
-    CK(cudaMemcpy(ctx->Ap[a], A.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->B[a], B.data(), sizeof(float) * B.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->Dp[a], D.data(), sizeof(float) * D.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->rB[a], rb.data(), sizeof(float) * rb.size(), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, ctx->Ap[a], A.data(), sizeof(float) * A.size()));
+    CK(h2d(ctx, ctx->B[a], B.data(), sizeof(float) * B.size()));
+    CK(h2d(ctx, ctx->Dp[a], D.data(), sizeof(float) * D.size()));
+    CK(h2d(ctx, ctx->rB[a], rb.data(), sizeof(float) * rb.size()));
   }
   if (p.use_cerjan) {
     int np[3] = {d.nx, d.ny, d.nz};
     for (int a = 0; a < 3; a++) {
       std::vector<float> prof;
       cerjan_profile(&p, np[a], !(a == 1 && !ylo), !(a == 2 && fs) && !(a == 1 && !yhi), prof);
-      CK(cudaMemcpy(ctx->damp[a], prof.data(), sizeof(float) * prof.size(), cudaMemcpyHostToDevice));
+      CK(h2d(ctx, ctx->damp[a], prof.data(), sizeof(float) * prof.size()));
     }
   }
   if (fs) launch_wave_free(d, ctx->M, ctx->B[0], ctx->B[1], ctx->B[2], ctx->mVx2Vz, ctx->mVy2Vz, s);
@@ -926,12 +938,14 @@ int dfd_synchronize(dfd_ctx* ctx) {
 
 // dense host fields (nf, nx, nz, ny) <-> pitched device fields (nf, nx, nz, py) at offset oy:
 // all nf*nx*nz rows share one pitch, so one 2-D copy moves them
+// dense reference layout <-> padded rows, on the stepping stream, complete on return
 static int volume_copy(dfd_ctx* ctx, float* host, float* dev, int nf, bool to_host) {
   const Dims& d = ctx->d;
   size_t w = sizeof(float) * d.ny, hp = w, dp = sizeof(float) * d.py;
   size_t rows = (size_t)nf * d.nx * d.nz;
-  if (to_host) CK(cudaMemcpy2D(host, hp, dev + d.oy, dp, w, rows, cudaMemcpyDeviceToHost));
-  else CK(cudaMemcpy2D(dev + d.oy, dp, host, hp, w, rows, cudaMemcpyHostToDevice));
+  if (to_host) CK(cudaMemcpy2DAsync(host, hp, dev + d.oy, dp, w, rows, cudaMemcpyDeviceToHost, ctx->s0));
+  else CK(cudaMemcpy2DAsync(dev + d.oy, dp, host, hp, w, rows, cudaMemcpyHostToDevice, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
   return DFD_OK;
 }
 
@@ -1199,7 +1213,7 @@ int dfd_set_guess_net(dfd_ctx* ctx, const float* w, int n) {
   if (!ctx || (w && n != DFD_MLP_PARAMS) || (!w && n != 0)) return DFD_ERR_PARAM;
   cudaSetDevice(ctx->device);
   CK(cudaStreamSynchronize(ctx->s0));
-  if (w) CK(cudaMemcpy(ctx->guess_net, w, sizeof(float) * n, cudaMemcpyHostToDevice));
+  if (w) CK(h2d(ctx, ctx->guess_net, w, sizeof(float) * n));
   ctx->p.rs_guess = w ? 1 : 0;
   // the switch is baked into the step graphs: rebuild them
   for (auto& g : ctx->graph)
@@ -1300,7 +1314,8 @@ int dfd_newton_record(dfd_ctx* ctx, int capacity, int every) {
     CK(cudaMalloc(&ctx->rec, sizeof(float) * 5 * (size_t)capacity));
     ctx->rec_cap = capacity;
   }
-  CK(cudaMemset(ctx->rec_n, 0, sizeof(unsigned)));
+  CK(cudaMemsetAsync(ctx->rec_n, 0, sizeof(unsigned), ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
   // the recording buffer is baked into the step graphs: rebuild them
   for (auto& g : ctx->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
@@ -1317,7 +1332,8 @@ int dfd_newton_samples(dfd_ctx* ctx, float* host, int max, int* n) {
   m = std::min(m, max);
   if (m > 0) CK(cudaMemcpy(host, ctx->rec, sizeof(float) * 5 * (size_t)m, cudaMemcpyDeviceToHost));
   *n = m;
-  CK(cudaMemset(ctx->rec_n, 0, sizeof(unsigned)));
+  CK(cudaMemsetAsync(ctx->rec_n, 0, sizeof(unsigned), ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
   return DFD_OK;
 }
 
@@ -1633,7 +1649,11 @@ static int ens_upload(dfd_ens* e, T** dst, const std::vector<T>& v) {
   void* p = nullptr;
   ECK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(v.size(), 1)));
   e->allocs.push_back(p);
-  if (!v.empty()) ECK(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  if (!v.empty()) {
+    // on the ensemble's stream and complete on return (see h2d)
+    ECK(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, e->s0));
+    ECK(cudaStreamSynchronize(e->s0));
+  }
   *dst = (T*)p;
   return DFD_OK;
 }
@@ -1819,7 +1839,9 @@ int dfd_ens_create(dfd_ctx* const* scenarios, int n, dfd_ens** out) {
   cudaEventCreateWithFlags(&e->ev_join2, cudaEventDisableTiming);
   void* p = nullptr;
   if (cudaMalloc(&p, 6 * sizeof(int)) != cudaSuccess) return done(DFD_ERR_CUDA);
-  cudaMemset(p, 0, 6 * sizeof(int));
+  // cleared on the ensemble's stream (a plain cudaMemset is not ordered with it)
+  if (cudaMemsetAsync(p, 0, 6 * sizeof(int), e->s0) != cudaSuccess || cudaStreamSynchronize(e->s0) != cudaSuccess)
+    return done(DFD_ERR_CUDA);
   e->it_dev = (int*)p;
   e->sched = e->it_dev + 1;  // unit and finished-CTA counters of the interior, then the PML kernel
   e->err = e->it_dev + 5;
