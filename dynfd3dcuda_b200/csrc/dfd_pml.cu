@@ -22,17 +22,32 @@
 namespace dfd {
 
 namespace {
-// W0 9, the stage-1 input or T 9, then the face's ADE state: the current value 9, y0 or the
-// accumulator 9, y1 9 (aux_block)
-constexpr int PSLOT_M = 45 * PB;
-constexpr int MS = 6, MP = 2, MQ = 2;  // ring depths (stencil planes, pointwise planes, unit planes)
 constexpr int PCW = TK;                 // computing warps: one per row of the tile, all nine fields
 constexpr int PTOT = PCW * 32 + 32;     // plus one copy-issuing warp
-constexpr size_t PML_SMEM =
-    (size_t)(MS * HSLOT + MP * PSLOT_M + MQ * QSLOT) * 4 + MQ * sizeof(TileUnit) + 2 * (MS + MP + MQ) * 8 + MQ * 4;
-static_assert(PML_SMEM <= 232448, "PML ring exceeds the shared memory of one CTA");
-static_assert((PSLOT_M * 4) % 128 == 0, "slot alignment");
 }  // namespace
+
+// Ring shapes of stage IRK.  A pointwise slot holds, in this order, W0 (stages 1, 2), the
+// second box (stage 2: the stage-1 input; stage 3: the accumulator) and the ADE blocks of
+// the unit's own face that the stage reads (the current value, then y0 or the accumulator,
+// then y1: aux_block): 9, 27, 45 and 27 fields at stages 0..3.  The shared memory that
+// the smaller slots leave goes to more slots: the stencil ring (5 planes in use) then runs
+// 4, 3, 1 and 3 planes ahead.
+template <int IRK>
+struct PmlRing {
+  static constexpr bool W0 = IRK == 1 || IRK == 2, T = IRK >= 2;
+  static constexpr int NAUX = IRK == 0 ? 9 : IRK == 2 ? 27 : 18;  // ADE fields staged per plane
+  static constexpr int TOFF = W0 ? 9 : 0;                          // second box in the slot
+  static constexpr int AOFF = 9 * ((W0 ? 1 : 0) + (T ? 1 : 0));    // ADE blocks in the slot
+  static constexpr int PF = AOFF + NAUX;                           // fields per slot
+  static constexpr int PSLOT = PF * PB;
+  static constexpr int MS = IRK == 0 ? 9 : IRK == 2 ? 6 : 8;      // stencil planes
+  static constexpr int MP = IRK == 0 ? 4 : 2;                      // pointwise planes
+  static constexpr int MQ = 2;                                     // unit-plane sets
+  static constexpr size_t SMEM =
+      (size_t)(MS * HSLOT + MP * PSLOT + MQ * QSLOT) * 4 + MQ * sizeof(TileUnit) + 2 * (MS + MP + MQ) * 8 + MQ * 4;
+  static_assert(SMEM <= 232448, "PML ring exceeds the shared memory of one CTA");
+  static_assert((PSLOT * 4) % 128 == 0, "slot alignment");
+};
 
 // tile origin, x range, own face (-1: none), node bounds (j < jhi, k < khi) and shape
 // (strip: 16 x 16, else 32 x 8) of local unit lu
@@ -297,8 +312,8 @@ __device__ __forceinline__ void pml_node(const VolArgs& a, int PW, const float* 
 // fields (the lean interior path for a warp whose nodes lie in no PML slab).  The nine warps
 // allow 168 registers a thread (three warps on one of the SM's four 16 K-register
 // partitions), what the ADE path needs without spilling.  Rings as in the interior
-// kernel, with shallower stencil and pointwise rings: a pointwise slot also holds the own
-// face's ADE state, so it is 2.5 times larger.
+// kernel, with shallower rings (PmlRing): a pointwise slot also holds the own face's ADE
+// state.
 // IRK: the RK stage, compiled per stage as in the interior kernel.  BATCH: the units of
 // the nscen scenarios of tab in one launch; mp0, a0, sc0 describe scenario 0 and give the
 // stage's common values.
@@ -307,10 +322,12 @@ __global__ void __maxnreg__(168)
     volume_pml_kernel(const __grid_constant__ TileMaps mp0, const __grid_constant__ VolArgs a0,
                       const __grid_constant__ TileSched sc0, const TileScen* __restrict__ tab, int nscen, int nunits,
                       int* err, int* sched) {
+  using RG = PmlRing<IRK>;
+  constexpr int MS = RG::MS, MP = RG::MP, MQ = RG::MQ, PSLOT = RG::PSLOT;
   extern __shared__ __align__(1024) unsigned char smraw[];
   float* win = reinterpret_cast<float*>(smraw);
   float* pw = win + MS * HSLOT;
-  float* qs = pw + MP * PSLOT_M;
+  float* qs = pw + MP * PSLOT;
   TileUnit* uarg = reinterpret_cast<TileUnit*>(qs + MQ * QSLOT);
   uint64_t* full_w = reinterpret_cast<uint64_t*>(uarg + MQ);
   uint64_t* empty_w = full_w + MS;
@@ -325,8 +342,8 @@ __global__ void __maxnreg__(168)
   constexpr int irk = IRK;
   // pointwise boxes as in the interior kernel: y0 at stages 1 and 2, the second box (the
   // stage-1 input, the accumulator) at stages 2 and 3
-  constexpr bool needW0 = irk == 1 || irk == 2, needT = irk >= 2;
-  constexpr int naux = irk == 0 ? 9 : irk == 2 ? 27 : 18;  // ADE fields staged per plane
+  constexpr bool needW0 = RG::W0, needT = RG::T;
+  constexpr int naux = RG::NAUX;
   const int G = gridDim.x;
 
   if (threadIdx.x == 0) {
@@ -393,13 +410,13 @@ __global__ void __maxnreg__(168)
         if (m < 4 || !usep) continue;
         if (pcount >= MP && !(ok = mbar_wait(empty_p + pr.slot, pr.phase ^ 1))) break;
         uint64_t* b = full_p + pr.slot;
-        float* dst = pw + pr.slot * PSLOT_M;
+        float* dst = pw + pr.slot * PSLOT;
         const int i = pu.ib + (m - 4);
         mbar_expect_tx(b, ptx);
         if (needW0) tma_load4(dst, m_w0, cp0, cp1, i + 3, 0, b);
-        if (needT) tma_load4(dst + 9 * PB, m_t, cp0, cp1, i + 3, 0, b);
+        if (needT) tma_load4(dst + RG::TOFF * PB, m_t, cp0, cp1, i + 3, 0, b);
         for (int nb = 0; nb * 9 < na; nb++)
-          tma_load4(dst + (18 + 9 * nb) * PB, m_aux, ac0, ac1, i - aoff, 9 * aux_block(irk, nb), b);
+          tma_load4(dst + (RG::AOFF + 9 * nb) * PB, m_aux, ac0, ac1, i - aoff, 9 * aux_block(irk, nb), b);
         pr.next<MP>();
         pcount++;
       }
@@ -476,7 +493,7 @@ __global__ void __maxnreg__(168)
         return;
       }
       const int i = pu.ib + s;
-      const float* P = pw + pr.slot * PSLOT_M + pc;
+      const float* P = pw + pr.slot * PSLOT + pc;
       const float rA = nx_rA, dx = nx_dx, rbx = nx_rb, ddx = nx_dd, alx = nx_al;
       if (s + 1 < nst) {
         nx_rA = __ldg(a.rxa + i + 4);
@@ -510,7 +527,7 @@ __global__ void __maxnreg__(168)
         if (pu.strip || pml) {
           // (strips hold y-slab nodes and the few interior columns beside them)
           pml_node<FX, FY, FZ, IRK>(a, pu.strip ? STRIP + 8 : HW, x0, x1, x2, x3, x4, cur, g, i, j, k, fx, fy, fz, pu.face,
-                               P + 18 * PB, q, P, damp, rbx, ddx, alx, yz);
+                               P + RG::AOFF * PB, q, P, damp, rbx, ddx, alx, yz);
         } else {
           float hv[9];
           lean_velocity<FX, FY, FZ>(x0, x1, x2, x3, x4, cur, g, a.rDH, hv);
@@ -541,7 +558,8 @@ __global__ void __maxnreg__(168)
 template <int FX, int FY, int FZ, int IRK>
 static bool pml_smem_k() {
   auto one = [](const void* f) {
-    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PML_SMEM) == cudaSuccess;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PmlRing<IRK>::SMEM) ==
+           cudaSuccess;
   };
   return one((const void*)volume_pml_kernel<FX, FY, FZ, IRK, false>) &&
          one((const void*)volume_pml_kernel<FX, FY, FZ, IRK, true>);
@@ -614,14 +632,15 @@ static void pml_launch(const TileMaps& mp, const VolArgs& a, const TileSched& sc
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3(PTOT);
-  cfg.dynamicSmemBytes = PML_SMEM;
   cfg.stream = s;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = pdl ? 1 : 0;
-#define DFD_L(K) cudaLaunchKernelEx(&cfg, volume_pml_kernel<FX, FY, FZ, K, BATCH>, mp, a, sc, tab, n, nunits, err, sched + 2)
+#define DFD_L(K)                                   \
+  cfg.dynamicSmemBytes = PmlRing<K>::SMEM;         \
+  cudaLaunchKernelEx(&cfg, volume_pml_kernel<FX, FY, FZ, K, BATCH>, mp, a, sc, tab, n, nunits, err, sched + 2)
   DFD_BY_STAGE(a.irk, DFD_L);
 #undef DFD_L
 }

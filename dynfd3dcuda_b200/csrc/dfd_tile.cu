@@ -29,7 +29,7 @@
 namespace dfd {
 
 namespace {
-constexpr int PSLOT = 18 * PB;       // RK registers: W0 9, then the stage-1 input or T 9
+constexpr int PSLOT = 18 * PB;       // RK registers: W0 9, then the stage-1 input 9; T alone at stage 3
 constexpr int NS = 8, NP = 3, NQ = 2;  // ring depths (stencil planes, RK registers, unit planes)
 constexpr size_t SMEM_BYTES =
     (size_t)(NS * HSLOT + NP * PSLOT + NQ * QSLOT) * 4 + NQ * sizeof(TileUnit) + 2 * (NS + NP + NQ) * 8 + NQ * 4;
@@ -145,7 +145,7 @@ __global__ void __maxnreg__(96)
         const int cp2 = ib + (m - 4) + 3;
         mbar_expect_tx(b, ptx);
         if (needW0) tma_load4(dst, &mp.w0, cp0, cp1, cp2, 0, b);
-        if (needT) tma_load4(dst + 9 * PB, &mp.t, cp0, cp1, cp2, 0, b);
+        if (needT) tma_load4(dst + (needW0 ? 9 : 0) * PB, &mp.t, cp0, cp1, cp2, 0, b);
         pr.next<NP>();
         pcount++;
       }

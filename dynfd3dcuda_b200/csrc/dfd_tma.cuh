@@ -114,7 +114,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
 // sponge factor (rk4.cu:20-33, cerjan.cu:166-200): step-start values from the stencil
 // input at stage 0, from the pointwise slot P at stages 1 and 2; at stage 2 the slot's
 // second box holds the stage-1 input, from which, with y0 and the stage input, the
-// accumulator is formed (rk_sum, rk_acc); at stage 3 that box holds the accumulator.  IRK: the
+// accumulator is formed (rk_sum, rk_acc); at stage 3 the slot holds the accumulator
+// alone, first.  IRK: the
 // stage (the kernels are compiled per stage).
 template <int F0, int F1, int IRK>
 __device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, long long q, const float* cur,
@@ -133,7 +134,7 @@ __device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, lon
       a.T[x] = rk_acc(y0, rk_sum(y0, P[(9 + f) * PB], cur[f * HBOX], rd), a.rkb, hv[f]);
       w = fmaf(a.rka, hv[f], y0);
     } else {
-      w = fmaf(a.rkb, hv[f], P[(9 + f) * PB]);
+      w = fmaf(a.rkb, hv[f], P[f * PB]);
     }
     a.Wout[x] = w * damp;
   }
