@@ -341,7 +341,7 @@ def learned_rs(dfd, steps=600, every=7, epochs=4, device=0):
 def run_ensemble(args, dfd, local):
     """Batched ensemble (64 scenarios, grids of 100-300 nodes per axis, slip weakening and
     rate and state mixed): aggregate Gpt-steps/s of the whole batch, after the autotuner has
-    picked the unit length of the tiled kernel."""
+    picked the tile shape and the unit length of the interior kernel."""
     import cases
     import torch
 
@@ -356,7 +356,7 @@ def run_ensemble(args, dfd, local):
     sims = [dfd.Simulation(p, fx, st, None, device=local) for p, fx, st in specs]
     ens = dfd.Ensemble(sims)
     setup_s = time.perf_counter() - t0
-    times, best, it = ens.autotune(0, candidates=(0, 32, 64, 128), steps=2)
+    times, best, it = ens.autotune(0, candidates=(0, 32, 64, 128), steps=2, rows=(8, 4))
     ens.run(it, args.warmup)
     ens.synchronize()
     it += args.warmup
@@ -380,7 +380,8 @@ def run_ensemble(args, dfd, local):
                        "nodes": nodes, "fault_nodes": nf, "scenarios": n, "parallelism": "one batched launch "
                        "per kernel and RK stage, CUDA graph per step",
                        "l2": "inputs larger than L2; no flush"},
-            "autotune": {"unit_planes_ms": {str(k): v for k, v in times.items()}, "chosen": best},
+            "autotune": {"layout_ms": {f"rows {r}, unit planes {c}": v for (r, c), v in times.items()},
+                         "chosen": {"tile_rows": best[0], "unit_planes": best[1]}},
             "setup_s": setup_s, "gpu_launches": ens_launches * args.steps, "clocks": clocks}
     ens.close()
     for s in sims:

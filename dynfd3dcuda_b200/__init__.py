@@ -74,24 +74,35 @@ class Ensemble:
         """x planes per unit of the tiled kernel (0: each scenario's own plan)."""
         self._check(lib().dfd_ens_set_chunk(self.h, int(chunk)))
 
+    def set_tile_rows(self, rows):
+        """Rows of the interior kernel's tiles for every scenario: 8 (one CTA per SM) or 4
+        (two CTAs per SM)."""
+        self._check(lib().dfd_ens_set_tile_rows(self.h, int(rows)))
+
     def nodes(self):
         n = ctypes.c_longlong()
         self._check(lib().dfd_ens_nodes(self.h, ctypes.byref(n)))
         return n.value
 
-    def autotune(self, it0, candidates=(0, 16, 32, 64, 128), steps=4):
-        """Time a few steps with each unit length and keep the fastest; returns {chunk: ms}.
-        The steps are real steps: the scenarios advance by len(candidates) * steps."""
+    def autotune(self, it0, candidates=(0, 16, 32, 64, 128), steps=4, rows=(8, 4)):
+        """Time a few steps with each layout of the interior kernel's units, a tile shape
+        (rows of a 32-wide tile, with the CTAs per SM it allows) times a unit length (x
+        planes, 0: each scenario's own plan), and keep the fastest.  Returns
+        ({(rows, chunk): ms}, best (rows, chunk), next step).  The steps are real steps: the
+        scenarios advance by (1 + steps) per candidate."""
         times = {}
         it = it0
-        for c in candidates:
-            self.set_chunk(c)
-            self.run(it, 1)  # graphs of this layout
-            it += 1
-            times[c] = self.run_timed(it, steps)
-            it += steps
+        for r in rows:
+            self.set_tile_rows(r)
+            for c in candidates:
+                self.set_chunk(c)
+                self.run(it, 1)  # graphs of this layout
+                it += 1
+                times[(r, c)] = self.run_timed(it, steps)
+                it += steps
         best = min(times, key=times.get)
-        self.set_chunk(best)
+        self.set_tile_rows(best[0])
+        self.set_chunk(best[1])
         return times, best, it
 
     def close(self):
@@ -237,7 +248,7 @@ def lib():
             "dfd_interior_stats": [V, P(ctypes.c_float), P(ctypes.c_longlong)],
             "dfd_ens_create": [V, I, P(ctypes.c_void_p)], "dfd_ens_destroy": [V], "dfd_ens_run": [V, I, I],
             "dfd_ens_synchronize": [V], "dfd_ens_run_timed": [V, I, I, P(ctypes.c_float)],
-            "dfd_ens_set_chunk": [V, I], "dfd_ens_nodes": [V, P(ctypes.c_longlong)],
+            "dfd_ens_set_chunk": [V, I], "dfd_ens_set_tile_rows": [V, I], "dfd_set_tile_rows": [V, I], "dfd_ens_nodes": [V, P(ctypes.c_longlong)],
             "dfd_newton_record": [V, I, I], "dfd_rs_profile": [V, I, I], "dfd_test_wait_drill": [V, I],
             "dfd_halo_floats": [V, P(ctypes.c_longlong)], "dfd_halo_pack": [V, I, I, V], "dfd_halo_unpack": [V, I, I, V],
             "dfd_rs_solve_stats": [V, P(ctypes.c_longlong), P(ctypes.c_longlong), P(ctypes.c_double),
@@ -478,6 +489,11 @@ class Simulation:
             return
         a = np.ascontiguousarray(w, np.float32).ravel()
         self._check(lib().dfd_set_guess_net(self.h, a.ctypes.data, a.size))
+
+    def set_tile_rows(self, rows):
+        """Rows of the interior kernel's tiles: 8 (one CTA per SM, the default) or 4 (two
+        CTAs per SM); the same results either way."""
+        self._check(lib().dfd_set_tile_rows(self.h, int(rows)))
 
     def newton_record(self, capacity, every=1):
         """Record (psi/a, log10 Vhat, log10 coef, a, x* residual) of one in `every` converged

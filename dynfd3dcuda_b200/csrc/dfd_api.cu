@@ -1300,6 +1300,18 @@ int dfd_rs_solve_stats(dfd_ctx* ctx, long long* accepted, long long* fallback, d
   return DFD_OK;
 }
 
+int dfd_set_tile_rows(dfd_ctx* ctx, int rows) {
+  if (!ctx || (rows != 8 && rows != 4)) return DFD_ERR_PARAM;
+  if (mid_step(ctx)) return fail(ctx, DFD_ERR_STATE, "a step is half done (dfd_stage)");
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  ctx->tile.tr = rows;
+  // the tile shape is baked into the step graphs: rebuild them
+  for (auto& g : ctx->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return DFD_OK;
+}
+
 int dfd_newton_record(dfd_ctx* ctx, int capacity, int every) {
   if (!ctx || capacity < 0 || every < 1) return DFD_ERR_PARAM;
   ctx->rec_every = every;
@@ -1621,6 +1633,7 @@ struct dfd_ens {
   int device = 0;
   int nsm = 148;
   int chunk = 0;               // planes per unit of the tiled kernel (0: per-scenario plan)
+  int tr = TILE_K;             // rows of the interior kernel's tiles (every scenario's)
   cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
   int* it_dev = nullptr;
@@ -1702,7 +1715,7 @@ static int ens_build(dfd_ens* e) {
         memset(&sch, 0, sizeof sch);
         if (pl.tiled) {
           int grid = 0;
-          sch = tile_plan(pl.lo, pl.hi, e->nsm, &grid);
+          sch = tile_plan(pl.lo, pl.hi, e->nsm * tile_ctas_per_sm(e->tr), &grid, e->tr);
           if (e->chunk > 0) {
             sch.ci = std::min(e->chunk, pl.hi.x - pl.lo.x);
             sch.nunits = sch.ntj * sch.ntk * ((pl.hi.x - pl.lo.x + sch.ci - 1) / sch.ci);
@@ -1755,7 +1768,7 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
     }
   if (nr) launch_fault_node_batch(S.fault, S.fstart, nr, S.fblocks, S.FY, S.FZ, e->s0);
   if (e->sc[0]->serial) {
-    launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
+    launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, e->tr, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
     launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, S.nunits > 0,
                      e->s0);
     // the general kernel beside the fault band kernel
@@ -1779,7 +1792,7 @@ static int ens_enqueue(dfd_ens* e, int pat, int irk) {
   launch_shell_batch(S.vol, S.boxes, S.sstart, n, S.sblocks, S.FX, S.FY, S.FZ, false, irk, e->s2);
   launch_shell_batch(S.vol, S.boxes, S.tstart, n, S.tblocks, S.FX, S.FY, S.FZ, true, irk, e->s2);
   cudaEventRecord(e->ev_join2, e->s2);
-  launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
+  launch_tile_batch(S.first, S.tile, n, S.nunits, e->nsm, e->tr, S.FX, S.FY, S.FZ, e->err, e->sched, e->s0);
   launch_pml_batch(S.pfirst, S.ptile, n, S.punits, e->nsm, S.FX, S.FY, S.FZ, e->err, e->sched, S.nunits > 0,
                      e->s0);
   if (nr) cudaStreamWaitEvent(e->s0, e->ev_join, 0);
@@ -1826,6 +1839,12 @@ int dfd_ens_create(dfd_ctx* const* scenarios, int n, dfd_ens** out) {
   }
   cudaSetDevice(e->device);
   e->nsm = scenarios[0]->tile.nsm;
+  e->tr = scenarios[0]->tile.tr;  // one batched launch: every scenario with the same tile rows
+  for (int i = 1; i < n; i++)
+    if (scenarios[i]->tile.tr != e->tr) {
+      delete e;
+      return DFD_ERR_PARAM;
+    }
   auto done = [&](int rc) {
     if (rc) dfd_ens_destroy(e);
     return rc;
@@ -1930,6 +1949,16 @@ int dfd_ens_set_chunk(dfd_ens* e, int chunk) {
   ECK(cudaStreamSynchronize(e->s0));
   ens_drop_graphs(e);
   e->chunk = chunk;
+  return ens_build(e);
+}
+
+int dfd_ens_set_tile_rows(dfd_ens* e, int rows) {
+  if (!e || (rows != 8 && rows != 4)) return DFD_ERR_PARAM;
+  cudaSetDevice(e->device);
+  ECK(cudaStreamSynchronize(e->s0));
+  ens_drop_graphs(e);
+  e->tr = rows;
+  for (dfd_ctx* c : e->sc) c->tile.tr = rows;  // the scenarios' maps follow (tile_maps)
   return ens_build(e);
 }
 

@@ -237,6 +237,8 @@ struct TileMaps {
   CUtensorMap aux[6];  // PML state of each face (27 fields), pointwise box of 9 fields
   // the same for the 16 x 16 strip tiles (halo box 24 x 20)
   CUtensorMap win_s, w0_s, t_s, plane_s, auxy_s[2];
+  // the interior kernel's: its tiles are 32 x 8 (the maps above) or 32 x 4 (TileCtx::tr)
+  CUtensorMap win_i, w0_i, t_i, plane_i;
 };
 // Per-context state of the tiled kernels: maps of the four volume buffers, of the metric
 // and of the PML state (fixed addresses, encoded once), the error flag, the SM count.
@@ -246,6 +248,8 @@ struct TileCtx {
   CUtensorMap plane;
   CUtensorMap aux[6];
   CUtensorMap halo_s[4], centre_s[4], plane_s, auxy_s[2];  // strip tiles
+  CUtensorMap halo4[4], centre4[4], plane4;                // 32 x 4 tiles of the interior kernel
+  int tr = TILE_K;       // rows of the interior kernel's tiles: 8 (one CTA per SM) or 4 (two)
   int* err = nullptr;
   int* sched = nullptr;  // unit counter and finished-CTA counter (zero between launches)
   int nsm = 0;
@@ -308,7 +312,10 @@ struct VolPlan {
 };
 VolPlan plan_volume(const VolArgs& a, const TileCtx* tc);
 bool tile_feasible(const TileCtx* tc, const VolArgs& a, int3 lo, int3 hi);
-TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid);
+// slots: CTAs resident at once (SMs x CTAs per SM); tr: rows of a tile
+TileSched tile_plan(int3 lo, int3 hi, int slots, int* grid, int tr = TILE_K);
+// CTAs of the interior kernel resident per SM with tiles of tr rows
+int tile_ctas_per_sm(int tr);
 // units of the PML kernel around the interior box (dfd_pml.cu)
 TileSched pml_plan(const VolArgs& a, int ya, int yb, int za, int zb, int ktop, int nsm, int* grid);
 bool pml_setup();
@@ -319,8 +326,8 @@ void launch_pml(const TileCtx* tc, const VolArgs& a, int FX, int FY, int FZ, int
 void launch_pml_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY, int FZ,
                       int* err, int* sched, bool pdl, cudaStream_t s);
 // batched launches (dfd_volume.cu, dfd_tile.cu, dfd_fault.cu)
-void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,
-                       int FZ, int* err, int* sched, cudaStream_t s);
+void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int tr, int FX,
+                       int FY, int FZ, int* err, int* sched, cudaStream_t s);
 // top: the free-surface boxes (start: per-scenario block starts of those), else the others;
 // irk: the stage of every scenario's arguments
 void launch_shell_batch(const VolArgs* tab, const Boxes* boxes, const int* start, int n, int blocks, int FX, int FY,

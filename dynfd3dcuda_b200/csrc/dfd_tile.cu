@@ -29,31 +29,47 @@
 namespace dfd {
 
 namespace {
-constexpr int PSLOT = 18 * PB;       // RK registers: W0 9, then the stage-1 input 9; T alone at stage 3
-constexpr int NS = 8, NP = 3, NQ = 2;  // ring depths (stencil planes, RK registers, unit planes)
-constexpr size_t SMEM_BYTES =
-    (size_t)(NS * HSLOT + NP * PSLOT + NQ * QSLOT) * 4 + NQ * sizeof(TileUnit) + 2 * (NS + NP + NQ) * 8 + NQ * 4;
-static_assert(SMEM_BYTES <= 232448, "tile ring exceeds the shared memory of one CTA");
-static_assert((PSLOT * 4) % 128 == 0, "slot alignment");
+// Shape of the interior kernel's tiles: 32 (y) x TR (z) nodes.  TR = 8: 16 computing warps
+// and one CTA per SM; TR = 4: 8 computing warps, shallower stencil ring and two CTAs per
+// SM (each within half of the SM's 228 KB of shared memory, 1 KB of it reserved per CTA).
+// An RK slot holds W0 and the stage-1 input (stage 2), W0 (stage 1) or T alone (stage 3).
+template <int TR>
+struct TileShape {
+  static constexpr int HH = TR + 4, HB = HW * HH, HSLOT = 9 * HB, PB = TJ * TR, QSLOT = 12 * PB;
+  static constexpr int PSLOT = 18 * PB;
+  static constexpr int NCW = 2 * TR, NTOT = NCW * 32 + 32;
+  static constexpr int NS = TR == 8 ? 8 : 6, NP = 3, NQ = 2;  // stencil planes, RK slots, unit planes
+  static constexpr int CTAS = TR == 8 ? 1 : 2;
+  static constexpr size_t SMEM =
+      (size_t)(NS * HSLOT + NP * PSLOT + NQ * QSLOT) * 4 + NQ * sizeof(TileUnit) + 2 * (NS + NP + NQ) * 8 + NQ * 4;
+  static_assert(TR == 8 || TR == 4, "tiles of 8 or 4 rows");
+  static_assert(SMEM <= 232448 && CTAS * (SMEM + 1024) <= 233472, "tile ring exceeds the shared memory");
+  static_assert((PSLOT * 4) % 128 == 0 && (HSLOT * 4) % 128 == 0 && (QSLOT * 4) % 128 == 0, "slot alignment");
+};
 }  // namespace
 
-// Warp NCW issues the copies; warps 0..NCW-1 compute one node each per plane.  Each ring
+int tile_ctas_per_sm(int tr) { return tr == 4 ? TileShape<4>::CTAS : TileShape<8>::CTAS; }
+
+// Warp NCW issues the copies; warps 0..NCW-1 compute one node each per plane (NCW = 2 TR).  Each ring
 // slot has a "full" barrier (completed by the copy's transaction bytes) and an "empty"
 // barrier (one arrival per computing warp once it has finished reading the slot).  Three
 // rings: stencil planes (NS), RK registers of the step (NP; none at stage 0, whose
 // step-start values are the stencil input), metric/media planes of the unit (NQ).  At
-// most 96 registers: the 17 warps are spread over the SM's four 16 K-register partitions,
-// five warps on one of them.
+// most 96 registers: with 8-row tiles the 17 warps are spread over the SM's four 16 K-register
+// partitions, five warps on one of them; with 4-row tiles two CTAs of 9 warps share them.
 
 // IRK: the RK stage (a0.irk), a compile-time constant so that each stage's code and
 // register allocation carry only its own RK registers.  BATCH: the units of the nscen
 // scenarios of tab (an ensemble) in one launch; the parameters mp0, a0, sc0 then
-// describe scenario 0 and give the stage's common values.
-template <int FX, int FY, int FZ, int IRK, bool BATCH>
+// describe scenario 0 and give the stage's common values.  TR: rows of a tile (TileShape).
+template <int FX, int FY, int FZ, int IRK, bool BATCH, int TR>
 __global__ void __maxnreg__(96)
     volume_tile_kernel(const __grid_constant__ TileMaps mp0, const __grid_constant__ VolArgs a0,
                        const __grid_constant__ TileSched sc0, const TileScen* __restrict__ tab, int nscen,
                        int nunits, int* err, int* sched) {
+  using SH = TileShape<TR>;
+  constexpr int TK = TR, HSLOT = SH::HSLOT, PSLOT = SH::PSLOT, QSLOT = SH::QSLOT, PB = SH::PB, NCW = SH::NCW;
+  constexpr int NS = SH::NS, NP = SH::NP, NQ = SH::NQ;
   extern __shared__ __align__(1024) unsigned char smraw[];
   float* win = reinterpret_cast<float*>(smraw);
   float* pw = win + NS * HSLOT;
@@ -127,14 +143,14 @@ __global__ void __maxnreg__(96)
       } else {
         mbar_expect_tx(full_q + qr.slot, QSLOT * 4);
       }
-      tma_load3(qs + qr.slot * QSLOT, &mp.plane, cp0, cp1, 0, full_q + qr.slot);
+      tma_load3(qs + qr.slot * QSLOT, &mp.plane_i, cp0, cp1, 0, full_q + qr.slot);
       qr.next<NQ>();
       qcount++;
       for (int m = 0; m < nst + 4 && ok; m++) {
         // stencil plane m of the unit (first needed by step m - 4)
         if (wcount >= NS && !(ok = mbar_wait(empty_w + wr.slot, wr.phase ^ 1))) break;
         mbar_expect_tx(full_w + wr.slot, HSLOT * 4);
-        tma_load4(win + wr.slot * HSLOT, &mp.win, cw0, cw1, ib + XLO + m + 3, 0, full_w + wr.slot);
+        tma_load4(win + wr.slot * HSLOT, &mp.win_i, cw0, cw1, ib + XLO + m + 3, 0, full_w + wr.slot);
         wr.next<NS>();
         wcount++;
         if (m < 4 || !usep) continue;
@@ -144,8 +160,8 @@ __global__ void __maxnreg__(96)
         float* dst = pw + pr.slot * PSLOT;
         const int cp2 = ib + (m - 4) + 3;
         mbar_expect_tx(b, ptx);
-        if (needW0) tma_load4(dst, &mp.w0, cp0, cp1, cp2, 0, b);
-        if (needT) tma_load4(dst + (needW0 ? 9 : 0) * PB, &mp.t, cp0, cp1, cp2, 0, b);
+        if (needW0) tma_load4(dst, &mp.w0_i, cp0, cp1, cp2, 0, b);
+        if (needT) tma_load4(dst + (needW0 ? 9 : 0) * PB, &mp.t_i, cp0, cp1, cp2, 0, b);
         pr.next<NP>();
         pcount++;
       }
@@ -242,11 +258,11 @@ __global__ void __maxnreg__(96)
         const long long q = qyz + (long long)(i + 3) * d.sx;
         float hv[9];
         if (role == 0) {
-          lean_velocity<FX, FY, FZ>(xs0, xs1, xs2, xs3, xs4, cur, g, a.rDH, hv);
-          rk_tile_store<0, 3, IRK>(a, n, q, cur, P, hv, damp);
+          lean_velocity<FX, FY, FZ, HW, SH::HB>(xs0, xs1, xs2, xs3, xs4, cur, g, a.rDH, hv);
+          rk_tile_store<0, 3, IRK, SH::HB, PB>(a, n, q, cur, P, hv, damp);
         } else {
-          lean_stress<FX, FY, FZ>(xs0, xs1, xs2, xs3, xs4, cur, g, a.rDH, hv);
-          rk_tile_store<3, 9, IRK>(a, n, q, cur, P, hv, damp);
+          lean_stress<FX, FY, FZ, HW, SH::HB>(xs0, xs1, xs2, xs3, xs4, cur, g, a.rDH, hv);
+          rk_tile_store<3, 9, IRK, SH::HB, PB>(a, n, q, cur, P, hv, damp);
         }
       }
       // release the slots this warp has finished with
@@ -298,11 +314,13 @@ static bool make_map(CUtensorMap* m, const Dims& d, const float* base, int nf, i
 
 template <int FX, int FY, int FZ, int IRK>
 static bool set_smem_k() {
-  auto one = [](const void* f) {
-    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES) == cudaSuccess;
+  auto one = [](const void* f, size_t bytes) {
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
   };
-  return one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, false>) &&
-         one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, true>);
+  return one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, false, 8>, TileShape<8>::SMEM) &&
+         one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, true, 8>, TileShape<8>::SMEM) &&
+         one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, false, 4>, TileShape<4>::SMEM) &&
+         one((const void*)volume_tile_kernel<FX, FY, FZ, IRK, true, 4>, TileShape<4>::SMEM);
 }
 template <int FX, int FY, int FZ>
 static bool set_smem() {
@@ -352,11 +370,15 @@ bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* plan
   for (int b = 0; b < 4 && ok; b++) {
     ok = make_map(&tc->halo[b], d, W[b], 9, HW, HH, 9);
     ok = ok && make_map(&tc->centre[b], d, W[b], 9, TJ, TK, 9);
+    // 32 x 4 tiles of the interior kernel: halo box 40 x 8
+    ok = ok && make_map(&tc->halo4[b], d, W[b], 9, HW, TileShape<4>::HH, 9);
+    ok = ok && make_map(&tc->centre4[b], d, W[b], 9, TJ, 4, 9);
     // strip tiles of the PML kernel: 16 x 16 nodes, halo box 24 x 20
     ok = ok && make_map(&tc->halo_s[b], d, W[b], 9, STRIP + 8, STRIP + 4, 9);
     ok = ok && make_map(&tc->centre_s[b], d, W[b], 9, STRIP, STRIP, 9);
   }
   ok = ok && make_plane_map(&tc->plane, d, planes, TJ, TK);
+  ok = ok && make_plane_map(&tc->plane4, d, planes, TJ, 4);
   ok = ok && make_plane_map(&tc->plane_s, d, planes, STRIP, STRIP);
   for (int f = 0; f < 6 && ok; f++) {
     memset(&tc->aux[f], 0, sizeof(CUtensorMap));
@@ -376,12 +398,13 @@ bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* plan
 
 // Chunking of the x range: minimise the busiest CTA's plane loads, ceil(units / grid) x
 // (planes per chunk + 4 halo planes).
-TileSched tile_plan(int3 lo, int3 hi, int nsm, int* grid) {
+TileSched tile_plan(int3 lo, int3 hi, int slots, int* grid, int tr) {
   TileSched s;
   memset(&s, 0, sizeof s);
   s.lo_x = lo.x; s.lo_y = lo.y; s.lo_z = lo.z; s.hi_x = hi.x; s.hi_y = hi.y; s.hi_z = hi.z;
   s.ntj = (hi.y - lo.y + TJ - 1) / TJ;
-  s.ntk = (hi.z - lo.z + TK - 1) / TK;
+  s.ntk = (hi.z - lo.z + tr - 1) / tr;
+  const int nsm = slots;
   int nx = hi.x - lo.x, ntile = s.ntj * s.ntk;
   long long best = -1;
   for (int nch = 1; nch <= 64 && nch <= nx; nch++) {
@@ -412,19 +435,31 @@ TileMaps tile_maps(const TileCtx& tc, int bin, int irk) {
   mp.plane_s = tc.plane_s;
   mp.auxy_s[0] = tc.auxy_s[0];
   mp.auxy_s[1] = tc.auxy_s[1];
+  const bool four = tc.tr == 4;
+  mp.win_i = four ? tc.halo4[bin] : mp.win;
+  mp.w0_i = four ? tc.centre4[0] : mp.w0;
+  mp.t_i = four ? tc.centre4[p2] : mp.t;
+  mp.plane_i = four ? tc.plane4 : mp.plane;
   return mp;
 }
 
-template <int FX, int FY, int FZ>
-static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
+template <int FX, int FY, int FZ, int TR>
+static void launch_tr(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
+  using SH = TileShape<TR>;
   const TileMaps mp = tile_maps(tc, bin, a.irk);
   int grid = 0;
-  TileSched sc = tile_plan(lo, hi, tc.nsm, &grid);
+  TileSched sc = tile_plan(lo, hi, tc.nsm * SH::CTAS, &grid, TR);
   sc.drill = tc.drill;
-#define DFD_L(K) \
-  volume_tile_kernel<FX, FY, FZ, K, false><<<grid, NTOT, SMEM_BYTES, s>>>(mp, a, sc, nullptr, 1, sc.nunits, tc.err, tc.sched)
+#define DFD_L(K)                                                                                             \
+  volume_tile_kernel<FX, FY, FZ, K, false, TR><<<grid, SH::NTOT, SH::SMEM, s>>>(mp, a, sc, nullptr, 1, sc.nunits, \
+                                                                               tc.err, tc.sched)
   DFD_BY_STAGE(a.irk, DFD_L);
 #undef DFD_L
+}
+template <int FX, int FY, int FZ>
+static void launch_t(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
+  if (tc.tr == 4) launch_tr<FX, FY, FZ, 4>(tc, a, bin, lo, hi, s);
+  else launch_tr<FX, FY, FZ, 8>(tc, a, bin, lo, hi, s);
 }
 
 // true when the tiled kernel can take the box lo..hi
@@ -433,28 +468,37 @@ bool tile_feasible(const TileCtx* tc, const VolArgs& a, int3 lo, int3 hi) {
   return (lo.y + 3 + a.d.oy) % 4 == 0 && lo.z >= 0 && hi.x > lo.x && hi.y > lo.y && hi.z > lo.z;
 }
 
-template <int FX, int FY, int FZ>
-static void launch_tb(const TileScen& f, const TileScen* tab, int n, int nunits, int grid, int* err, int* sched,
-                      cudaStream_t s) {
-#define DFD_L(K) \
-  volume_tile_kernel<FX, FY, FZ, K, true><<<grid, NTOT, SMEM_BYTES, s>>>(f.mp, f.u.a, f.u.sc, tab, n, nunits, err, sched)
+template <int FX, int FY, int FZ, int TR>
+static void launch_tbr(const TileScen& f, const TileScen* tab, int n, int nunits, int grid, int* err, int* sched,
+                       cudaStream_t s) {
+  using SH = TileShape<TR>;
+#define DFD_L(K)                                                                                                \
+  volume_tile_kernel<FX, FY, FZ, K, true, TR><<<grid * SH::CTAS, SH::NTOT, SH::SMEM, s>>>(f.mp, f.u.a, f.u.sc, tab, n, \
+                                                                                         nunits, err, sched)
   DFD_BY_STAGE(f.u.a.irk, DFD_L);
 #undef DFD_L
 }
-// every scenario of an ensemble in one persistent launch (units numbered across them)
-void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int FX, int FY,
-                       int FZ, int* err, int* sched, cudaStream_t s) {
+template <int FX, int FY, int FZ>
+static void launch_tb(const TileScen& f, const TileScen* tab, int n, int nunits, int grid, int tr, int* err,
+                      int* sched, cudaStream_t s) {
+  if (tr == 4) launch_tbr<FX, FY, FZ, 4>(f, tab, n, nunits, grid, err, sched, s);
+  else launch_tbr<FX, FY, FZ, 8>(f, tab, n, nunits, grid, err, sched, s);
+}
+// every scenario of an ensemble in one persistent launch (units numbered across them);
+// grid: SMs (each takes tile_ctas_per_sm(tr) CTAs); tr: the scenarios' tile rows
+void launch_tile_batch(const TileScen& first, const TileScen* tab, int n, int nunits, int grid, int tr, int FX,
+                       int FY, int FZ, int* err, int* sched, cudaStream_t s) {
   if (nunits <= 0) return;
   int code = (FX > 0) * 4 + (FY > 0) * 2 + (FZ > 0);
   switch (code) {
-    case 0: launch_tb<-1, -1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 1: launch_tb<-1, -1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 2: launch_tb<-1, 1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 3: launch_tb<-1, 1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 4: launch_tb<1, -1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 5: launch_tb<1, -1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
-    case 6: launch_tb<1, 1, -1>(first, tab, n, nunits, grid, err, sched, s); break;
-    default: launch_tb<1, 1, 1>(first, tab, n, nunits, grid, err, sched, s); break;
+    case 0: launch_tb<-1, -1, -1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
+    case 1: launch_tb<-1, -1, 1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
+    case 2: launch_tb<-1, 1, -1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
+    case 3: launch_tb<-1, 1, 1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
+    case 4: launch_tb<1, -1, -1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
+    case 5: launch_tb<1, -1, 1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
+    case 6: launch_tb<1, 1, -1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
+    default: launch_tb<1, 1, 1>(first, tab, n, nunits, grid, tr, err, sched, s); break;
   }
 }
 

@@ -117,7 +117,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
 // accumulator is formed (rk_sum, rk_acc); at stage 3 the slot holds the accumulator
 // alone, first.  IRK: the
 // stage (the kernels are compiled per stage).
-template <int F0, int F1, int IRK>
+template <int F0, int F1, int IRK, int HB = HBOX, int PBB = PB>
 __device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, long long q, const float* cur,
                                               const float* P, const float* hv, float damp) {
   const float rd = IRK == 2 ? rk_rd(damp) : 1.0f;
@@ -126,15 +126,15 @@ __device__ __forceinline__ void rk_tile_store(const VolArgs& a, long long n, lon
     const long long x = f * n + q;
     float w;
     if (IRK == 0) {
-      w = fmaf(a.rka, hv[f], cur[f * HBOX]);
+      w = fmaf(a.rka, hv[f], cur[f * HB]);
     } else if (IRK == 1) {
-      w = fmaf(a.rka, hv[f], P[f * PB]);
+      w = fmaf(a.rka, hv[f], P[f * PBB]);
     } else if (IRK == 2) {
-      const float y0 = P[f * PB];
-      a.T[x] = rk_acc(y0, rk_sum(y0, P[(9 + f) * PB], cur[f * HBOX], rd), a.rkb, hv[f]);
+      const float y0 = P[f * PBB];
+      a.T[x] = rk_acc(y0, rk_sum(y0, P[(9 + f) * PBB], cur[f * HB], rd), a.rkb, hv[f]);
       w = fmaf(a.rka, hv[f], y0);
     } else {
-      w = fmaf(a.rkb, hv[f], P[f * PB]);
+      w = fmaf(a.rkb, hv[f], P[f * PBB]);
     }
     a.Wout[x] = w * damp;
   }
@@ -155,10 +155,11 @@ struct NodeMetric {
 // The x row of the metric has three
 // components; the y and z rows have no x component, so the terms with it (exact zeros)
 // and the derivative of Txx along y and z drop out.  Reference wave.cu:8-204.
-#define DFD_DERX(f) d5v<FX>(xs0[(f) * HBOX], xs1[(f) * HBOX], xs2[(f) * HBOX], xs3[(f) * HBOX], xs4[(f) * HBOX])
-#define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HBOX)
-#define DFD_DERZ(f) d5s<FZ, PW>(cur + (f) * HBOX)
-template <int FX, int FY, int FZ, int PW = HW>
+// HB: floats per field of the stencil box.
+#define DFD_DERX(f) d5v<FX>(xs0[(f) * HB], xs1[(f) * HB], xs2[(f) * HB], xs3[(f) * HB], xs4[(f) * HB])
+#define DFD_DERY(f) d5s<FY, 1>(cur + (f) * HB)
+#define DFD_DERZ(f) d5s<FZ, PW>(cur + (f) * HB)
+template <int FX, int FY, int FZ, int PW = HW, int HB = HBOX>
 __device__ __forceinline__ void lean_velocity(const float* xs0, const float* xs1, const float* xs2, const float* xs3,
                                               const float* xs4, const float* cur, const NodeMetric& g, float r,
                                               float* hv) {
@@ -190,7 +191,7 @@ __device__ __forceinline__ void lean_velocity(const float* xs0, const float* xs1
 #undef DFD_VAXIS0
   hv[0] = h0; hv[1] = h1; hv[2] = h2;
 }
-template <int FX, int FY, int FZ, int PW = HW>
+template <int FX, int FY, int FZ, int PW = HW, int HB = HBOX>
 __device__ __forceinline__ void lean_stress(const float* xs0, const float* xs1, const float* xs2, const float* xs3,
                                             const float* xs4, const float* cur, const NodeMetric& g, float r,
                                             float* hv) {

@@ -260,6 +260,11 @@ int dfd_output_close(dfd_ctx *ctx);
  * the first DFD_MLP_TRAINABLE are trained. */
 #define DFD_MLP_PARAMS 1259
 #define DFD_MLP_TRAINABLE 1249
+/* Tile shape of the TMA-staged interior kernel (no counterpart in the reference, whose
+ * stencil kernels use fixed thread blocks): rows 8 (32 x 8 tiles, one CTA per SM, the
+ * default) or 4 (32 x 4 tiles, two CTAs per SM).  Results are the same bits either way;
+ * the speed depends on the grid.  Between steps only (DFD_ERR_STATE mid-step). */
+int dfd_set_tile_rows(dfd_ctx *ctx, int rows);
 /* load the weights and switch the learned guess on (weights NULL, n 0: switch it off) */
 int dfd_set_guess_net(dfd_ctx *ctx, const float *weights, int n);
 /* record (psi/a, log10 Vhat, log10 coef, a, x* residual) of one in `every` converged plain
@@ -308,6 +313,9 @@ int dfd_ens_synchronize(dfd_ens *e);
 int dfd_ens_run_timed(dfd_ens *e, int it0, int nsteps, float *ms);
 /* x planes per unit of the tiled kernel (0: each scenario's own plan); for autotuning */
 int dfd_ens_set_chunk(dfd_ens *e, int chunk);
+/* rows of the interior kernel's tiles for every scenario (dfd_set_tile_rows); for
+ * autotuning together with the chunk */
+int dfd_ens_set_tile_rows(dfd_ens *e, int rows);
 int dfd_ens_nodes(const dfd_ens *e, long long *nodes);
 const char *dfd_ens_last_error(const dfd_ens *e);
 

@@ -1,7 +1,7 @@
 """The batched ensemble (dfd_ens_*): scenarios of uneven grid sizes, slip weakening and
 rate and state mixed, stepped together with one batched launch per kernel and RK stage.
 Each scenario must end where the single-scenario path puts it, whatever the unit length
-the autotuner picks.  The batched kernels evaluate the same expressions as the single
+and tile shape the autotuner picks.  The batched kernels evaluate the same expressions as the single
 ones but are compiled as other kernels, so the compiler may fuse a multiply and an add
 differently: agreement is to FP32 rounding (1e-5 of each field's maximum, as between the
 tiled and the plain interior kernels), not bit for bit."""
@@ -47,8 +47,8 @@ def state(sim):
     return sim.wave(), {k: sim.fault(k) for k in ("slip", "Vs1", "Tn", "State")}
 
 
-@pytest.mark.parametrize("chunk", [0, 8])
-def test_ensemble_matches_single_runs(chunk):
+@pytest.mark.parametrize("chunk,rows", [(0, 8), (8, 8), (0, 4)])
+def test_ensemble_matches_single_runs(chunk, rows):
     import dynfd3dcuda_b200 as dfd
 
     specs = [make(i) for i in range(5)]
@@ -56,6 +56,7 @@ def test_ensemble_matches_single_runs(chunk):
     batch = [dfd.Simulation(p, fx, st, None) for p, fx, st in specs]
     ens = dfd.Ensemble(batch)
     ens.set_chunk(chunk)
+    ens.set_tile_rows(rows)
     steps = 24
     ens.run(0, steps)
     ens.synchronize()
@@ -83,7 +84,9 @@ def test_autotune_keeps_results():
     b = [dfd.Simulation(p, fx, st, None) for p, fx, st in specs]
     ens = dfd.Ensemble(a)
     times, best, it = ens.autotune(0, candidates=(0, 8, 16), steps=2)
-    assert best in times and it == 9
+    # every tile shape (rows 8 and 4) with every unit length, 1 + 2 steps each
+    assert set(times) == {(r, c) for r in (8, 4) for c in (0, 8, 16)}
+    assert best in times and it == 3 * len(times)
     ens.run(it, 3)
     ens.synchronize()
     for s in b:
