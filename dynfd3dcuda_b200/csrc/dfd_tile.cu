@@ -1,21 +1,21 @@
 // Interior box of the volume stage, staged through shared memory by TMA.
 //
-// The box is cut into tiles of 32 (y) x 8 (z) nodes; a CTA owns one tile column and
-// marches along x over a chunk of planes.  Per plane it needs
+// The box is cut into tiles of 32 (y) x 8 (z) nodes (or 32 x 4, TileShape); a CTA owns
+// one tile column and marches along x over a chunk of planes.  Per plane it needs
 //   - the stencil input (9 fields) of the planes x-1..x+3 (forward x operator) or
 //     x-3..x+1 (backward), with a y/z halo on the current plane: one 4-D TMA box
 //     (40 y, 12 z, 1 x, 9 fields) per plane, held in a ring of NS plane slots;
 //   - the pointwise streams of the node: 12 metric/media fields, and the RK registers
 //     W0 (stages 1, 2), the stage-1 input (stage 2) and T (stage 3): TMA boxes (32, 8, 1, n)
 //     in a ring of NP slots.
-// A dedicated warp issues the copies ahead of the sixteen computing warps (full/empty
+// A dedicated warp issues the copies ahead of the sixteen (eight) computing warps (full/empty
 // mbarrier pairs per slot, no block-wide barrier in the loop), so HBM traffic stays in
 // flight while the stencils are evaluated from shared memory with immediate offsets.
 // No node of the box lies in a PML slab or the free-surface rows (dfd_pml.cu and the
 // general kernel take those).  Outputs (Wout, and T at stage 2) are written straight from
 // registers.
 //
-// The kernel is persistent: one CTA per SM takes units (tile column x chunk) from a global
+// The kernel is persistent: one CTA per SM (two with 4-row tiles) takes units (tile column x chunk) from a global
 // counter, and its copy stream runs across unit boundaries, so the next unit's planes
 // arrive while the current one finishes.
 //
