@@ -336,6 +336,19 @@ VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
     // strips start); the PML kernel every other node below the free-surface rows
     int ya = a.aux[2] ? (d.N + STRIP - 1) / STRIP * STRIP : 0;
     int yb = a.aux[3] ? (d.nj - d.N) / 4 * 4 : d.nj;
+    if (a.aux[3] && yb > ya) {
+      // A column of the interior kernel's 32-wide tiles and a column of the PML kernel's
+      // 16-wide strips cost about the same (half the nodes at about twice the cost per
+      // node), and a partial column costs nearly a full one.  Of the y ends up to 28
+      // columns earlier, take the one with the fewest columns of both (ties: the latest):
+      // with NY = 600 and PML 20 that is 576 (17 whole tiles, two strips), not 580 (an
+      // 18th tile 4 columns wide, the same two strips).
+      auto cols = [&](int y) { return (y - ya + TILE_J - 1) / TILE_J + (d.nj - y + STRIP - 1) / STRIP; };
+      int best = yb;
+      for (int y = yb - 4; y >= yb - 28 && y > ya; y -= 4)
+        if (cols(y) < cols(best)) best = y;
+      yb = best;
+    }
     int za = a.aux[4] ? d.N : 0;
     int zb = a.aux[5] ? d.nk - d.N : ktop;
     if (yb <= ya) ya = yb = 0;     // no interior column: strips over every column
@@ -346,6 +359,17 @@ VolPlan plan_volume(const VolArgs& a, const TileCtx* tc) {
     if (zb - za >= TILE_K && zr) {
       if (a.aux[4]) za += zr;
       else zb -= zr;
+    }
+    // ... unless they then cost the z1 slab a row of z tiles of its own: a row of the PML
+    // kernel's tiles costs about two of the interior kernel's, so with PML 20 and 297 rows
+    // (25 rows: a fourth z-tile row holding one) the slab keeps its 20 rows in three tile
+    // rows and the interior box ends in a partial tile row
+    if (a.aux[4] && zb - za >= TILE_K) {
+      auto rows = [&](int z) { return 2 * ((z + TILE_K - 1) / TILE_K) + (zb - z + TILE_K - 1) / TILE_K; };
+      int best = za;
+      for (int z = d.N; z < za; z++)
+        if (rows(z) < rows(best)) best = z;
+      za = best;
     }
     if (zb <= za || zb - za < TILE_K) za = zb = ktop;  // no interior row: z tiles over every row
     int grid = 0;
