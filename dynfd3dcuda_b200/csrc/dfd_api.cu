@@ -1722,7 +1722,7 @@ static int ens_build(dfd_ens* e) {
           }
         }
         TileScen& t = ts[i];
-        t.mp = tile_maps(c->tile, bin[irk], irk);
+        t.mp = tile_maps(c->tile, bin[irk], irk, e->tr);
         t.u.a = a;
         t.u.sc = sch;
         t.u.unit0 = units;

@@ -259,7 +259,8 @@ struct TileCtx {
 bool tile_setup(TileCtx* tc, const Dims& d, float* const W[4], const float* planes, float* const aux[6], int* err,
                 int* sched, int device);
 // every map the tiled kernels read at a stage whose stencil input is buffer `bin`
-TileMaps tile_maps(const TileCtx& tc, int bin, int irk);
+// (the interior kernel's maps for tiles of tr rows)
+TileMaps tile_maps(const TileCtx& tc, int bin, int irk, int tr);
 // Units of a tiled kernel: tile columns times chunks of x planes.
 //   interior kernel: the 32 x 8 tiles of the box lo..hi (the last ones partial);
 //   PML kernel: the nodes below the free-surface rows (k < ktop) outside the interior

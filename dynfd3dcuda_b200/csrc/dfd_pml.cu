@@ -648,7 +648,7 @@ static void pml_launch(const TileMaps& mp, const VolArgs& a, const TileSched& sc
 template <int FX, int FY, int FZ>
 static void launch_p(const TileCtx& tc, const VolArgs& a, int bin, const TileSched& ps, int grid, bool pdl,
                      cudaStream_t s) {
-  const TileMaps mp = tile_maps(tc, bin, a.irk);
+  const TileMaps mp = tile_maps(tc, bin, a.irk, tc.tr);
   pml_launch<FX, FY, FZ, false>(mp, a, ps, nullptr, 1, ps.nunits, grid, tc.err, tc.sched, pdl, s);
 }
 

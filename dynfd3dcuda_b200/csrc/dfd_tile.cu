@@ -420,7 +420,7 @@ TileSched tile_plan(int3 lo, int3 hi, int slots, int* grid, int tr) {
 
 // maps of stage irk with stencil input buffer bin; the second pointwise box reads, at
 // stage 2, the stage-1 input (the buffer the stage overwrites) and otherwise the accumulator
-TileMaps tile_maps(const TileCtx& tc, int bin, int irk) {
+TileMaps tile_maps(const TileCtx& tc, int bin, int irk, int tr) {
   TileMaps mp;
   memset(&mp, 0, sizeof mp);
   const int p2 = irk == 2 ? stage_out(2) : 3;
@@ -435,7 +435,7 @@ TileMaps tile_maps(const TileCtx& tc, int bin, int irk) {
   mp.plane_s = tc.plane_s;
   mp.auxy_s[0] = tc.auxy_s[0];
   mp.auxy_s[1] = tc.auxy_s[1];
-  const bool four = tc.tr == 4;
+  const bool four = tr == 4;
   mp.win_i = four ? tc.halo4[bin] : mp.win;
   mp.w0_i = four ? tc.centre4[0] : mp.w0;
   mp.t_i = four ? tc.centre4[p2] : mp.t;
@@ -446,7 +446,7 @@ TileMaps tile_maps(const TileCtx& tc, int bin, int irk) {
 template <int FX, int FY, int FZ, int TR>
 static void launch_tr(const TileCtx& tc, const VolArgs& a, int bin, int3 lo, int3 hi, cudaStream_t s) {
   using SH = TileShape<TR>;
-  const TileMaps mp = tile_maps(tc, bin, a.irk);
+  const TileMaps mp = tile_maps(tc, bin, a.irk, TR);
   int grid = 0;
   TileSched sc = tile_plan(lo, hi, tc.nsm * SH::CTAS, &grid, TR);
   sc.drill = tc.drill;
