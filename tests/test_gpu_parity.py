@@ -172,6 +172,9 @@ TILED_CASES = [
     ("vol_curved", {"NX": 36, "NY": 90, "NZ": 44, "useCerjan": 1, "DAMP_N": 8}),
     ("vol_curved", {"NX": 48, "NY": 110, "NZ": 60, "PML_N": 20}),  # two 16-wide strips per y slab
     ("vol_curved", {"NX": 40, "NY": 101, "NZ": 53, "PML_N": 13}),  # slab widths not multiples of 4
+    # the interior box ends at y = 96, not 100, where it would need a fourth tile column
+    # 4 nodes wide; the z1 slab keeps three whole z-tile rows and the box a partial row
+    ("vol_curved", {"NX": 48, "NY": 120, "NZ": 60, "PML_N": 20}),
 ]
 
 
